@@ -1,0 +1,236 @@
+/*
+ * qsmgpu.h — C ABI of the B200 (sm_100a) implementation of QSM.rs's FFT-driven
+ * reconstruction path: TV-ADMM, TKD/TSVD, Tikhonov, Laplacian unwrapping and
+ * SMV/SHARP/V-SHARP background removal, plus the pipeline dispatchers.
+ *
+ * Every entry point mirrors one function of the reference crate (astewartau/QSM.rs);
+ * the citation beside each declaration is the Rust function it replaces.  Conventions:
+ *   - volumes are flat arrays of nx*ny*nz values in Fortran order, index
+ *     i + j*nx + k*nx*ny (src/fft.rs:236-241); masks are uint8 (0 = outside);
+ *   - inputs are borrowed, outputs are caller-allocated buffers of the same length
+ *     (the Rust wrapper allocates the Vec and passes its pointer);
+ *   - plain entry points take HOST pointers and are synchronous; the *_device
+ *     variants take pointers to device memory on the context's GPU and return once
+ *     the result is written (the context's stream is synchronised);
+ *   - every function returns a qsm_status; qsm_last_error(ctx) describes the last
+ *     failure on that context.  A context is not thread-safe.
+ */
+#ifndef QSMGPU_H
+#define QSMGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define QSM_API __attribute__((visibility("default")))
+#else
+#define QSM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status -- */
+typedef enum {
+  QSM_OK = 0,
+  QSM_ERR_INVALID_ARGUMENT = 1, /* null pointer, non-finite or out-of-range parameter */
+  QSM_ERR_DIMENSION_MISMATCH = 2, /* PipelineError::DimensionMismatch (src/pipeline/config.rs:343-368) */
+  QSM_ERR_UNSUPPORTED_SIZE = 3, /* an axis length with a prime factor > 13, or too large */
+  QSM_ERR_ALLOC = 4,
+  QSM_ERR_CUDA = 5,
+  QSM_ERR_INVALID_CONFIG = 6, /* PipelineError::InvalidConfig */
+  QSM_ERR_NO_DEVICE = 7
+} qsm_status;
+
+/* Arithmetic used by a context.  QSM_PRECISION_F64 runs every FFT, stencil and
+ * reduction in double (the reference's arithmetic).  QSM_PRECISION_MIXED runs FFTs
+ * and stencils in float with FP64 reductions (convergence tests, norms) and FP64
+ * k-space multipliers; inputs and outputs stay double. */
+typedef enum { QSM_PRECISION_F64 = 0, QSM_PRECISION_MIXED = 1 } qsm_precision;
+
+typedef struct qsm_ctx qsm_ctx;
+
+/* Progress callback (current, max) — the reference's `impl FnMut(usize, usize)`. */
+typedef void (*qsm_progress_fn)(void* user, size_t current, size_t max);
+
+/* Grid — src/grid.rs:9-13 (dims, voxel_size in mm). */
+typedef struct {
+  size_t nx, ny, nz;
+  double vsx, vsy, vsz;
+} qsm_grid;
+
+/* ----------------------------------------------------------------- context -- */
+/* Create a context on CUDA device `device` with the given precision. */
+QSM_API qsm_status qsm_ctx_create(int device, int precision, qsm_ctx** out);
+QSM_API qsm_status qsm_ctx_destroy(qsm_ctx* ctx);
+QSM_API qsm_status qsm_ctx_set_precision(qsm_ctx* ctx, int precision);
+QSM_API int qsm_ctx_get_precision(const qsm_ctx* ctx);
+/* Free cached device workspaces (they are otherwise reused between calls). */
+QSM_API qsm_status qsm_ctx_release_workspace(qsm_ctx* ctx);
+QSM_API const char* qsm_last_error(const qsm_ctx* ctx);
+/* Number of kernels this context has launched (cumulative). */
+QSM_API uint64_t qsm_ctx_kernel_launches(const qsm_ctx* ctx);
+QSM_API const char* qsm_version(void);
+/* 1 when every axis length of `grid` has a transform plan (factors 2..13). */
+QSM_API int qsm_grid_supported(const qsm_grid* grid);
+
+/* ---------------------------------------------------------------- params --- */
+/* TvParams — src/inversion/tv.rs:23-43 (defaults 2e-4, 2e-2, 1e-3, 250). */
+typedef struct { double lambda, rho, tol; size_t max_iter; } qsm_tv_params;
+/* TkdParams — src/inversion/tkd.rs:23-32 (default threshold 0.15). */
+typedef struct { double threshold; } qsm_tkd_params;
+/* Regularization + TikhonovParams — src/inversion/tikhonov.rs:26-49. */
+typedef enum { QSM_REG_IDENTITY = 0, QSM_REG_GRADIENT = 1, QSM_REG_LAPLACIAN = 2 } qsm_regularization;
+typedef struct { double lambda; int reg; } qsm_tikhonov_params;
+/* SharpParams — src/bgremove/sharp.rs:22-37 (0.05, 6.0). */
+typedef struct { double threshold, radius; } qsm_sharp_params;
+/* VsharpParams — src/bgremove/vsharp.rs:22-40 (0.05, 12.0, 1.0). */
+typedef struct { double threshold, max_radius, min_radius; } qsm_vsharp_params;
+
+QSM_API void qsm_tv_params_default(qsm_tv_params* p);
+QSM_API void qsm_tkd_params_default(qsm_tkd_params* p);
+QSM_API void qsm_tikhonov_params_default(qsm_tikhonov_params* p);
+QSM_API void qsm_sharp_params_default(qsm_sharp_params* p);
+QSM_API void qsm_vsharp_params_default(qsm_vsharp_params* p);
+
+/* -------------------------------------------------------- dipole inversion -- */
+/* inversion::tv_admm — src/inversion/tv.rs:63-97 (+ admm.rs:76-178). */
+QSM_API qsm_status qsm_tv_admm(qsm_ctx* ctx, const double* local_field, const uint8_t* mask, const qsm_grid* grid,
+                       const double bdir[3], const qsm_tv_params* params, qsm_progress_fn progress, void* user,
+                       double* out_chi);
+QSM_API qsm_status qsm_tv_admm_device(qsm_ctx* ctx, const double* d_local_field, const uint8_t* d_mask,
+                              const qsm_grid* grid, const double bdir[3], const qsm_tv_params* params,
+                              qsm_progress_fn progress, void* user, double* d_out_chi);
+/* Iterations actually run by the last tv_admm call on this context (early exit). */
+QSM_API size_t qsm_tv_last_iterations(const qsm_ctx* ctx);
+
+/* inversion::tkd — src/inversion/tkd.rs:48-99. */
+QSM_API qsm_status qsm_tkd(qsm_ctx* ctx, const double* local_field, const uint8_t* mask, const qsm_grid* grid,
+                   const double bdir[3], const qsm_tkd_params* params, double* out_chi);
+QSM_API qsm_status qsm_tkd_device(qsm_ctx* ctx, const double* d_local_field, const uint8_t* d_mask, const qsm_grid* grid,
+                          const double bdir[3], const qsm_tkd_params* params, double* d_out_chi);
+/* inversion::tsvd — src/inversion/tkd.rs:105-153. */
+QSM_API qsm_status qsm_tsvd(qsm_ctx* ctx, const double* local_field, const uint8_t* mask, const qsm_grid* grid,
+                    const double bdir[3], const qsm_tkd_params* params, double* out_chi);
+QSM_API qsm_status qsm_tsvd_device(qsm_ctx* ctx, const double* d_local_field, const uint8_t* d_mask,
+                           const qsm_grid* grid, const double bdir[3], const qsm_tkd_params* params,
+                           double* d_out_chi);
+/* inversion::tikhonov — src/inversion/tikhonov.rs:62-138. */
+QSM_API qsm_status qsm_tikhonov(qsm_ctx* ctx, const double* local_field, const uint8_t* mask, const qsm_grid* grid,
+                        const double bdir[3], const qsm_tikhonov_params* params, double* out_chi);
+QSM_API qsm_status qsm_tikhonov_device(qsm_ctx* ctx, const double* d_local_field, const uint8_t* d_mask,
+                               const qsm_grid* grid, const double bdir[3], const qsm_tikhonov_params* params,
+                               double* d_out_chi);
+
+/* Forward dipole model out = Re IFFT(D * FFT(chi)) (src/fft.rs:214-233,
+ * apply_dipole_inplace), used to synthesise local fields. */
+QSM_API qsm_status qsm_dipole_forward(qsm_ctx* ctx, const double* chi, const qsm_grid* grid, const double bdir[3],
+                              double* out_field);
+
+/* ---------------------------------------------------------------- unwrap ---- */
+/* unwrap::laplacian_unwrap — src/unwrap/laplacian.rs:135-161. */
+QSM_API qsm_status qsm_laplacian_unwrap(qsm_ctx* ctx, const double* phase, const uint8_t* mask, const qsm_grid* grid,
+                                double* out_unwrapped);
+QSM_API qsm_status qsm_laplacian_unwrap_device(qsm_ctx* ctx, const double* d_phase, const uint8_t* d_mask,
+                                       const qsm_grid* grid, double* d_out_unwrapped);
+
+/* ----------------------------------------------------- background removal -- */
+/* bgremove::smv — src/bgremove/smv.rs:31-59. */
+QSM_API qsm_status qsm_smv(qsm_ctx* ctx, const double* field, const uint8_t* mask, const qsm_grid* grid, double radius,
+                   double* out_local, uint8_t* out_mask);
+/* bgremove::sharp — src/bgremove/sharp.rs:51-131. */
+QSM_API qsm_status qsm_sharp(qsm_ctx* ctx, const double* field, const uint8_t* mask, const qsm_grid* grid,
+                     const qsm_sharp_params* params, double* out_local, uint8_t* out_mask);
+/* bgremove::vsharp — src/bgremove/vsharp.rs:55-63. */
+QSM_API qsm_status qsm_vsharp(qsm_ctx* ctx, const double* field, const uint8_t* mask, const qsm_grid* grid,
+                      const qsm_vsharp_params* params, qsm_progress_fn progress, void* user, double* out_local,
+                      uint8_t* out_mask);
+/* bgremove::vsharp_with_radii — src/bgremove/vsharp.rs:88-199 (radii in mm, any order). */
+QSM_API qsm_status qsm_vsharp_with_radii(qsm_ctx* ctx, const double* field, const uint8_t* mask, const qsm_grid* grid,
+                                 const double* radii, size_t n_radii, double threshold, qsm_progress_fn progress,
+                                 void* user, double* out_local, uint8_t* out_mask);
+QSM_API qsm_status qsm_vsharp_with_radii_device(qsm_ctx* ctx, const double* d_field, const uint8_t* d_mask,
+                                        const qsm_grid* grid, const double* radii, size_t n_radii,
+                                        double threshold, qsm_progress_fn progress, void* user,
+                                        double* d_out_local, uint8_t* d_out_mask);
+
+/* ----------------------------------------------------------------- pipeline -- */
+/* InversionAlgorithm — src/pipeline/config.rs:47-58, same variant order.  Variants
+ * this library does not compute return QSM_ERR_INVALID_CONFIG; Tgv and Qsmart return
+ * it as the reference does (src/pipeline/inversion.rs:106-110). */
+typedef enum {
+  QSM_INV_TKD = 0,
+  QSM_INV_TSVD = 1,
+  QSM_INV_TIKHONOV = 2,
+  QSM_INV_TV = 3,
+  QSM_INV_RTS = 4,
+  QSM_INV_NLTV = 5,
+  QSM_INV_MEDI = 6,
+  QSM_INV_ILSQR = 7,
+  QSM_INV_TGV = 8,
+  QSM_INV_QSMART = 9
+} qsm_inversion_algorithm;
+
+/* ScanMetadata — src/pipeline/config.rs:302-324 (echo times not needed on this path). */
+typedef struct {
+  size_t nx, ny, nz;
+  double vsx, vsy, vsz;
+  double field_strength;
+  double b0_direction[3];
+} qsm_scan_metadata;
+
+/* InversionConfig subset — src/pipeline/config.rs:234-264. */
+typedef struct {
+  int algorithm;
+  qsm_tkd_params tkd;
+  qsm_tkd_params tsvd;
+  qsm_tikhonov_params tikhonov;
+  qsm_tv_params tv;
+} qsm_inversion_config;
+
+/* BgRemovalAlgorithm — src/pipeline/config.rs:33-42, same variant order.  Variants
+ * this library does not compute return QSM_ERR_INVALID_CONFIG. */
+typedef enum {
+  QSM_BG_VSHARP = 0,
+  QSM_BG_PDF = 1,
+  QSM_BG_LBV = 2,
+  QSM_BG_ISMV = 3,
+  QSM_BG_SHARP = 4,
+  QSM_BG_RESHARP = 5,
+  QSM_BG_HARPERELLA = 6,
+  QSM_BG_IHARPERELLA = 7
+} qsm_bg_algorithm;
+
+/* BgRemovalConfig subset — src/pipeline/config.rs:204-230 (default V-SHARP). */
+typedef struct {
+  int algorithm;
+  qsm_vsharp_params vsharp;
+  qsm_sharp_params sharp;
+} qsm_bg_removal_config;
+
+QSM_API void qsm_inversion_config_default(qsm_inversion_config* c);
+QSM_API void qsm_bg_removal_config_default(qsm_bg_removal_config* c);
+
+/* pipeline::run_dipole_inversion — src/pipeline/inversion.rs:28-114.  `len` is the
+ * length of local_field (checked against nx*ny*nz -> QSM_ERR_DIMENSION_MISMATCH). */
+QSM_API qsm_status qsm_run_dipole_inversion(qsm_ctx* ctx, const double* local_field_ppm, size_t len, const uint8_t* mask,
+                                    const qsm_scan_metadata* metadata, const qsm_inversion_config* config,
+                                    qsm_progress_fn progress, void* user, double* out_chi);
+/* pipeline::run_bg_removal — src/pipeline/bg_removal.rs:20-92. */
+QSM_API qsm_status qsm_run_bg_removal(qsm_ctx* ctx, const double* field_ppm, size_t len, const uint8_t* mask,
+                              const qsm_scan_metadata* metadata, const qsm_bg_removal_config* config,
+                              qsm_progress_fn progress, void* user, double* out_local_field,
+                              uint8_t* out_eroded_mask);
+
+/* ---------------------------------------------------------- FFT primitives -- */
+/* Forward 3D transform of a real volume, returned as the full complex spectrum
+ * (interleaved re, im; nx*ny*nz complex values) — src/fft.rs:412-430 fft3d on real
+ * data.  Exposed for parity testing of the transform engine. */
+QSM_API qsm_status qsm_fft3d_real(qsm_ctx* ctx, const double* in, const qsm_grid* grid, double* out_complex);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QSMGPU_H */

@@ -1,0 +1,233 @@
+// Context, workspace cache, twiddle tables, argument validation and the
+// context-level C ABI entry points.
+#include "internal.h"
+#include "common.cuh"
+
+#include <cstring>
+
+namespace qsm {
+
+void* ws_get(qsm_ctx* ctx, const std::string& name, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  DevBuf& b = ctx->ws[name];
+  if (b.bytes < bytes) {
+    if (b.p) {
+      QSM_CUDA(cudaStreamSynchronize(ctx->stream));
+      QSM_CUDA(cudaFree(b.p));
+      b.p = nullptr;
+      b.bytes = 0;
+    }
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      throw QsmError(QSM_ERR_ALLOC, "device allocation of " + std::to_string(bytes) + " bytes for '" + name +
+                                        "' failed: " + cudaGetErrorString(e));
+    }
+    b.p = p;
+    b.bytes = bytes;
+  }
+  return b.p;
+}
+
+void ws_release(qsm_ctx* ctx) {
+  cudaStreamSynchronize(ctx->stream);
+  for (auto& kv : ctx->ws)
+    if (kv.second.p) cudaFree(kv.second.p);
+  ctx->ws.clear();
+  for (auto& kv : ctx->graphs)
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+  ctx->graphs.clear();
+}
+
+FftPlan1D plan_or_throw(int n) {
+  FftPlan1D pl;
+  if (!make_fft_plan(n, &pl))
+    throw QsmError(QSM_ERR_UNSUPPORTED_SIZE,
+                   "axis length " + std::to_string(n) + " has no transform plan (prime factors must be <= 13, n <= " +
+                       std::to_string(kFftMaxLen) + ")");
+  return pl;
+}
+
+const void* twiddle_table(qsm_ctx* ctx, int n, bool dbl) {
+  const long long key = (long long)n * 2 + (dbl ? 1 : 0);
+  auto it = ctx->twiddles.find(key);
+  if (it != ctx->twiddles.end()) return it->second;
+  size_t elem = dbl ? sizeof(double2) : sizeof(float2);
+  std::vector<unsigned char> host(elem * (size_t)n);
+  for (int k = 0; k < n; ++k) {
+    // forward twiddle exp(-2 pi i k / n)
+    double c = cos2pi(k, n), s = -sin2pi(k, n);
+    if (dbl) {
+      double2 v = make_double2(c, s);
+      std::memcpy(&host[elem * k], &v, elem);
+    } else {
+      float2 v = make_float2((float)c, (float)s);
+      std::memcpy(&host[elem * k], &v, elem);
+    }
+  }
+  void* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, host.size());
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    throw QsmError(QSM_ERR_ALLOC, "twiddle table allocation failed");
+  }
+  QSM_CUDA(cudaMemcpy(d, host.data(), host.size(), cudaMemcpyHostToDevice));
+  ctx->twiddles[key] = d;
+  return d;
+}
+
+const void* upload_table(qsm_ctx* ctx, const std::string& key, const void* host, size_t bytes) {
+  auto it = ctx->tables.find(key);
+  if (it != ctx->tables.end()) return it->second;
+  void* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, bytes ? bytes : 16);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    throw QsmError(QSM_ERR_ALLOC, "table allocation failed");
+  }
+  if (bytes) QSM_CUDA(cudaMemcpy(d, host, bytes, cudaMemcpyHostToDevice));
+  ctx->tables[key] = d;
+  return d;
+}
+
+GridDims check_grid(const qsm_grid* g) {
+  if (g == nullptr) throw QsmError(QSM_ERR_INVALID_ARGUMENT, "grid is null");
+  if (g->nx == 0 || g->ny == 0 || g->nz == 0) throw QsmError(QSM_ERR_INVALID_ARGUMENT, "grid has a zero dimension");
+  if (g->nx > (size_t)kFftMaxLen || g->ny > (size_t)kFftMaxLen || g->nz > (size_t)kFftMaxLen)
+    throw QsmError(QSM_ERR_UNSUPPORTED_SIZE, "grid dimension above " + std::to_string(kFftMaxLen));
+  for (double v : {g->vsx, g->vsy, g->vsz})
+    if (!std::isfinite(v) || v <= 0.0) throw QsmError(QSM_ERR_INVALID_ARGUMENT, "voxel size must be finite and > 0");
+  GridDims d;
+  d.nx = (int)g->nx;
+  d.ny = (int)g->ny;
+  d.nz = (int)g->nz;
+  d.vsx = g->vsx;
+  d.vsy = g->vsy;
+  d.vsz = g->vsz;
+  d.n = (long long)d.nx * d.ny * d.nz;
+  if ((long long)d.ny * d.nz > (1LL << 30)) throw QsmError(QSM_ERR_UNSUPPORTED_SIZE, "too many rows");
+  plan_or_throw(d.nx);
+  plan_or_throw(d.ny);
+  plan_or_throw(d.nz);
+  return d;
+}
+
+void check_ptr(const void* p, const char* name) {
+  if (p == nullptr) throw QsmError(QSM_ERR_INVALID_ARGUMENT, std::string(name) + " is null");
+}
+
+void check_finite(double v, const char* name) {
+  if (!std::isfinite(v)) throw QsmError(QSM_ERR_INVALID_ARGUMENT, std::string(name) + " is not finite");
+}
+
+void h2d(qsm_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  QSM_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+}
+void d2h(qsm_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  QSM_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+}
+void sync(qsm_ctx* ctx) { QSM_CUDA(cudaStreamSynchronize(ctx->stream)); }
+
+}  // namespace qsm
+
+using namespace qsm;
+
+extern "C" {
+
+qsm_status qsm_ctx_create(int device, int precision, qsm_ctx** out) {
+  if (out == nullptr) return QSM_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (precision != QSM_PRECISION_F64 && precision != QSM_PRECISION_MIXED) return QSM_ERR_INVALID_ARGUMENT;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    (void)cudaGetLastError();
+    return QSM_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= count) return QSM_ERR_INVALID_ARGUMENT;
+  if (cudaSetDevice(device) != cudaSuccess) return QSM_ERR_CUDA;
+  qsm_ctx* c = new (std::nothrow) qsm_ctx();
+  if (!c) return QSM_ERR_ALLOC;
+  c->device = device;
+  c->precision = precision;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return QSM_ERR_CUDA;
+  }
+  *out = c;
+  return QSM_OK;
+}
+
+qsm_status qsm_ctx_destroy(qsm_ctx* ctx) {
+  if (ctx == nullptr) return QSM_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  ws_release(ctx);
+  for (auto& kv : ctx->twiddles) cudaFree(kv.second);
+  for (auto& kv : ctx->tables) cudaFree(kv.second);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return QSM_OK;
+}
+
+qsm_status qsm_ctx_set_precision(qsm_ctx* ctx, int precision) {
+  if (ctx == nullptr) return QSM_ERR_INVALID_ARGUMENT;
+  if (precision != QSM_PRECISION_F64 && precision != QSM_PRECISION_MIXED) {
+    ctx->err = "unknown precision";
+    return QSM_ERR_INVALID_ARGUMENT;
+  }
+  ctx->precision = precision;
+  return QSM_OK;
+}
+
+int qsm_ctx_get_precision(const qsm_ctx* ctx) { return ctx ? ctx->precision : -1; }
+
+qsm_status qsm_ctx_release_workspace(qsm_ctx* ctx) {
+  if (ctx == nullptr) return QSM_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  ws_release(ctx);
+  return QSM_OK;
+}
+
+const char* qsm_last_error(const qsm_ctx* ctx) {
+  if (ctx == nullptr) return "null context";
+  return ctx->err.c_str();
+}
+
+uint64_t qsm_ctx_kernel_launches(const qsm_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+const char* qsm_version(void) { return "qsmgpu 0.1.0 (sm_100a)"; }
+
+int qsm_grid_supported(const qsm_grid* grid) {
+  if (grid == nullptr) return 0;
+  return fft_length_supported((int)grid->nx) && fft_length_supported((int)grid->ny) &&
+         fft_length_supported((int)grid->nz);
+}
+
+void qsm_tv_params_default(qsm_tv_params* p) {
+  if (!p) return;
+  p->lambda = 2e-4;
+  p->rho = 2e-2;
+  p->tol = 1e-3;
+  p->max_iter = 250;
+}
+void qsm_tkd_params_default(qsm_tkd_params* p) {
+  if (p) p->threshold = 0.15;
+}
+void qsm_tikhonov_params_default(qsm_tikhonov_params* p) {
+  if (!p) return;
+  p->lambda = 0.01;
+  p->reg = QSM_REG_IDENTITY;
+}
+void qsm_sharp_params_default(qsm_sharp_params* p) {
+  if (!p) return;
+  p->threshold = 0.05;
+  p->radius = 6.0;
+}
+void qsm_vsharp_params_default(qsm_vsharp_params* p) {
+  if (!p) return;
+  p->threshold = 0.05;
+  p->max_radius = 12.0;
+  p->min_radius = 1.0;
+}
+
+}  // extern "C"

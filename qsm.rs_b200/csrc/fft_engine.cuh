@@ -1,0 +1,265 @@
+// Register/shared-memory Stockham FFT engine for one pencil per thread group.
+//
+// A 1D transform of length n is split into stages of radix R (2..16).  Each stage
+// is the autosort (Stockham) step: butterfly j reads its R inputs at j + r*(n/R),
+// twiddles input r by W_{Ns*R}^{(j mod Ns)*r} (Ns = product of the radices already
+// done), runs a register DFT of size R, and writes output r to
+// (j - j mod Ns)*R + (j mod Ns) + r*Ns.  The first stage reads straight from the
+// caller's fetch functor (global memory, coalesced across j) and the last stage
+// writes natural-order outputs straight through the emit functor, so a two-stage
+// transform crosses shared memory once.  Radices and the per-pencil thread count T
+// come from a host-side plan, so one kernel binary serves every supported length.
+//
+// Replaces the per-axis rustfft plans of the reference (src/fft.rs:42-234,
+// 423-479); the 3D passes built on this engine live in passes.cuh.
+#pragma once
+
+#include <utility>
+#include "common.cuh"
+#include "fft_plan.h"
+
+namespace qsm {
+
+template <long long P, long long Q> inline constexpr double kCos2pi = cos2pi(P, Q);
+template <long long P, long long Q> inline constexpr double kSin2pi = sin2pi(P, Q);
+
+// a * exp(DIR * 2*pi*i * M / R), M and R compile-time
+template <int DIR, int M, int R, typename C>
+__device__ __forceinline__ C tw_const(C a) {
+  constexpr int m = ((M % R) + R) % R;
+  using S = decltype(a.x);
+  if constexpr (m == 0) {
+    return a;
+  } else if constexpr (2 * m == R) {
+    return mk<C>(-a.x, -a.y);
+  } else if constexpr (4 * m == R) {
+    if constexpr (DIR < 0) return cmul_mi(a); else return cmul_i(a);
+  } else if constexpr (4 * m == 3 * R) {
+    if constexpr (DIR < 0) return cmul_i(a); else return cmul_mi(a);
+  } else {
+    constexpr S c = (S)kCos2pi<m, R>;
+    constexpr S s = (S)((double)DIR * kSin2pi<m, R>);
+    return mk<C>(c * a.x - s * a.y, c * a.y + s * a.x);
+  }
+}
+
+template <int R, int DIR, typename C> struct Dft;
+
+template <int DIR, typename C> struct Dft<1, DIR, C> {
+  static __device__ __forceinline__ void run(C*) {}
+};
+
+template <int DIR, typename C> struct Dft<2, DIR, C> {
+  static __device__ __forceinline__ void run(C* v) {
+    C a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  }
+};
+
+template <int DIR, typename C> struct Dft<4, DIR, C> {
+  static __device__ __forceinline__ void run(C* v) {
+    C t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+    C t2 = cadd(v[1], v[3]), d = csub(v[1], v[3]);
+    C t3 = (DIR < 0) ? cmul_mi(d) : cmul_i(d);  // (v1 - v3) * (DIR * i)
+    v[0] = cadd(t0, t2);
+    v[2] = csub(t0, t2);
+    v[1] = cadd(t1, t3);
+    v[3] = csub(t1, t3);
+  }
+};
+
+// Odd prime R via symmetric pairs: y_k = v0 + sum_m (v_m + v_{R-m}) cos(2 pi m k/R)
+//                                      + i*DIR*sum_m (v_m - v_{R-m}) sin(2 pi m k/R)
+template <int R, int DIR, typename C> struct DftOdd {
+  static constexpr int H = (R - 1) / 2;
+  template <int K, int... M>
+  static __device__ __forceinline__ void out_k(const C* s, const C* d, C v0, C* y, std::integer_sequence<int, M...>) {
+    using S = decltype(v0.x);
+    C A = v0;
+    C B = mk<C>(S(0), S(0));
+    ((A = mk<C>(A.x + (S)kCos2pi<(M + 1) * K, R> * s[M].x, A.y + (S)kCos2pi<(M + 1) * K, R> * s[M].y)), ...);
+    ((B = mk<C>(B.x + (S)kSin2pi<(M + 1) * K, R> * d[M].x, B.y + (S)kSin2pi<(M + 1) * K, R> * d[M].y)), ...);
+    C iB = (DIR < 0) ? cmul_mi(B) : cmul_i(B);
+    y[K] = cadd(A, iB);
+    y[R - K] = csub(A, iB);
+  }
+  template <int... K>
+  static __device__ __forceinline__ void all_k(const C* s, const C* d, C v0, C* y, std::integer_sequence<int, K...>) {
+    (out_k<K + 1>(s, d, v0, y, std::make_integer_sequence<int, H>{}), ...);
+  }
+  static __device__ __forceinline__ void run(C* v) {
+    C s[H], d[H];
+    C y0 = v[0];
+#pragma unroll
+    for (int m = 1; m <= H; ++m) {
+      s[m - 1] = cadd(v[m], v[R - m]);
+      d[m - 1] = csub(v[m], v[R - m]);
+      y0 = cadd(y0, s[m - 1]);
+    }
+    C y[R];
+    all_k(s, d, v[0], y, std::make_integer_sequence<int, H>{});
+    v[0] = y0;
+#pragma unroll
+    for (int k = 1; k < R; ++k) v[k] = y[k];
+  }
+};
+template <int DIR, typename C> struct Dft<3, DIR, C> : DftOdd<3, DIR, C> {};
+template <int DIR, typename C> struct Dft<5, DIR, C> : DftOdd<5, DIR, C> {};
+template <int DIR, typename C> struct Dft<7, DIR, C> : DftOdd<7, DIR, C> {};
+template <int DIR, typename C> struct Dft<11, DIR, C> : DftOdd<11, DIR, C> {};
+template <int DIR, typename C> struct Dft<13, DIR, C> : DftOdd<13, DIR, C> {};
+
+// Composite R = R1*R2 in registers (Cooley-Tukey with constant twiddles):
+// n = R2*n1 + n2, k = k1 + R1*k2.
+template <int R1, int R2, int DIR, typename C> struct DftSplit {
+  static constexpr int R = R1 * R2;
+  template <int N2, int... K1>
+  static __device__ __forceinline__ void twid(const C* t, C* a, std::integer_sequence<int, K1...>) {
+    ((a[N2 * R1 + K1] = tw_const<DIR, N2 * K1, R>(t[K1])), ...);
+  }
+  template <int N2>
+  static __device__ __forceinline__ void col(const C* v, C* a) {
+    C t[R1];
+#pragma unroll
+    for (int n1 = 0; n1 < R1; ++n1) t[n1] = v[R2 * n1 + N2];
+    Dft<R1, DIR, C>::run(t);
+    twid<N2>(t, a, std::make_integer_sequence<int, R1>{});
+  }
+  template <int... N2>
+  static __device__ __forceinline__ void step1(const C* v, C* a, std::integer_sequence<int, N2...>) {
+    (col<N2>(v, a), ...);
+  }
+  static __device__ __forceinline__ void run(C* v) {
+    C a[R];
+    step1(v, a, std::make_integer_sequence<int, R2>{});
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) {
+      C t[R2];
+#pragma unroll
+      for (int n2 = 0; n2 < R2; ++n2) t[n2] = a[n2 * R1 + k1];
+      Dft<R2, DIR, C>::run(t);
+#pragma unroll
+      for (int k2 = 0; k2 < R2; ++k2) v[k1 + R1 * k2] = t[k2];
+    }
+  }
+};
+template <int DIR, typename C> struct Dft<6, DIR, C> : DftSplit<2, 3, DIR, C> {};
+template <int DIR, typename C> struct Dft<8, DIR, C> : DftSplit<2, 4, DIR, C> {};
+template <int DIR, typename C> struct Dft<9, DIR, C> : DftSplit<3, 3, DIR, C> {};
+template <int DIR, typename C> struct Dft<10, DIR, C> : DftSplit<2, 5, DIR, C> {};
+template <int DIR, typename C> struct Dft<12, DIR, C> : DftSplit<4, 3, DIR, C> {};
+template <int DIR, typename C> struct Dft<15, DIR, C> : DftSplit<3, 5, DIR, C> {};
+template <int DIR, typename C> struct Dft<16, DIR, C> : DftSplit<4, 4, DIR, C> {};
+
+// ---------------------------------------------------------------------------
+// Shared-memory addressing of one pencil.  Strided: element e of column px of a
+// P-wide tile at sm[e*P + px] (Y/Z passes, 128-byte rows, conflict-free).
+// Padded: element e of a contiguous row at row[e + e/G] (X pass; the skew keeps
+// the stride-R writes of the first stage off a single bank).
+// ---------------------------------------------------------------------------
+struct SAStrided {
+  int P;
+  __device__ __forceinline__ int operator()(int e) const { return e * P; }
+};
+template <int G> struct SAPadded {
+  __device__ __forceinline__ int operator()(int e) const { return e + e / G; }
+};
+
+// One Stockham stage of compile-time radix R.  Every thread of the block must call
+// this (it contains __syncthreads); inactive threads skip the memory traffic.
+template <int R, int DIR, int EMAX, typename C, class SA, class Fetch, class Emit>
+__device__ __forceinline__ void fft_stage(C (&v)[EMAX], const FftPlan1D& pl, int s, int t, bool active,
+                                          C* sp, const SA& sa, const C* tw, Fetch& fetch, Emit& emit) {
+  constexpr int CM = EMAX / R;
+  const int n = pl.n;
+  const int nb = n / R;
+  const int T = pl.T;
+  const int Ns = pl.ns[s];
+  const int tws = pl.tws[s];
+  const bool first = (s == 0);
+  const bool last = (s == pl.nstages - 1);
+  if (active) {
+#pragma unroll
+    for (int c = 0; c < CM; ++c) {
+      const int j = t + c * T;
+      if (j < nb) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int e = j + r * nb;
+          v[c * R + r] = first ? fetch(e) : sp[sa(e)];
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (active) {
+#pragma unroll
+    for (int c = 0; c < CM; ++c) {
+      const int j = t + c * T;
+      if (j < nb) {
+        const int k = j % Ns;
+        if (!first) {
+#pragma unroll
+          for (int r = 1; r < R; ++r) {
+            const C w = tw[k * r * tws];
+            v[c * R + r] = (DIR < 0) ? cmul(v[c * R + r], w) : cmulc(v[c * R + r], w);
+          }
+        }
+        Dft<R, DIR, C>::run(&v[c * R]);
+        const int base = (j - k) * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int e = base + r * Ns;
+          if (last) emit(e, v[c * R + r]);
+          else sp[sa(e)] = v[c * R + r];
+        }
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// Full 1D transform of one pencil. DIR = -1 forward (exp(-2 pi i nk/n)), +1 inverse
+// (unnormalised).  tw points at the forward table W_n^k, k in [0, n).
+//
+// The pencil is read from global memory (SRC_G: gsrc[base + e*stride]) or from its
+// shared-memory slot (sp[sa(e)]), and written likewise (DST_G).  Solver-specific
+// work (loaders, multipliers, stores) runs in coalesced loops around this call, so
+// the engine is compiled once per I/O shape instead of once per solver operator.
+template <int DIR, typename C, class SA, bool SRC_G, bool DST_G>
+__device__ __noinline__ void fft_pencil(const FftPlan1D* plp, int t, bool active, C* sp, SA sa, const C* tw,
+                                        const C* gsrc, C* gdst, long long base, long long stride) {
+  const FftPlan1D& pl = *plp;
+  auto fetch = [&](int e) -> C {
+    if constexpr (SRC_G) return gsrc[base + e * stride];
+    else return sp[sa(e)];
+  };
+  auto emit = [&](int e, C v) {
+    if constexpr (DST_G) gdst[base + e * stride] = v;
+    else sp[sa(e)] = v;
+  };
+  constexpr int EMAX = kFftEmax;
+  C v[EMAX];
+  for (int s = 0; s < pl.nstages; ++s) {
+    switch (pl.radix[s]) {
+      case 1: fft_stage<1, DIR>(v, pl, s, t, active, sp, sa, tw, fetch, emit); break;
+      case 2: fft_stage<2, DIR>(v, pl, s, t, active, sp, sa, tw, fetch, emit); break;
+      case 3: fft_stage<3, DIR>(v, pl, s, t, active, sp, sa, tw, fetch, emit); break;
+      case 4: fft_stage<4, DIR>(v, pl, s, t, active, sp, sa, tw, fetch, emit); break;
+      case 5: fft_stage<5, DIR>(v, pl, s, t, active, sp, sa, tw, fetch, emit); break;
+      case 6: fft_stage<6, DIR>(v, pl, s, t, active, sp, sa, tw, fetch, emit); break;
+      case 7: fft_stage<7, DIR>(v, pl, s, t, active, sp, sa, tw, fetch, emit); break;
+      case 8: fft_stage<8, DIR>(v, pl, s, t, active, sp, sa, tw, fetch, emit); break;
+      case 9: fft_stage<9, DIR>(v, pl, s, t, active, sp, sa, tw, fetch, emit); break;
+      case 10: fft_stage<10, DIR>(v, pl, s, t, active, sp, sa, tw, fetch, emit); break;
+      case 11: fft_stage<11, DIR>(v, pl, s, t, active, sp, sa, tw, fetch, emit); break;
+      case 12: fft_stage<12, DIR>(v, pl, s, t, active, sp, sa, tw, fetch, emit); break;
+      case 13: fft_stage<13, DIR>(v, pl, s, t, active, sp, sa, tw, fetch, emit); break;
+      case 15: fft_stage<15, DIR>(v, pl, s, t, active, sp, sa, tw, fetch, emit); break;
+      default: fft_stage<16, DIR>(v, pl, s, t, active, sp, sa, tw, fetch, emit); break;
+    }
+  }
+}
+
+}  // namespace qsm

@@ -1,0 +1,107 @@
+// Host-side context, workspace cache and error plumbing behind the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/qsmgpu.h"
+#include "fft_plan.h"
+
+namespace qsm {
+
+struct QsmError : std::runtime_error {
+  qsm_status code;
+  QsmError(qsm_status c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define QSM_CUDA(call)                                                                   \
+  do {                                                                                   \
+    cudaError_t e__ = (call);                                                            \
+    if (e__ != cudaSuccess)                                                              \
+      throw ::qsm::QsmError(QSM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e__)); \
+  } while (0)
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+struct GraphCache {
+  cudaGraphExec_t exec = nullptr;
+  std::string key;
+};
+
+}  // namespace qsm
+
+struct qsm_ctx {
+  int device = 0;
+  int precision = QSM_PRECISION_F64;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  std::map<std::string, qsm::DevBuf> ws;
+  std::map<long long, void*> twiddles;  // key n*2 + (double ? 1 : 0)
+  std::map<std::string, void*> tables;  // small per-grid tables
+  std::map<std::string, qsm::GraphCache> graphs;
+  uint64_t launches = 0;
+  size_t tv_last_iters = 0;
+};
+
+namespace qsm {
+
+// Named device workspace, grown on demand and reused across calls.
+void* ws_get(qsm_ctx* ctx, const std::string& name, size_t bytes);
+template <typename P> P* ws(qsm_ctx* ctx, const std::string& name, size_t count) {
+  return reinterpret_cast<P*>(ws_get(ctx, name, count * sizeof(P)));
+}
+void ws_release(qsm_ctx* ctx);
+
+// Forward twiddle table W_n^k (k in [0,n)) on the device, float2 or double2.
+const void* twiddle_table(qsm_ctx* ctx, int n, bool dbl);
+FftPlan1D plan_or_throw(int n);
+
+// Upload a small host vector as a cached device table keyed by name.
+const void* upload_table(qsm_ctx* ctx, const std::string& key, const void* host, size_t bytes);
+
+// Validation helpers
+struct GridDims {
+  int nx, ny, nz;
+  double vsx, vsy, vsz;
+  long long n;
+};
+GridDims check_grid(const qsm_grid* g);
+void check_ptr(const void* p, const char* name);
+void check_finite(double v, const char* name);
+
+// Host <-> device staging used by the host-pointer entry points.
+void h2d(qsm_ctx* ctx, void* dst, const void* src, size_t bytes);
+void d2h(qsm_ctx* ctx, void* dst, const void* src, size_t bytes);
+void sync(qsm_ctx* ctx);
+
+// Run fn and convert exceptions into a status + last error string.
+template <class F> qsm_status guarded(qsm_ctx* ctx, F&& fn) {
+  if (ctx == nullptr) return QSM_ERR_INVALID_ARGUMENT;
+  try {
+    QSM_CUDA(cudaSetDevice(ctx->device));
+    fn();
+    ctx->err.clear();
+    return QSM_OK;
+  } catch (const QsmError& e) {
+    ctx->err = e.what();
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    ctx->err = "host allocation failed";
+    return QSM_ERR_ALLOC;
+  } catch (const std::exception& e) {
+    ctx->err = e.what();
+    return QSM_ERR_CUDA;
+  }
+}
+
+}  // namespace qsm

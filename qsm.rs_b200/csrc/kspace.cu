@@ -1,0 +1,93 @@
+// Host construction of the per-grid k-space tables (cached per context).
+#include "launch.cuh"
+
+#include <cmath>
+
+namespace qsm {
+
+namespace {
+
+// numpy-style fftfreq, src/fft.rs:544-566
+std::vector<double> fftfreq(int n, double d) {
+  std::vector<double> f(n);
+  const double val = 1.0 / ((double)n * d);
+  if (n % 2 == 0) {
+    for (int i = 0; i < n / 2; ++i) f[i] = (double)i * val;
+    for (int i = n / 2; i < n; ++i) f[i] = (double)(i - n) * val;
+  } else {
+    for (int i = 0; i <= (n - 1) / 2; ++i) f[i] = (double)i * val;
+    for (int i = (n + 1) / 2; i < n; ++i) f[i] = (double)(i - n) * val;
+  }
+  return f;
+}
+
+// One axis of Re(FFT(laplacian_kernel(negative=true))): the kernel holds 2h at 0 and
+// -h at indices 1 and n-1 (one entry when they coincide, none when n == 1),
+// src/kernels/laplacian.rs:20-61.
+std::vector<double> lapneg_axis(int n, double vs) {
+  const double h = 1.0 / (vs * vs);
+  std::vector<double> l(n);
+  for (int i = 0; i < n; ++i) {
+    double v = 2.0 * h;
+    if (n > 1) {
+      v -= h * cos2pi((long long)i * 1, n);
+      if (n - 1 != 1) v -= h * cos2pi((long long)i * (n - 1), n);
+    }
+    l[i] = v;
+  }
+  return l;
+}
+
+// Poisson eigenvalue of one axis, src/unwrap/laplacian.rs:91-105:
+// 2*(cos(2*pi*f) - 1)/h^2 with f = i/n (i <= n/2) or (i - n)/n.
+std::vector<double> poisson_axis(int n, double vs) {
+  const double idx2 = 1.0 / (vs * vs);
+  std::vector<double> q(n);
+  for (int i = 0; i < n; ++i) {
+    const double f = (i <= n / 2) ? (double)i / (double)n : ((double)i - (double)n) / (double)n;
+    q[i] = 2.0 * (std::cos(2.0 * kPi * f) - 1.0) * idx2;
+  }
+  return q;
+}
+
+const double* table(qsm_ctx* ctx, const std::string& key, const std::vector<double>& v) {
+  return (const double*)upload_table(ctx, key, v.data(), v.size() * sizeof(double));
+}
+
+std::string k(const char* what, int n, double vs) {
+  char buf[96];
+  std::snprintf(buf, sizeof buf, "%s:%d:%.17g", what, n, vs);
+  return buf;
+}
+
+}  // namespace
+
+KSpace make_kspace(qsm_ctx* ctx, const GridDims& d, const double bdir[3]) {
+  KSpace K;
+  K.fx = table(ctx, k("freq", d.nx, d.vsx), fftfreq(d.nx, d.vsx));
+  K.fy = table(ctx, k("freq", d.ny, d.vsy), fftfreq(d.ny, d.vsy));
+  K.fz = table(ctx, k("freq", d.nz, d.vsz), fftfreq(d.nz, d.vsz));
+  K.lx = table(ctx, k("lap", d.nx, d.vsx), lapneg_axis(d.nx, d.vsx));
+  K.ly = table(ctx, k("lap", d.ny, d.vsy), lapneg_axis(d.ny, d.vsy));
+  K.lz = table(ctx, k("lap", d.nz, d.vsz), lapneg_axis(d.nz, d.vsz));
+  K.qx = table(ctx, k("poi", d.nx, d.vsx), poisson_axis(d.nx, d.vsx));
+  K.qy = table(ctx, k("poi", d.ny, d.vsy), poisson_axis(d.ny, d.vsy));
+  K.qz = table(ctx, k("poi", d.nz, d.vsz), poisson_axis(d.nz, d.vsz));
+  K.nyqx = (d.nx % 2 == 0) ? d.nx / 2 : -1;
+  K.nyqy = (d.ny % 2 == 0) ? d.ny / 2 : -1;
+  K.nyqz = (d.nz % 2 == 0) ? d.nz / 2 : -1;
+  double bx = 0, by = 0, bz = 1;
+  if (bdir) {
+    bx = bdir[0];
+    by = bdir[1];
+    bz = bdir[2];
+  }
+  // src/kernels/dipole.rs:38-43 normalises b (a zero vector yields NaN there too)
+  const double bn = std::sqrt(bx * bx + by * by + bz * bz);
+  K.bx = bx / bn;
+  K.by = by / bn;
+  K.bz = bz / bn;
+  return K;
+}
+
+}  // namespace qsm

@@ -1,0 +1,180 @@
+// Host launchers for the pass kernels, the per-grid transform bundle and the
+// double-precision k-space geometry shared by every spectral multiplier.
+#pragma once
+
+#include "internal.h"
+#include "passes.cuh"
+
+namespace qsm {
+
+template <typename T> struct Fft3 {
+  Geom g;
+  FftPlan1D px, py, pz;
+  const cplx_t<T>* twx;
+  const cplx_t<T>* twy;
+  const cplx_t<T>* twz;
+};
+
+template <typename T> Fft3<T> make_fft3(qsm_ctx* ctx, const GridDims& d) {
+  Fft3<T> f;
+  f.g.nx = d.nx;
+  f.g.ny = d.ny;
+  f.g.nz = d.nz;
+  f.g.nxh = d.nx / 2 + 1;
+  // rows start on 32-byte boundaries in both precisions, and float and double
+  // spectra of one grid share a layout (mixed-precision ops index both)
+  f.g.pitch = (f.g.nxh + 3) / 4 * 4;
+  f.px = plan_or_throw(d.nx);
+  f.py = plan_or_throw(d.ny);
+  f.pz = plan_or_throw(d.nz);
+  const bool dbl = sizeof(T) == 8;
+  f.twx = (const cplx_t<T>*)twiddle_table(ctx, d.nx, dbl);
+  f.twy = (const cplx_t<T>*)twiddle_table(ctx, d.ny, dbl);
+  f.twz = (const cplx_t<T>*)twiddle_table(ctx, d.nz, dbl);
+  return f;
+}
+
+template <class K> void ensure_smem(K kernel, size_t bytes) {
+  if (bytes > 227u * 1024u) throw QsmError(QSM_ERR_UNSUPPORTED_SIZE, "transform tile exceeds shared memory");
+  static size_t done = 48u * 1024u;  // one per kernel instantiation
+  if (bytes > done) {
+    QSM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    done = bytes;
+  }
+}
+
+inline void after_launch(qsm_ctx* ctx) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) throw QsmError(QSM_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  ctx->launches++;
+}
+
+// Threads per pencil in the X passes: the plan's T rounded up to a divisor of 32
+// (T <= 32) or to a multiple of 32, so that a block is a whole number of warps.
+inline int x_block_t(int T_) {
+  if (T_ <= 32) {
+    int b = 1;
+    while (b < T_) b <<= 1;
+    return b;
+  }
+  return (T_ + 31) / 32 * 32;
+}
+
+template <typename T> inline int x_pencils_per_block(int T_) {
+  int P = 256 / x_block_t(T_);
+  if (P < 1) P = 1;
+  return P;
+}
+
+template <typename T> inline long long x_blocks(const Fft3<T>& f) {
+  const int P = x_pencils_per_block<T>(f.px.T);
+  const long long npairs = ((long long)f.g.nrows() + 1) / 2;
+  return (npairs + P - 1) / P;
+}
+
+template <typename T, class Load>
+void run_x_r2c(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* spec, const Load& ld, const int* done) {
+  using C = cplx_t<T>;
+  const int Tt = x_block_t(f.px.T);
+  const int P = x_pencils_per_block<T>(f.px.T);
+  const size_t smem = (size_t)(f.px.n + P * x_rowlen<T>(f.px.n)) * sizeof(C);
+  auto kern = k_x_r2c<T, Load>;
+  ensure_smem(kern, smem);
+  kern<<<(unsigned)x_blocks(f), dim3(Tt, P), smem, ctx->stream>>>(f.g, f.px, f.twx, spec, ld, done);
+  after_launch(ctx);
+}
+
+template <typename T, class Store>
+void run_x_c2r(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* spec, const Store& st, const int* done) {
+  using C = cplx_t<T>;
+  const int Tt = x_block_t(f.px.T);
+  const int P = x_pencils_per_block<T>(f.px.T);
+  const size_t smem = (size_t)(f.px.n + P * x_rowlen<T>(f.px.n)) * sizeof(C);
+  auto kern = k_x_c2r<T, Store>;
+  ensure_smem(kern, smem);
+  kern<<<(unsigned)x_blocks(f), dim3(Tt, P), smem, ctx->stream>>>(f.g, f.px, f.twx, spec, st, done);
+  after_launch(ctx);
+}
+
+template <typename T> inline int yz_cols() { return sizeof(T) == 4 ? 16 : 8; }
+
+// AXIS 1 = y, 2 = z; DIR -1 forward, +1 inverse.
+template <typename T, int DIR, int AXIS, class Op>
+void run_yz(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst, const Op& op, const int* done) {
+  using C = cplx_t<T>;
+  const FftPlan1D& pl = (AXIS == 1) ? f.py : f.pz;
+  const cplx_t<T>* tw = (AXIS == 1) ? f.twy : f.twz;
+  const int P = yz_cols<T>();
+  if (P * pl.T > 1024) throw QsmError(QSM_ERR_UNSUPPORTED_SIZE, "axis too long for one tile");
+  const size_t smem = (size_t)(pl.n + pl.n * P) * sizeof(C);
+  auto kern = k_pass_yz<T, DIR, AXIS, Op>;
+  ensure_smem(kern, smem);
+  dim3 grid((f.g.nxh + P - 1) / P, AXIS == 1 ? f.g.nz : f.g.ny);
+  kern<<<grid, dim3(P, pl.T), smem, ctx->stream>>>(f.g, pl, tw, src, dst, op, done);
+  after_launch(ctx);
+}
+
+template <typename T, class Op>
+void run_z_fused(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst, const Op& op,
+                 const int* done) {
+  using C = cplx_t<T>;
+  const FftPlan1D& pl = f.pz;
+  const int P = yz_cols<T>();
+  if (P * pl.T > 1024) throw QsmError(QSM_ERR_UNSUPPORTED_SIZE, "axis too long for one tile");
+  const size_t smem = (size_t)(pl.n + pl.n * P) * sizeof(C);
+  auto kern = k_z_fused<T, Op>;
+  ensure_smem(kern, smem);
+  dim3 grid((f.g.nxh + P - 1) / P, f.g.ny);
+  kern<<<grid, dim3(P, pl.T), smem, ctx->stream>>>(f.g, pl, f.twz, src, dst, op, done);
+  after_launch(ctx);
+}
+
+// ---------------------------------------------------------------------------
+// k-space geometry in double: fftfreq per axis (src/fft.rs:544-566), per-axis
+// eigenvalues of the negative 7-point Laplacian (the FFT of
+// laplacian_kernel(negative=true), src/kernels/laplacian.rs:20-61, which is a sum of
+// per-axis terms), the Poisson eigenvalues of the unwrapping solver
+// (src/unwrap/laplacian.rs:91-105), and the normalised B0 direction.
+// ---------------------------------------------------------------------------
+struct KSpace {
+  const double* fx;
+  const double* fy;
+  const double* fz;
+  const double* lx;
+  const double* ly;
+  const double* lz;
+  const double* qx;
+  const double* qy;
+  const double* qz;
+  int nyqx, nyqy, nyqz;  // index n/2 for even n, else -1
+  double bx, by, bz;
+
+  __device__ __forceinline__ double dipole(double kx, double ky, double kz) const {
+    const double kdb = kx * bx + ky * by + kz * bz;
+    const double k2 = kx * kx + ky * ky + kz * kz;
+    return k2 > 1e-20 ? (1.0 / 3.0) - (kdb * kdb) / k2 : 0.0;
+  }
+  __device__ __forceinline__ double lapneg(int ix, int iy, int iz) const { return (lx[ix] + ly[iy]) + lz[iz]; }
+  __device__ __forceinline__ double poisson(int ix, int iy, int iz) const { return (qx[ix] + qy[iy]) + qz[iz]; }
+  __device__ __forceinline__ bool on_nyquist(int ix, int iy, int iz) const {
+    return ix == nyqx || iy == nyqy || iz == nyqz;
+  }
+  // Evaluate a multiplier M(kx,ky,kz,ix,iy,iz) symmetrised over k -> -k: the C2C
+  // reference keeps Re(IFFT(F * M)), which equals IFFT(F * (M(k) + M(-k))/2) for real
+  // input.  M(-k) differs from M(k) only on even-length Nyquist planes, where the
+  // mirrored index keeps its frequency -n/2 while the other coordinates flip sign.
+  template <class F>
+  __device__ __forceinline__ double sym(int ix, int iy, int iz, const F& m) const {
+    const double kx = fx[ix], ky = fy[iy], kz = fz[iz];
+    double v = m(kx, ky, kz, ix, iy, iz);
+    if (on_nyquist(ix, iy, iz)) {
+      const double v2 = m(ix == nyqx ? -kx : kx, iy == nyqy ? -ky : ky, iz == nyqz ? -kz : kz, ix, iy, iz);
+      v = 0.5 * (v + v2);
+    }
+    return v;
+  }
+};
+
+KSpace make_kspace(qsm_ctx* ctx, const GridDims& d, const double bdir[3]);
+
+}  // namespace qsm

@@ -1,0 +1,87 @@
+"""Background field removal — mirrors the reference's ``bgremove`` module (src/bgremove/)."""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Callable, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from . import Grid, Context, _ctx, _check, _as_f64, _as_u8, _ptr_d, _ptr_u8, _progress, _check_len
+
+
+@dataclass
+class SharpParams:
+    """src/bgremove/sharp.rs:22-37."""
+
+    threshold: float = 0.05
+    radius: float = 6.0
+
+    def _c(self):
+        return _lib.QsmSharpParams(self.threshold, self.radius)
+
+
+@dataclass
+class VsharpParams:
+    """src/bgremove/vsharp.rs:22-40."""
+
+    threshold: float = 0.05
+    max_radius: float = 12.0
+    min_radius: float = 1.0
+
+    def _c(self):
+        return _lib.QsmVsharpParams(self.threshold, self.max_radius, self.min_radius)
+
+
+def _io(field, mask, grid):
+    f = _as_f64(field, grid, "field")
+    m = _as_u8(mask, "mask")
+    _check_len(f, grid, "field")
+    _check_len(m, grid, "mask")
+    return f, m, np.empty_like(f), np.empty_like(m)
+
+
+def smv(field, mask, grid: Grid, radius: float, *, ctx: Optional[Context] = None):
+    """bgremove::smv (src/bgremove/smv.rs:31-59) -> (local_field, eroded_mask)."""
+    c = _ctx(ctx)
+    f, m, out, om = _io(field, mask, grid)
+    g = grid._c()
+    _check(c, c._lib.qsm_smv(c.handle, _ptr_d(f), _ptr_u8(m), C.byref(g), float(radius), _ptr_d(out), _ptr_u8(om)))
+    return out, om
+
+
+def sharp(field, mask, grid: Grid, params: SharpParams = SharpParams(), *, ctx: Optional[Context] = None):
+    """bgremove::sharp (src/bgremove/sharp.rs:51-131) -> (local_field, eroded_mask)."""
+    c = _ctx(ctx)
+    f, m, out, om = _io(field, mask, grid)
+    g = grid._c()
+    p = params._c()
+    _check(c, c._lib.qsm_sharp(c.handle, _ptr_d(f), _ptr_u8(m), C.byref(g), C.byref(p), _ptr_d(out), _ptr_u8(om)))
+    return out, om
+
+
+def vsharp(field, mask, grid: Grid, params: VsharpParams = VsharpParams(),
+           progress: Optional[Callable[[int, int], None]] = None, *, ctx: Optional[Context] = None):
+    """bgremove::vsharp (src/bgremove/vsharp.rs:55-63) -> (local_field, final_mask)."""
+    c = _ctx(ctx)
+    f, m, out, om = _io(field, mask, grid)
+    g = grid._c()
+    p = params._c()
+    cb, _keep = _progress(progress)
+    _check(c, c._lib.qsm_vsharp(c.handle, _ptr_d(f), _ptr_u8(m), C.byref(g), C.byref(p), cb, None, _ptr_d(out),
+                                _ptr_u8(om)))
+    return out, om
+
+
+def vsharp_with_radii(field, mask, grid: Grid, radii: Sequence[float], threshold: float,
+                      progress: Optional[Callable[[int, int], None]] = None, *, ctx: Optional[Context] = None):
+    """bgremove::vsharp_with_radii (src/bgremove/vsharp.rs:88-199)."""
+    c = _ctx(ctx)
+    f, m, out, om = _io(field, mask, grid)
+    g = grid._c()
+    r = np.ascontiguousarray(np.asarray(list(radii), dtype=np.float64))
+    cb, _keep = _progress(progress)
+    _check(c, c._lib.qsm_vsharp_with_radii(c.handle, _ptr_d(f), _ptr_u8(m), C.byref(g), _ptr_d(r), r.size,
+                                           float(threshold), cb, None, _ptr_d(out), _ptr_u8(om)))
+    return out, om

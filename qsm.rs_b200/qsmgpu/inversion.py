@@ -1,0 +1,135 @@
+"""Dipole inversion — mirrors the reference's ``inversion`` module (src/inversion/)."""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Callable, Optional
+
+import numpy as np
+
+from . import _lib
+from . import Grid, Context, _ctx, _check, _as_f64, _as_u8, _ptr_d, _ptr_u8, _bdir, _progress, _check_len
+
+IDENTITY, GRADIENT, LAPLACIAN = 0, 1, 2  # Regularization, src/inversion/tikhonov.rs:26-34
+
+
+@dataclass
+class TvParams:
+    """src/inversion/tv.rs:23-43."""
+
+    lambda_: float = 2e-4
+    rho: float = 2e-2
+    tol: float = 1e-3
+    max_iter: int = 250
+
+    def _c(self):
+        return _lib.QsmTvParams(self.lambda_, self.rho, self.tol, int(self.max_iter))
+
+
+@dataclass
+class TkdParams:
+    """src/inversion/tkd.rs:23-32."""
+
+    threshold: float = 0.15
+
+    def _c(self):
+        return _lib.QsmTkdParams(self.threshold)
+
+
+@dataclass
+class TikhonovParams:
+    """src/inversion/tikhonov.rs:38-49."""
+
+    lambda_: float = 0.01
+    reg: int = IDENTITY
+
+    def _c(self):
+        return _lib.QsmTikhonovParams(self.lambda_, int(self.reg))
+
+
+def _closed(fn_name, local_field, mask, grid: Grid, bdir, params, ctx):
+    c = _ctx(ctx)
+    f = _as_f64(local_field, grid, "local_field")
+    m = _as_u8(mask, "mask")
+    _check_len(f, grid, "local_field")
+    _check_len(m, grid, "mask")
+    out = np.empty_like(f)
+    b, _keep = _bdir(bdir)
+    g = grid._c()
+    p = params._c()
+    st = getattr(c._lib, fn_name)(c.handle, _ptr_d(f), _ptr_u8(m), C.byref(g), b, C.byref(p), _ptr_d(out))
+    _check(c, st)
+    return out
+
+
+def tkd(local_field, mask, grid: Grid, bdir=(0.0, 0.0, 1.0), params: TkdParams = TkdParams(), *,
+        ctx: Optional[Context] = None):
+    """inversion::tkd (src/inversion/tkd.rs:48-99)."""
+    return _closed("qsm_tkd", local_field, mask, grid, bdir, params, ctx)
+
+
+def tsvd(local_field, mask, grid: Grid, bdir=(0.0, 0.0, 1.0), params: TkdParams = TkdParams(), *,
+         ctx: Optional[Context] = None):
+    """inversion::tsvd (src/inversion/tkd.rs:105-153)."""
+    return _closed("qsm_tsvd", local_field, mask, grid, bdir, params, ctx)
+
+
+def tikhonov(local_field, mask, grid: Grid, bdir=(0.0, 0.0, 1.0), params: TikhonovParams = TikhonovParams(), *,
+             ctx: Optional[Context] = None):
+    """inversion::tikhonov (src/inversion/tikhonov.rs:62-138)."""
+    return _closed("qsm_tikhonov", local_field, mask, grid, bdir, params, ctx)
+
+
+def tv_admm(local_field, mask, grid: Grid, bdir=(0.0, 0.0, 1.0), params: TvParams = TvParams(),
+            progress: Optional[Callable[[int, int], None]] = None, *, ctx: Optional[Context] = None):
+    """inversion::tv_admm (src/inversion/tv.rs:63-97).
+
+    progress(iter, max_iter) is called once per iteration (delivered in batches between
+    CUDA-graph launches) and (iters, iters) on convergence, as in the reference.
+    """
+    c = _ctx(ctx)
+    f = _as_f64(local_field, grid, "local_field")
+    m = _as_u8(mask, "mask")
+    _check_len(f, grid, "local_field")
+    _check_len(m, grid, "mask")
+    out = np.empty_like(f)
+    b, _keep = _bdir(bdir)
+    g = grid._c()
+    p = params._c()
+    cb, _cbkeep = _progress(progress)
+    st = c._lib.qsm_tv_admm(c.handle, _ptr_d(f), _ptr_u8(m), C.byref(g), b, C.byref(p), cb, None, _ptr_d(out))
+    _check(c, st)
+    return out
+
+
+def tv_admm_device(ctx: Context, d_local_field: int, d_mask: int, grid: Grid, bdir, params: TvParams,
+                   d_out: int, progress=None):
+    """Device-pointer variant (inputs/outputs already on ctx's GPU); pointers are ints."""
+    b, _keep = _bdir(bdir)
+    g = grid._c()
+    p = params._c()
+    cb, _cbkeep = _progress(progress)
+    st = ctx._lib.qsm_tv_admm_device(ctx.handle, C.c_void_p(d_local_field), C.c_void_p(d_mask), C.byref(g), b,
+                                     C.byref(p), cb, None, C.c_void_p(d_out))
+    _check(ctx, st)
+
+
+def tkd_device(ctx: Context, d_local_field: int, d_mask: int, grid: Grid, bdir, params: TkdParams, d_out: int):
+    b, _keep = _bdir(bdir)
+    g = grid._c()
+    p = params._c()
+    st = ctx._lib.qsm_tkd_device(ctx.handle, C.c_void_p(d_local_field), C.c_void_p(d_mask), C.byref(g), b,
+                                 C.byref(p), C.c_void_p(d_out))
+    _check(ctx, st)
+
+
+def dipole_forward(chi, grid: Grid, bdir=(0.0, 0.0, 1.0), *, ctx: Optional[Context] = None):
+    """Re IFFT(D * FFT(chi)) (src/fft.rs:214-233)."""
+    c = _ctx(ctx)
+    x = _as_f64(chi, grid, "chi")
+    _check_len(x, grid, "chi")
+    out = np.empty_like(x)
+    b, _keep = _bdir(bdir)
+    g = grid._c()
+    _check(c, c._lib.qsm_dipole_forward(c.handle, _ptr_d(x), C.byref(g), b, _ptr_d(out)))
+    return out
