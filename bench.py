@@ -1,0 +1,416 @@
+#!/usr/bin/env python
+"""Benchmark: TV-ADMM dipole inversion throughput on B200.
+
+Workload (one "step"): one TV-ADMM solve (src/inversion/tv.rs:63-97) of a 256x256x176
+volume at 1 mm, B0 = z, default TvParams with tol = 0 so that exactly 250 iterations run,
+mixed precision (float FFTs and stencils, FP64 reductions and multipliers).  Input is a
+seeded synthetic ellipsoid phantom inside a 100x120x75-voxel ellipsoid brain mask
+(local field = dipole-convolved chi + N(0, 0.01 ppm) noise); no public dataset is used.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Ranks (torchrun, one per GPU) each solve their own volumes (weak scaling, no collective
+in the data path); value = volumes all ranks solved / max-over-ranks device time.
+Rank 0 prints one JSON line.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "qsm.rs_b200"))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+DIMS = (256, 256, 176)
+ITERS = 250
+METRIC = "TV-ADMM volumes/s at 256x256x176 (250 iterations)"
+UNIT = "volumes/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--skip-cpu-baseline", action="store_true")
+    ap.add_argument("--skip-fp64", action="store_true")
+    ap.add_argument("--one-shot", type=int, default=0, metavar="ITERS",
+                    help="profiling aid: run one TV-ADMM solve of ITERS iterations (mixed) and exit")
+    ap.add_argument("--one-shot-precision", default="mixed", choices=["mixed", "f64"])
+    return ap.parse_args()
+
+
+def one_shot(args):
+    """Small, self-contained run for ncu captures: one full-size solve, no timing."""
+    import torch
+    import qsmgpu
+    from qsmgpu import Grid, inversion
+    f, mask = make_case(0)
+    dev = torch.device("cuda", 0)
+    d_f = torch.from_numpy(f.ravel()).to(dev)
+    d_m = torch.from_numpy(mask.ravel()).to(dev)
+    d_o = torch.empty(f.size, dtype=torch.float64, device=dev)
+    with qsmgpu.Context(0, args.one_shot_precision) as ctx:
+        inversion.tv_admm_device(ctx, d_f.data_ptr(), d_m.data_ptr(), Grid.new(*DIMS), (0.0, 0.0, 1.0),
+                                 inversion.TvParams(2e-4, 2e-2, 0.0, args.one_shot), d_o.data_ptr())
+    torch.cuda.synchronize()
+    print(f"one-shot ok: {args.one_shot} iterations, |chi|max={float(d_o.abs().max()):.4g}")
+
+
+def make_case(seed):
+    from qsmgpu import phantom
+    nx, ny, nz = DIMS
+    rng = np.random.default_rng(seed)
+    shape = (nz, ny, nx)
+    mask = phantom.ellipsoid_mask(shape, (100.0, 120.0, 75.0))
+    chi = np.zeros(shape)
+    ctr = ((nx - 1) / 2, (ny - 1) / 2, (nz - 1) / 2)
+    box = [(ctr[0] - 60, ctr[0] + 60), (ctr[1] - 72, ctr[1] + 72), (ctr[2] - 45, ctr[2] + 45)]
+    phantom.add_ellipsoids(chi, rng, 12, box)
+    chi *= mask
+    f = phantom.forward_field(chi) + rng.normal(0.0, 0.01, size=shape) * mask
+    return np.ascontiguousarray(f), np.ascontiguousarray(mask)
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.samples = []
+        self.proc = None
+        self.t0 = self.t1 = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
+                 "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append((time.time(), line.strip()))
+
+    def mark(self, which):
+        if which == "start":
+            self.t0 = time.time()
+        else:
+            self.t1 = time.time()
+
+    def stop(self):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = [s for (t, s) in self.samples if self.t0 is not None and self.t0 - 0.05 <= t <= (self.t1 or t) + 0.05]
+        if not rows:
+            rows = [s for (_, s) in self.samples]
+        sms, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            p = [x.strip() for x in r.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sms.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sms) if sms else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sms)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def kernel_bytes_model(N, s):
+    """Algorithmic bytes per launch of each TV-ADMM kernel (s = 4 FP32, 8 FP64).
+    A half spectrum is counted as N*s bytes."""
+    return {
+        "tv_stencil": 8 * N * s,   # read x, u(3); write u(3), div
+        "fft_x_r2c": 2 * N * s,    # read div, write spectrum
+        "fft_y_fwd": 2 * N * s,
+        "fft_z_fused": 3 * N * s,  # read spectrum + f_hat, write spectrum
+        "fft_y_inv": 2 * N * s,
+        "fft_x_c2r": 3 * N * s,    # read spectrum + x_prev, write x
+    }
+
+
+def _timed_oracle_tv(f, mask, iters):
+    """Run the oracle TV-ADMM for `iters` iterations and time the spectral preparation and
+    each iteration through the progress callback (called at the start of every iteration,
+    src/inversion/tv.rs:81)."""
+    from oracle import qsm_oracle as O
+    grid = O.Grid.new(*DIMS)
+    stamps = []
+    t0 = time.perf_counter()
+    O.tv_admm(f, mask, grid, (0, 0, 1), O.TvParams(2e-4, 2e-2, 0.0, iters),
+              lambda a, b: stamps.append(time.perf_counter()))
+    t_end = time.perf_counter()
+    stamps.append(t_end)
+    t_prep = stamps[0] - t0
+    per_iter = [b - a for a, b in zip(stamps[:-1], stamps[1:])]
+    return t_prep, per_iter
+
+
+def cpu_baseline_tv(f, mask, budget_iters=4):
+    """Oracle (f64 numpy/scipy restatement) timed on this host: preparation + a few
+    iterations at full size; per-volume time = prep + ITERS * median iteration time."""
+    from oracle import qsm_oracle as O
+    cores = os.cpu_count() or 1
+    O.set_fft_workers(cores)
+    try:
+        t_prep, per_iter = _timed_oracle_tv(f, mask, budget_iters)
+    finally:
+        O.set_fft_workers(None)
+    t_iter = statistics.median(per_iter[1:] if len(per_iter) > 1 else per_iter)
+    vol_s = t_prep + ITERS * t_iter
+    return {"value": 1.0 / vol_s, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"oracle TV-ADMM at {DIMS[0]}x{DIMS[1]}x{DIMS[2]}: preparation + {budget_iters} iterations "
+                      f"timed, scaled to {ITERS} ({t_iter * 1e3:.0f} ms/iteration, scipy.fft workers={cores})",
+            "ms_per_iteration": t_iter * 1e3}
+
+
+def run_reference(args):
+    """Reference arm: the reference (Rust) cannot be built here, so its CPU algorithm is
+    timed through the f64 restatement in oracle/ on this host's cores, same workload.
+    A step is one TV-ADMM iteration at full size (a bounded sample of the 250-iteration
+    solve); the volume rate adds the one-off spectral preparation."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import qsm_oracle as O
+    f, mask = make_case(0)
+    cores = os.cpu_count() or 1
+    O.set_fft_workers(cores)
+    try:
+        t_prep, per_iter = _timed_oracle_tv(f, mask, args.warmup + args.steps)
+    finally:
+        O.set_fft_workers(None)
+    timed = per_iter[args.warmup:]
+    t_iter = statistics.median(timed)
+    vol_s = t_prep + ITERS * t_iter
+    v = 1.0 / vol_s
+    sample = (f"{args.steps} timed TV-ADMM iterations at {DIMS[0]}x{DIMS[1]}x{DIMS[2]} after {args.warmup} warm-up "
+              f"(oracle port, scipy.fft workers={cores}), scaled to {ITERS} iterations + preparation "
+              f"({t_prep:.2f} s)")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_iter * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"tv_admm {DIMS[0]}x{DIMS[1]}x{DIMS[2]} x{ITERS} iterations",
+                       "iterations": ITERS, "precision": "f64 (reference CPU arithmetic)"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    if args.one_shot:
+        one_shot(args)
+        return
+
+    import torch
+    import qsmgpu
+    from qsmgpu import Grid, inversion
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    f, mask = make_case(rank)
+    N = f.size
+    grid = Grid.new(*DIMS)
+    bdir = (0.0, 0.0, 1.0)
+    params = inversion.TvParams(2e-4, 2e-2, 0.0, ITERS)
+    dev = torch.device("cuda", local)
+    d_f = torch.from_numpy(f.ravel()).to(dev)
+    d_m = torch.from_numpy(mask.ravel()).to(dev)
+    d_out = torch.empty(N, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+
+    ctx = qsmgpu.Context(local, "mixed")
+    stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=dev)
+
+    def step():
+        inversion.tv_admm_device(ctx, d_f.data_ptr(), d_m.data_ptr(), grid, bdir, params, d_out.data_ptr())
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = ctx.kernel_launches()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    clocks.mark("start")
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clocks.mark("stop")
+    launches = ctx.kernel_launches() - l0
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    clocks.stop()
+    chi_mixed = d_out.cpu().numpy().copy()
+    value = world * args.steps / (ms / 1e3)
+    ms_step = ms / args.steps
+
+    # end to end through the host API: page-locked host input/output, H2D + solve + D2H
+    h_f = torch.from_numpy(f.ravel()).pin_memory()
+    h_m = torch.from_numpy(mask.ravel()).pin_memory()
+    h_o = torch.empty(N, dtype=torch.float64).pin_memory()
+    hf, hm, ho = h_f.numpy(), h_m.numpy(), h_o.numpy()
+    inversion.tv_admm(hf, hm, grid, bdir, params, ctx=ctx, out=ho)
+    if dist:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(2, min(args.steps, 5))
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        inversion.tv_admm(hf, hm, grid, bdir, params, ctx=ctx, out=ho)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * e2e_steps / (e2e_ms / 1e3)
+
+    # per-kernel profile (separate pass: every launch bracketed by events on the library stream)
+    ctx.set_profiling(True)
+    ctx.profile_reset()
+    step()
+    prof = ctx.profile()
+    ctx.set_profiling(False)
+    peak, peak_kind = measured_peak()
+    model = kernel_bytes_model(N, 4)
+    kernels = {}
+    for name, (cnt, tot) in prof.items():
+        avg = tot / max(cnt, 1)
+        k = {"launches": cnt, "total_ms": round(tot, 4), "avg_us": round(avg * 1e3, 2)}
+        if name in model:
+            gbs = model[name] / (avg / 1e3) / 1e9
+            k.update({"alg_bytes": model[name], "gbs": round(gbs, 1), "frac": round(gbs / peak, 3)})
+        kernels[name] = k
+    tot_all = sum(v["total_ms"] for v in kernels.values()) or 1.0
+    for v in kernels.values():
+        v["share"] = round(v["total_ms"] / tot_all, 3)
+    dom = max((n for n in kernels if n in model), key=lambda n: kernels[n]["total_ms"])
+    iter_bytes = 20 * N * 4
+    roofline = {"bound": "hbm", "achieved": kernels[dom]["gbs"], "peak": peak, "unit": "GB/s",
+                "frac": round(kernels[dom]["gbs"] / peak, 3), "traffic": None, "kernel": dom,
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
+                "fallback 6.65 TB/s",
+                "iteration_model_gbs": round(iter_bytes / (ms_step / ITERS / 1e3) / 1e9, 1),
+                "iteration_model_frac": round(iter_bytes / (ms_step / ITERS / 1e3) / 1e9 / peak, 3)}
+
+    extra = {}
+    if not args.skip_fp64:
+        ctx64 = qsmgpu.Context(local, "f64")
+        s64 = torch.cuda.ExternalStream(ctx64.stream_handle(), device=dev)
+        d_o64 = torch.empty(N, dtype=torch.float64, device=dev)
+
+        def step64():
+            inversion.tv_admm_device(ctx64, d_f.data_ptr(), d_m.data_ptr(), grid, bdir, params, d_o64.data_ptr())
+
+        step64()
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        k64 = max(2, min(args.steps, 4))
+        a0.record(s64)
+        for _ in range(k64):
+            step64()
+        a1.record(s64)
+        torch.cuda.synchronize()
+        ms64 = a0.elapsed_time(a1) / k64
+        chi64 = d_o64.cpu().numpy()
+        err = float(np.linalg.norm(chi_mixed - chi64) / np.linalg.norm(chi64))
+        extra = {"fp64_plain": {"volumes_per_s": round(1e3 / ms64, 3), "ms_per_iteration": round(ms64 / ITERS, 4)},
+                 "mixed_vs_fp64_speedup": round(ms64 / ms_step, 3),
+                 "rel_l2_mixed_vs_fp64": err, "max_abs_mixed_vs_fp64": float(np.abs(chi_mixed - chi64).max())}
+        ctx64.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu_baseline:
+        cpu = cpu_baseline_tv(f, mask)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": max(args.warmup, 3), "ms_per_step": round(ms_step, 3), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": f"tv_admm {DIMS[0]}x{DIMS[1]}x{DIMS[2]} x{ITERS} iterations "
+                                       "(ellipsoid phantom, B0=z, TvParams default with tol=0)",
+                           "dims": list(DIMS), "iterations": ITERS,
+                           "precision": "mixed: f32 FFTs/stencils, f64 reductions and k-space multipliers",
+                           "l2": "no flush: per-iteration working set ~0.5 GB > 126 MB L2",
+                           "parallelism": f"volumes sharded over {world} rank(s), no collective"},
+                "ms_per_iteration": round(ms_step / ITERS, 4),
+                "roofline": roofline, "kernels": kernels,
+                "e2e": {"value": round(e2e_value, 4), "unit": UNIT, "h2d_bytes_per_step": int(N * 8 + N),
+                        "d2h_bytes_per_step": int(N * 8)},
+                "gpu_launches": int(launches), "clocks": clocks.summary()}
+        line.update(extra)
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -69,9 +69,20 @@ QSM_API int qsm_ctx_get_precision(const qsm_ctx* ctx);
 /* Free cached device workspaces (they are otherwise reused between calls). */
 QSM_API qsm_status qsm_ctx_release_workspace(qsm_ctx* ctx);
 QSM_API const char* qsm_last_error(const qsm_ctx* ctx);
+/* The context's CUDA stream (a cudaStream_t), so callers can order their own work
+ * and timing events with the library's launches. */
+QSM_API void* qsm_ctx_stream(const qsm_ctx* ctx);
 /* Number of kernels this context has launched (cumulative). */
 QSM_API uint64_t qsm_ctx_kernel_launches(const qsm_ctx* ctx);
 QSM_API const char* qsm_version(void);
+/* Per-kernel timing: while on, every launch on this context is bracketed by CUDA
+ * events on its stream (iterative solvers then run without graph capture).  Totals
+ * accumulate per kernel name until qsm_ctx_profile_reset. */
+QSM_API qsm_status qsm_ctx_set_profiling(qsm_ctx* ctx, int on);
+QSM_API qsm_status qsm_ctx_profile_reset(qsm_ctx* ctx);
+QSM_API size_t qsm_ctx_profile_count(qsm_ctx* ctx);
+QSM_API qsm_status qsm_ctx_profile_entry(qsm_ctx* ctx, size_t i, char* name, size_t name_cap, uint64_t* launches,
+                                         double* total_ms);
 /* 1 when every axis length of `grid` has a transform plan (factors 2..13). */
 QSM_API int qsm_grid_supported(const qsm_grid* grid);
 

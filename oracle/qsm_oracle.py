@@ -96,13 +96,29 @@ def fftfreq(n: int, d: float) -> np.ndarray:
     return out
 
 
+_FFT_WORKERS = None
+
+
+def set_fft_workers(n: Optional[int]) -> None:
+    """Use scipy.fft with n threads for the 3D transforms (the reference's Rayon axis
+    passes, src/fft.rs:423-479); None restores single-threaded numpy.  Same DFT."""
+    global _FFT_WORKERS
+    _FFT_WORKERS = n
+
+
 def fft3d(a: np.ndarray) -> np.ndarray:
     """Forward unnormalised 3D C2C FFT (src/fft.rs:97-141, 412)."""
+    if _FFT_WORKERS:
+        import scipy.fft
+        return scipy.fft.fftn(a, workers=_FFT_WORKERS)
     return np.fft.fftn(a)
 
 
 def ifft3d(a: np.ndarray) -> np.ndarray:
     """Inverse 3D C2C FFT with 1/N (src/fft.rs:157-209, 485)."""
+    if _FFT_WORKERS:
+        import scipy.fft
+        return scipy.fft.ifftn(a, workers=_FFT_WORKERS)
     return np.fft.ifftn(a)
 
 

@@ -3,6 +3,7 @@
 #include "internal.h"
 #include "common.cuh"
 
+#include <algorithm>
 #include <cstring>
 
 namespace qsm {
@@ -129,6 +130,40 @@ void d2h(qsm_ctx* ctx, void* dst, const void* src, size_t bytes) {
 }
 void sync(qsm_ctx* ctx) { QSM_CUDA(cudaStreamSynchronize(ctx->stream)); }
 
+void LaunchScope::done() {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) throw QsmError(QSM_ERR_CUDA, std::string("kernel launch (") + name + "): " + cudaGetErrorString(e));
+  ctx->launches++;
+  if (ctx->profiling && ev0) {
+    cudaEvent_t ev1;
+    QSM_CUDA(cudaEventCreate(&ev1));
+    QSM_CUDA(cudaEventRecord(ev1, ctx->stream));
+    ctx->prof_pending.push_back(ProfRec{ctx->prof_prefix + name, ev0, ev1});
+    ev0 = nullptr;
+  }
+}
+
+// Fold pending launch events into per-name totals (synchronises the stream).
+void prof_collect(qsm_ctx* ctx) {
+  if (ctx->prof_pending.empty()) return;
+  QSM_CUDA(cudaStreamSynchronize(ctx->stream));
+  for (ProfRec& r : ctx->prof_pending) {
+    float ms = 0.f;
+    QSM_CUDA(cudaEventElapsedTime(&ms, r.start, r.stop));
+    cudaEventDestroy(r.start);
+    cudaEventDestroy(r.stop);
+    auto it = std::find_if(ctx->prof_stats.begin(), ctx->prof_stats.end(),
+                           [&](const std::pair<std::string, ProfStat>& kv) { return kv.first == r.name; });
+    if (it == ctx->prof_stats.end()) {
+      ctx->prof_stats.push_back({r.name, ProfStat{}});
+      it = ctx->prof_stats.end() - 1;
+    }
+    it->second.launches += 1;
+    it->second.total_ms += ms;
+  }
+  ctx->prof_pending.clear();
+}
+
 }  // namespace qsm
 
 using namespace qsm;
@@ -195,7 +230,44 @@ const char* qsm_last_error(const qsm_ctx* ctx) {
 
 uint64_t qsm_ctx_kernel_launches(const qsm_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+void* qsm_ctx_stream(const qsm_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
 const char* qsm_version(void) { return "qsmgpu 0.1.0 (sm_100a)"; }
+
+qsm_status qsm_ctx_set_profiling(qsm_ctx* ctx, int on) {
+  return guarded(ctx, [&] {
+    prof_collect(ctx);
+    ctx->profiling = on != 0;
+  });
+}
+
+qsm_status qsm_ctx_profile_reset(qsm_ctx* ctx) {
+  return guarded(ctx, [&] {
+    prof_collect(ctx);
+    ctx->prof_stats.clear();
+  });
+}
+
+size_t qsm_ctx_profile_count(qsm_ctx* ctx) {
+  if (!ctx) return 0;
+  if (guarded(ctx, [&] { prof_collect(ctx); }) != QSM_OK) return 0;
+  return ctx->prof_stats.size();
+}
+
+qsm_status qsm_ctx_profile_entry(qsm_ctx* ctx, size_t i, char* name, size_t name_cap, uint64_t* launches,
+                                 double* total_ms) {
+  return guarded(ctx, [&] {
+    prof_collect(ctx);
+    if (i >= ctx->prof_stats.size()) throw QsmError(QSM_ERR_INVALID_ARGUMENT, "profile index out of range");
+    const auto& kv = ctx->prof_stats[i];
+    if (name && name_cap) {
+      std::strncpy(name, kv.first.c_str(), name_cap - 1);
+      name[name_cap - 1] = 0;
+    }
+    if (launches) *launches = kv.second.launches;
+    if (total_ms) *total_ms = kv.second.total_ms;
+  });
+}
 
 int qsm_grid_supported(const qsm_grid* grid) {
   if (grid == nullptr) return 0;

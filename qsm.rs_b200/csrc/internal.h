@@ -38,6 +38,18 @@ struct GraphCache {
   std::string key;
 };
 
+// One timed kernel launch (profiling mode): events recorded around the launch on
+// the context's stream.
+struct ProfRec {
+  std::string name;
+  cudaEvent_t start, stop;
+};
+
+struct ProfStat {
+  uint64_t launches = 0;
+  double total_ms = 0.0;
+};
+
 }  // namespace qsm
 
 struct qsm_ctx {
@@ -51,6 +63,12 @@ struct qsm_ctx {
   std::map<std::string, qsm::GraphCache> graphs;
   uint64_t launches = 0;
   size_t tv_last_iters = 0;
+  // per-kernel CUDA-event profiling (qsm_ctx_set_profiling); iterative solvers run
+  // without graph capture while it is on
+  bool profiling = false;
+  std::string prof_prefix;
+  std::vector<qsm::ProfRec> prof_pending;
+  std::vector<std::pair<std::string, qsm::ProfStat>> prof_stats;
 };
 
 namespace qsm {
@@ -83,6 +101,22 @@ void check_finite(double v, const char* name);
 void h2d(qsm_ctx* ctx, void* dst, const void* src, size_t bytes);
 void d2h(qsm_ctx* ctx, void* dst, const void* src, size_t bytes);
 void sync(qsm_ctx* ctx);
+
+// Profiling scope around one launch: records a start event now and a stop event
+// (plus the launch-error check and launch count) in done().
+struct LaunchScope {
+  qsm_ctx* ctx;
+  const char* name;
+  cudaEvent_t ev0 = nullptr;
+  LaunchScope(qsm_ctx* c, const char* n) : ctx(c), name(n) {
+    if (ctx->profiling) {
+      QSM_CUDA(cudaEventCreate(&ev0));
+      QSM_CUDA(cudaEventRecord(ev0, ctx->stream));
+    }
+  }
+  void done();
+};
+void prof_collect(qsm_ctx* ctx);
 
 // Run fn and convert exceptions into a status + last error string.
 template <class F> qsm_status guarded(qsm_ctx* ctx, F&& fn) {

@@ -334,8 +334,9 @@ void tv_admm_impl(qsm_ctx* ctx, const GridDims& d, const double* d_f, const uint
   const T scale = (T)(1.0 / (double)N);
   const unsigned sgrid = grid1d(N);
   auto one_iter = [&](const T* ui, T* uo) {
+    LaunchScope ls(ctx, "tv_stencil");
     k_tv_stencil<T><<<sgrid, 256, 0, ctx->stream>>>(d.nx, d.ny, d.nz, hx, hy, hz, thr, x, ui, uo, div, done);
-    after_launch(ctx);
+    ls.done();
     run_x_r2c<T>(ctx, f, spec, LoadCast<T, T>{div, d.nx}, done);
     run_yz<T, -1, 1>(ctx, f, spec, spec, OpId<T>{}, done);
     run_z_fused<T>(ctx, f, spec, spec, OpAdmmSolve<T>{K, p.rho, fhat}, done);
@@ -343,6 +344,27 @@ void tv_admm_impl(qsm_ctx* ctx, const GridDims& d, const double* d_f, const uint
     run_x_c2r<T>(ctx, f, spec, StoreTvX<T>{x, d.nx, scale, partials, st, 0.0, 0.0}, done);
   };
 
+  if (ctx->profiling) {
+    // eager launches so that every kernel is timed individually
+    for (size_t it = 0; it < p.max_iter; ++it) {
+      if (it % 2 == 0) one_iter(u0, u1);
+      else one_iter(u1, u0);
+    }
+    TvState hs{};
+    QSM_CUDA(cudaMemcpyAsync(&hs, st, sizeof(TvState), cudaMemcpyDeviceToHost, ctx->stream));
+    {
+      LaunchScope ls(ctx, "mask_out");
+      k_mask_out<T><<<grid1d(N), 256, 0, ctx->stream>>>(N, x, d_mask, d_out);
+      ls.done();
+    }
+    sync(ctx);
+    if (progress) {
+      for (int i = 0; i < hs.iters; ++i) progress(user, (size_t)i + 1, p.max_iter);
+      if (hs.done) progress(user, (size_t)hs.iters, (size_t)hs.iters);
+    }
+    ctx->tv_last_iters = (size_t)hs.iters;
+    return;
+  }
   // Two iterations (u0 -> u1 -> u0) captured as one graph; an odd tail runs eagerly.
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -395,8 +417,11 @@ void tv_admm_impl(qsm_ctx* ctx, const GridDims& d, const double* d_f, const uint
   cudaGraphExecDestroy(exec);
 
   QSM_CUDA(cudaMemcpyAsync(&hs, st, sizeof(TvState), cudaMemcpyDeviceToHost, ctx->stream));
-  k_mask_out<T><<<grid1d(N), 256, 0, ctx->stream>>>(N, x, d_mask, d_out);
-  after_launch(ctx);
+  {
+    LaunchScope ls(ctx, "mask_out");
+    k_mask_out<T><<<grid1d(N), 256, 0, ctx->stream>>>(N, x, d_mask, d_out);
+    ls.done();
+  }
   sync(ctx);
   if (progress) {
     for (; reported < (size_t)hs.iters; ++reported) progress(user, reported + 1, max_iter);

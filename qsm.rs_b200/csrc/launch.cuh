@@ -80,8 +80,9 @@ void run_x_r2c(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* spec, const Load& ld, 
   const size_t smem = (size_t)(f.px.n + P * x_rowlen<T>(f.px.n)) * sizeof(C);
   auto kern = k_x_r2c<T, Load>;
   ensure_smem(kern, smem);
+  LaunchScope ls(ctx, "fft_x_r2c");
   kern<<<(unsigned)x_blocks(f), dim3(Tt, P), smem, ctx->stream>>>(f.g, f.px, f.twx, spec, ld, done);
-  after_launch(ctx);
+  ls.done();
 }
 
 template <typename T, class Store>
@@ -92,8 +93,9 @@ void run_x_c2r(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* spec, const Stor
   const size_t smem = (size_t)(f.px.n + P * x_rowlen<T>(f.px.n)) * sizeof(C);
   auto kern = k_x_c2r<T, Store>;
   ensure_smem(kern, smem);
+  LaunchScope ls(ctx, "fft_x_c2r");
   kern<<<(unsigned)x_blocks(f), dim3(Tt, P), smem, ctx->stream>>>(f.g, f.px, f.twx, spec, st, done);
-  after_launch(ctx);
+  ls.done();
 }
 
 template <typename T> inline int yz_cols() { return sizeof(T) == 4 ? 16 : 8; }
@@ -110,8 +112,9 @@ void run_yz(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst
   auto kern = k_pass_yz<T, DIR, AXIS, Op>;
   ensure_smem(kern, smem);
   dim3 grid((f.g.nxh + P - 1) / P, AXIS == 1 ? f.g.nz : f.g.ny);
+  LaunchScope ls(ctx, AXIS == 1 ? (DIR < 0 ? "fft_y_fwd" : "fft_y_inv") : (DIR < 0 ? "fft_z_fwd" : "fft_z_inv"));
   kern<<<grid, dim3(P, pl.T), smem, ctx->stream>>>(f.g, pl, tw, src, dst, op, done);
-  after_launch(ctx);
+  ls.done();
 }
 
 template <typename T, class Op>
@@ -125,8 +128,9 @@ void run_z_fused(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>
   auto kern = k_z_fused<T, Op>;
   ensure_smem(kern, smem);
   dim3 grid((f.g.nxh + P - 1) / P, f.g.ny);
+  LaunchScope ls(ctx, "fft_z_fused");
   kern<<<grid, dim3(P, pl.T), smem, ctx->stream>>>(f.g, pl, f.twz, src, dst, op, done);
-  after_launch(ctx);
+  ls.done();
 }
 
 // ---------------------------------------------------------------------------

@@ -138,11 +138,34 @@ class Context:
     def kernel_launches(self) -> int:
         return int(self._lib.qsm_ctx_kernel_launches(self._h))
 
+    def stream_handle(self) -> int:
+        """The context's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
+        return int(self._lib.qsm_ctx_stream(self._h) or 0)
+
     def release_workspace(self):
         _check(self, self._lib.qsm_ctx_release_workspace(self._h))
 
     def tv_last_iterations(self) -> int:
         return int(self._lib.qsm_tv_last_iterations(self._h))
+
+    def set_profiling(self, on: bool):
+        """Bracket every kernel launch with CUDA events on the context's stream."""
+        _check(self, self._lib.qsm_ctx_set_profiling(self._h, 1 if on else 0))
+
+    def profile_reset(self):
+        _check(self, self._lib.qsm_ctx_profile_reset(self._h))
+
+    def profile(self) -> dict:
+        """{kernel name: (launches, total_ms)} accumulated since the last reset."""
+        out = {}
+        n = int(self._lib.qsm_ctx_profile_count(self._h))
+        buf = C.create_string_buffer(128)
+        for i in range(n):
+            cnt = C.c_uint64()
+            ms = C.c_double()
+            _check(self, self._lib.qsm_ctx_profile_entry(self._h, i, buf, 128, C.byref(cnt), C.byref(ms)))
+            out[buf.value.decode()] = (int(cnt.value), float(ms.value))
+        return out
 
 
 def _prec_code(p: str) -> int:

@@ -81,7 +81,13 @@ _SIGS = [
     ("qsm_ctx_release_workspace", C.c_int, [C.c_void_p]),
     ("qsm_last_error", C.c_char_p, [C.c_void_p]),
     ("qsm_ctx_kernel_launches", C.c_uint64, [C.c_void_p]),
+    ("qsm_ctx_stream", C.c_void_p, [C.c_void_p]),
     ("qsm_version", C.c_char_p, []),
+    ("qsm_ctx_set_profiling", C.c_int, [C.c_void_p, C.c_int]),
+    ("qsm_ctx_profile_reset", C.c_int, [C.c_void_p]),
+    ("qsm_ctx_profile_count", C.c_size_t, [C.c_void_p]),
+    ("qsm_ctx_profile_entry", C.c_int, [C.c_void_p, C.c_size_t, C.c_char_p, C.c_size_t,
+                                        C.POINTER(C.c_uint64), C.POINTER(C.c_double)]),
     ("qsm_grid_supported", C.c_int, [C.POINTER(QsmGrid)]),
     ("qsm_tv_params_default", None, [C.POINTER(QsmTvParams)]),
     ("qsm_tkd_params_default", None, [C.POINTER(QsmTkdParams)]),

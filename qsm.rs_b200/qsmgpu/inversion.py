@@ -81,18 +81,23 @@ def tikhonov(local_field, mask, grid: Grid, bdir=(0.0, 0.0, 1.0), params: Tikhon
 
 
 def tv_admm(local_field, mask, grid: Grid, bdir=(0.0, 0.0, 1.0), params: TvParams = TvParams(),
-            progress: Optional[Callable[[int, int], None]] = None, *, ctx: Optional[Context] = None):
+            progress: Optional[Callable[[int, int], None]] = None, *, ctx: Optional[Context] = None,
+            out: Optional[np.ndarray] = None):
     """inversion::tv_admm (src/inversion/tv.rs:63-97).
 
     progress(iter, max_iter) is called once per iteration (delivered in batches between
     CUDA-graph launches) and (iters, iters) on convergence, as in the reference.
+    `out` may supply the result buffer (e.g. page-locked host memory).
     """
     c = _ctx(ctx)
     f = _as_f64(local_field, grid, "local_field")
     m = _as_u8(mask, "mask")
     _check_len(f, grid, "local_field")
     _check_len(m, grid, "mask")
-    out = np.empty_like(f)
+    if out is None:
+        out = np.empty_like(f)
+    elif out.dtype != np.float64 or not out.flags.c_contiguous or out.size != f.size:
+        raise ValueError("out must be a contiguous float64 array with one value per voxel")
     b, _keep = _bdir(bdir)
     g = grid._c()
     p = params._c()
