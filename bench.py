@@ -159,12 +159,12 @@ def kernel_bytes_model(N, s):
     """Algorithmic bytes per launch of each TV-ADMM kernel (s = 4 FP32, 8 FP64).
     A half spectrum is counted as N*s bytes."""
     return {
-        "tv_stencil": 8 * N * s,   # read x, u(3); write u(3), div
+        "tv_step": 10 * N * s,     # read x0, y_{i-1}, y_{i-2}, u(3); write u(3), div
         "fft_x_r2c": 2 * N * s,    # read div, write spectrum
         "fft_y_fwd": 2 * N * s,
-        "fft_z_fused": 3 * N * s,  # read spectrum + f_hat, write spectrum
+        "fft_z_fused": 2 * N * s,  # read + write spectrum (multiplier computed in-kernel)
         "fft_y_inv": 2 * N * s,
-        "fft_x_c2r": 3 * N * s,    # read spectrum + x_prev, write x
+        "fft_x_c2r": 2 * N * s,    # read spectrum, write y_i
     }
 
 

@@ -27,26 +27,26 @@ template <typename Tin, typename T> struct LoadMasked {
 // ----------------------------------------------------------------- stores --
 // out[i] = mask[i] != 0 ? v*scale : 0, written as double
 template <typename T> struct StoreMaskedF64 {
-  double* out;
-  const uint8_t* mask;
+  double* __restrict__ out;
+  const uint8_t* __restrict__ mask;
   int nx;
   T scale;
   __device__ __forceinline__ void operator()(int row, int e, T v) {
     const long long i = (long long)row * nx + e;
-    out[i] = mask == nullptr || mask[i] != 0 ? (double)(v * scale) : 0.0;
+    out[i] = mask == nullptr || __ldg(mask + i) != 0 ? (double)(v * scale) : 0.0;
   }
   __device__ __forceinline__ void finish() {}
 };
 
 // out[i] = (mask == null || mask[i] == 1) ? v*scale : 0 in working precision
 template <typename T> struct StoreMaskEqOne {
-  T* out;
-  const uint8_t* mask;
+  T* __restrict__ out;
+  const uint8_t* __restrict__ mask;
   int nx;
   T scale;
   __device__ __forceinline__ void operator()(int row, int e, T v) {
     const long long i = (long long)row * nx + e;
-    out[i] = (mask == nullptr || mask[i] == 1) ? v * scale : T(0);
+    out[i] = (mask == nullptr || __ldg(mask + i) == 1) ? v * scale : T(0);
   }
   __device__ __forceinline__ void finish() {}
 };

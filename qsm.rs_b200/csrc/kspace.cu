@@ -50,8 +50,9 @@ std::vector<double> poisson_axis(int n, double vs) {
   return q;
 }
 
-const double* table(qsm_ctx* ctx, const std::string& key, const std::vector<double>& v) {
-  return (const double*)upload_table(ctx, key, v.data(), v.size() * sizeof(double));
+template <typename S> const S* table(qsm_ctx* ctx, const std::string& key, const std::vector<double>& v) {
+  std::vector<S> h(v.begin(), v.end());
+  return (const S*)upload_table(ctx, key + (sizeof(S) == 4 ? ":f" : ":d"), h.data(), h.size() * sizeof(S));
 }
 
 std::string k(const char* what, int n, double vs) {
@@ -62,17 +63,17 @@ std::string k(const char* what, int n, double vs) {
 
 }  // namespace
 
-KSpace make_kspace(qsm_ctx* ctx, const GridDims& d, const double bdir[3]) {
-  KSpace K;
-  K.fx = table(ctx, k("freq", d.nx, d.vsx), fftfreq(d.nx, d.vsx));
-  K.fy = table(ctx, k("freq", d.ny, d.vsy), fftfreq(d.ny, d.vsy));
-  K.fz = table(ctx, k("freq", d.nz, d.vsz), fftfreq(d.nz, d.vsz));
-  K.lx = table(ctx, k("lap", d.nx, d.vsx), lapneg_axis(d.nx, d.vsx));
-  K.ly = table(ctx, k("lap", d.ny, d.vsy), lapneg_axis(d.ny, d.vsy));
-  K.lz = table(ctx, k("lap", d.nz, d.vsz), lapneg_axis(d.nz, d.vsz));
-  K.qx = table(ctx, k("poi", d.nx, d.vsx), poisson_axis(d.nx, d.vsx));
-  K.qy = table(ctx, k("poi", d.ny, d.vsy), poisson_axis(d.ny, d.vsy));
-  K.qz = table(ctx, k("poi", d.nz, d.vsz), poisson_axis(d.nz, d.vsz));
+template <typename S> KSpaceT<S> make_kspace_t(qsm_ctx* ctx, const GridDims& d, const double bdir[3]) {
+  KSpaceT<S> K;
+  K.fx = table<S>(ctx, k("freq", d.nx, d.vsx), fftfreq(d.nx, d.vsx));
+  K.fy = table<S>(ctx, k("freq", d.ny, d.vsy), fftfreq(d.ny, d.vsy));
+  K.fz = table<S>(ctx, k("freq", d.nz, d.vsz), fftfreq(d.nz, d.vsz));
+  K.lx = table<S>(ctx, k("lap", d.nx, d.vsx), lapneg_axis(d.nx, d.vsx));
+  K.ly = table<S>(ctx, k("lap", d.ny, d.vsy), lapneg_axis(d.ny, d.vsy));
+  K.lz = table<S>(ctx, k("lap", d.nz, d.vsz), lapneg_axis(d.nz, d.vsz));
+  K.qx = table<S>(ctx, k("poi", d.nx, d.vsx), poisson_axis(d.nx, d.vsx));
+  K.qy = table<S>(ctx, k("poi", d.ny, d.vsy), poisson_axis(d.ny, d.vsy));
+  K.qz = table<S>(ctx, k("poi", d.nz, d.vsz), poisson_axis(d.nz, d.vsz));
   K.nyqx = (d.nx % 2 == 0) ? d.nx / 2 : -1;
   K.nyqy = (d.ny % 2 == 0) ? d.ny / 2 : -1;
   K.nyqz = (d.nz % 2 == 0) ? d.nz / 2 : -1;
@@ -84,10 +85,17 @@ KSpace make_kspace(qsm_ctx* ctx, const GridDims& d, const double bdir[3]) {
   }
   // src/kernels/dipole.rs:38-43 normalises b (a zero vector yields NaN there too)
   const double bn = std::sqrt(bx * bx + by * by + bz * bz);
-  K.bx = bx / bn;
-  K.by = by / bn;
-  K.bz = bz / bn;
+  K.bx = (S)(bx / bn);
+  K.by = (S)(by / bn);
+  K.bz = (S)(bz / bn);
   return K;
+}
+
+template KSpaceT<float> make_kspace_t<float>(qsm_ctx*, const GridDims&, const double*);
+template KSpaceT<double> make_kspace_t<double>(qsm_ctx*, const GridDims&, const double*);
+
+KSpace make_kspace(qsm_ctx* ctx, const GridDims& d, const double bdir[3]) {
+  return make_kspace_t<double>(ctx, d, bdir);
 }
 
 }  // namespace qsm

@@ -67,6 +67,10 @@ template <typename T> inline int x_pencils_per_block(int T_) {
 }
 
 template <typename T> inline long long x_blocks(const Fft3<T>& f) {
+  // the X kernels hold a row's elements (<= kFftEmax) and half-spectrum entries
+  // (<= kXHalfMax) per thread in fixed register arrays
+  if ((f.px.n + f.px.T - 1) / f.px.T > kFftEmax || (f.g.nxh + f.px.T - 1) / f.px.T > kXHalfMax)
+    throw QsmError(QSM_ERR_UNSUPPORTED_SIZE, "x length outside the per-thread register budget");
   const int P = x_pencils_per_block<T>(f.px.T);
   const long long npairs = ((long long)f.g.nrows() + 1) / 2;
   return (npairs + P - 1) / P;
@@ -100,36 +104,74 @@ void run_x_c2r(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* spec, const Stor
 
 template <typename T> inline int yz_cols() { return sizeof(T) == 4 ? 16 : 8; }
 
+inline int sm_count(qsm_ctx* ctx) {
+  static int cached[64] = {0};
+  const int d = ctx->device & 63;
+  if (cached[d] == 0) QSM_CUDA(cudaDeviceGetAttribute(&cached[d], cudaDevAttrMultiProcessorCount, ctx->device));
+  return cached[d];
+}
+
+// Persistent grid: as many CTAs as fit on the device at once, capped by the work.
+template <class K> unsigned persistent_grid(qsm_ctx* ctx, K kernel, int threads, size_t smem, long long work) {
+  int per_sm = 0;
+  QSM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
+  if (per_sm < 1) throw QsmError(QSM_ERR_UNSUPPORTED_SIZE, "transform tile does not fit on an SM");
+  long long g = (long long)per_sm * sm_count(ctx);
+  if (g > work) g = work;
+  if (g < 1) g = 1;
+  return (unsigned)g;
+}
+
+template <typename T> TileWalk tile_walk(const Fft3<T>& f, int axis) {
+  const int P = yz_cols<T>();
+  TileWalk w;
+  w.ntx = (f.g.nxh + P - 1) / P;
+  if (axis == 1) {  // Y: outer = z
+    w.ntiles = w.ntx * f.g.nz;
+    w.ostride = (long long)f.g.pitch * f.g.ny;
+    w.estride = f.g.pitch;
+  } else {  // Z: outer = y
+    w.ntiles = w.ntx * f.g.ny;
+    w.ostride = f.g.pitch;
+    w.estride = (long long)f.g.pitch * f.g.ny;
+  }
+  return w;
+}
+
+template <typename T> inline size_t yz_smem(int n) {
+  return (size_t)(((n + 7) & ~7) + 2 * (size_t)n * yz_cols<T>()) * sizeof(cplx_t<T>);
+}
+
 // AXIS 1 = y, 2 = z; DIR -1 forward, +1 inverse.
 template <typename T, int DIR, int AXIS, class Op>
 void run_yz(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst, const Op& op, const int* done) {
-  using C = cplx_t<T>;
   const FftPlan1D& pl = (AXIS == 1) ? f.py : f.pz;
   const cplx_t<T>* tw = (AXIS == 1) ? f.twy : f.twz;
   const int P = yz_cols<T>();
   if (P * pl.T > 1024) throw QsmError(QSM_ERR_UNSUPPORTED_SIZE, "axis too long for one tile");
-  const size_t smem = (size_t)(pl.n + pl.n * P) * sizeof(C);
+  const size_t smem = yz_smem<T>(pl.n);
   auto kern = k_pass_yz<T, DIR, AXIS, Op>;
   ensure_smem(kern, smem);
-  dim3 grid((f.g.nxh + P - 1) / P, AXIS == 1 ? f.g.nz : f.g.ny);
+  const TileWalk w = tile_walk(f, AXIS);
+  const unsigned grid = persistent_grid(ctx, kern, P * pl.T, smem, w.ntiles);
   LaunchScope ls(ctx, AXIS == 1 ? (DIR < 0 ? "fft_y_fwd" : "fft_y_inv") : (DIR < 0 ? "fft_z_fwd" : "fft_z_inv"));
-  kern<<<grid, dim3(P, pl.T), smem, ctx->stream>>>(f.g, pl, tw, src, dst, op, done);
+  kern<<<grid, dim3(P, pl.T), smem, ctx->stream>>>(f.g, pl, w, tw, src, dst, op, done);
   ls.done();
 }
 
 template <typename T, class Op>
 void run_z_fused(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst, const Op& op,
                  const int* done) {
-  using C = cplx_t<T>;
   const FftPlan1D& pl = f.pz;
   const int P = yz_cols<T>();
   if (P * pl.T > 1024) throw QsmError(QSM_ERR_UNSUPPORTED_SIZE, "axis too long for one tile");
-  const size_t smem = (size_t)(pl.n + pl.n * P) * sizeof(C);
+  const size_t smem = yz_smem<T>(pl.n);
   auto kern = k_z_fused<T, Op>;
   ensure_smem(kern, smem);
-  dim3 grid((f.g.nxh + P - 1) / P, f.g.ny);
+  const TileWalk w = tile_walk(f, 2);
+  const unsigned grid = persistent_grid(ctx, kern, P * pl.T, smem, w.ntiles);
   LaunchScope ls(ctx, "fft_z_fused");
-  kern<<<grid, dim3(P, pl.T), smem, ctx->stream>>>(f.g, pl, f.twz, src, dst, op, done);
+  kern<<<grid, dim3(P, pl.T), smem, ctx->stream>>>(f.g, pl, w, f.twz, src, dst, op, done);
   ls.done();
 }
 
@@ -140,26 +182,30 @@ void run_z_fused(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>
 // per-axis terms), the Poisson eigenvalues of the unwrapping solver
 // (src/unwrap/laplacian.rs:91-105), and the normalised B0 direction.
 // ---------------------------------------------------------------------------
-struct KSpace {
-  const double* fx;
-  const double* fy;
-  const double* fz;
-  const double* lx;
-  const double* ly;
-  const double* lz;
-  const double* qx;
-  const double* qy;
-  const double* qz;
+template <typename S> struct KSpaceT {
+  const S* fx;
+  const S* fy;
+  const S* fz;
+  const S* lx;
+  const S* ly;
+  const S* lz;
+  const S* qx;
+  const S* qy;
+  const S* qz;
   int nyqx, nyqy, nyqz;  // index n/2 for even n, else -1
-  double bx, by, bz;
+  S bx, by, bz;
 
-  __device__ __forceinline__ double dipole(double kx, double ky, double kz) const {
-    const double kdb = kx * bx + ky * by + kz * bz;
-    const double k2 = kx * kx + ky * ky + kz * kz;
-    return k2 > 1e-20 ? (1.0 / 3.0) - (kdb * kdb) / k2 : 0.0;
+  __device__ __forceinline__ S dipole(S kx, S ky, S kz) const {
+    const S kdb = kx * bx + ky * by + kz * bz;
+    const S k2 = kx * kx + ky * ky + kz * kz;
+    return k2 > S(1e-20) ? S(1.0 / 3.0) - (kdb * kdb) / k2 : S(0);
   }
-  __device__ __forceinline__ double lapneg(int ix, int iy, int iz) const { return (lx[ix] + ly[iy]) + lz[iz]; }
-  __device__ __forceinline__ double poisson(int ix, int iy, int iz) const { return (qx[ix] + qy[iy]) + qz[iz]; }
+  __device__ __forceinline__ S lapneg(int ix, int iy, int iz) const {
+    return (__ldg(lx + ix) + __ldg(ly + iy)) + __ldg(lz + iz);
+  }
+  __device__ __forceinline__ S poisson(int ix, int iy, int iz) const {
+    return (__ldg(qx + ix) + __ldg(qy + iy)) + __ldg(qz + iz);
+  }
   __device__ __forceinline__ bool on_nyquist(int ix, int iy, int iz) const {
     return ix == nyqx || iy == nyqy || iz == nyqz;
   }
@@ -168,17 +214,19 @@ struct KSpace {
   // input.  M(-k) differs from M(k) only on even-length Nyquist planes, where the
   // mirrored index keeps its frequency -n/2 while the other coordinates flip sign.
   template <class F>
-  __device__ __forceinline__ double sym(int ix, int iy, int iz, const F& m) const {
-    const double kx = fx[ix], ky = fy[iy], kz = fz[iz];
-    double v = m(kx, ky, kz, ix, iy, iz);
+  __device__ __forceinline__ S sym(int ix, int iy, int iz, const F& m) const {
+    const S kx = __ldg(fx + ix), ky = __ldg(fy + iy), kz = __ldg(fz + iz);
+    S v = m(kx, ky, kz, ix, iy, iz);
     if (on_nyquist(ix, iy, iz)) {
-      const double v2 = m(ix == nyqx ? -kx : kx, iy == nyqy ? -ky : ky, iz == nyqz ? -kz : kz, ix, iy, iz);
-      v = 0.5 * (v + v2);
+      const S v2 = m(ix == nyqx ? -kx : kx, iy == nyqy ? -ky : ky, iz == nyqz ? -kz : kz, ix, iy, iz);
+      v = S(0.5) * (v + v2);
     }
     return v;
   }
 };
+using KSpace = KSpaceT<double>;
 
+template <typename S> KSpaceT<S> make_kspace_t(qsm_ctx* ctx, const GridDims& d, const double bdir[3]);
 KSpace make_kspace(qsm_ctx* ctx, const GridDims& d, const double bdir[3]);
 
 }  // namespace qsm

@@ -10,11 +10,13 @@
 //   k_x_r2c   : two real rows per complex pencil (z = a + i b), forward FFT along x,
 //               split into the two half spectra.  A loader functor produces the
 //               real input on the fly (cast from f64, masked, stencil, kernel image).
-//   k_pass_yz : C2C along y or z on a P-column tile (128-byte coalesced rows), with
-//               pre/post pointwise hooks.
-//   k_z_fused : forward z FFT -> pointwise multiplier -> inverse z FFT in one pass.
+//   k_pass_yz : C2C along y or z.  Persistent CTAs walk P-column tiles (128-byte rows);
+//               each tile is staged into shared memory with cp.async, double
+//               buffered so that the next tile's copy overlaps this tile's transform.
+//               Optional pre/post pointwise hooks.
+//   k_z_fused : same tiling; forward z FFT -> pointwise multiplier -> inverse z FFT.
 //   k_x_c2r   : rebuild two Hermitian rows, inverse FFT along x, hand each real
-//               value to a store functor (scale, mask, FP64 reductions, selection).
+//               value to a store functor (scale, mask, selection).
 #pragma once
 
 #include "fft_engine.cuh"
@@ -24,7 +26,7 @@ namespace qsm {
 struct Geom {
   int nx, ny, nz;
   int nxh;    // nx/2 + 1
-  int pitch;  // row pitch of the half spectrum, >= nxh
+  int pitch;  // row pitch of the half spectrum, >= nxh, multiple of 4
   __host__ __device__ long long nvox() const { return (long long)nx * ny * nz; }
   __host__ __device__ long long hsize() const { return (long long)pitch * ny * nz; }
   __host__ __device__ int nrows() const { return ny * nz; }
@@ -36,7 +38,7 @@ template <> struct PadG<double> { static constexpr int G = 8; };
 
 template <typename T> __host__ __device__ inline int x_rowlen(int n) { return n + n / PadG<T>::G + 1; }
 
-// Identity pointwise op: Y/Z passes with it stream global -> registers -> global.
+// Identity pointwise op: Y/Z passes with it go smem -> registers -> global.
 template <typename T> struct OpId {
   using C = cplx_t<T>;
   __device__ __forceinline__ C pre(C v, int, int, int, long long) const { return v; }
@@ -46,9 +48,24 @@ template <typename T> struct OpId {
 template <class Op> struct IsPlainOp { static constexpr bool value = false; };
 template <typename T> struct IsPlainOp<OpId<T>> { static constexpr bool value = true; };
 
+// ------------------------------------------------------------------ cp.async --
+// 16-byte global -> shared copy; when pred is false nothing is read and zeros are
+// written.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool pred) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int nbytes = pred ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(nbytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // ---------------------------------------------------------------------------
 // X forward: real rows -> half spectrum.  blockDim = (Tb, P) with Tb >= plan T
 // (threads t >= T idle, so blocks stay whole warps); P pencils (row pairs).
+// A thread holds at most kFftEmax elements of a row (T >= n/16), so the loader's
+// global reads are issued as one unrolled batch before any is consumed.
 // ---------------------------------------------------------------------------
 template <typename T, class Load>
 __global__ void k_x_r2c(Geom g, const __grid_constant__ FftPlan1D pl, const cplx_t<T>* __restrict__ twg,
@@ -71,11 +88,22 @@ __global__ void k_x_r2c(Geom g, const __grid_constant__ FftPlan1D pl, const cplx
   const bool hasb = b < nrows;
   C* sp = sm + p * rowlen;
   SAPadded<PadG<T>::G> sa;
-  if (active) {
-    for (int e = t; e < n; e += pl.T) {
-      const T va = ld((int)a, e);
-      const T vb = hasb ? ld((int)b, e) : T(0);
-      sp[sa(e)] = mk<C>(va, vb);
+  {
+    T va[kFftEmax], vb[kFftEmax];
+#pragma unroll
+    for (int c = 0; c < kFftEmax; ++c) {
+      const int e = t + c * pl.T;
+      va[c] = T(0);
+      vb[c] = T(0);
+      if (active && e < n) {
+        va[c] = ld((int)a, e);
+        if (hasb) vb[c] = ld((int)b, e);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < kFftEmax; ++c) {
+      const int e = t + c * pl.T;
+      if (active && e < n) sp[sa(e)] = mk<C>(va[c], vb[c]);
     }
   }
   __syncthreads();
@@ -95,7 +123,11 @@ __global__ void k_x_r2c(Geom g, const __grid_constant__ FftPlan1D pl, const cplx
 
 // ---------------------------------------------------------------------------
 // X inverse: half spectrum -> real rows.  blockDim = (Tb, P) as for k_x_r2c.
+// A thread loads at most 9 half-spectrum entries per row (nx/2+1 <= 9T), issued as
+// one batch; the results are handed to the store functor in one unrolled batch.
 // ---------------------------------------------------------------------------
+constexpr int kXHalfMax = 9;
+
 template <typename T, class Store>
 __global__ void k_x_c2r(Geom g, const __grid_constant__ FftPlan1D pl, const cplx_t<T>* __restrict__ twg,
                         const cplx_t<T>* __restrict__ spec, Store st0, const int* __restrict__ done) {
@@ -117,119 +149,184 @@ __global__ void k_x_c2r(Geom g, const __grid_constant__ FftPlan1D pl, const cplx
   const bool hasb = b < nrows;
   C* sp = sm + p * rowlen;
   SAPadded<PadG<T>::G> sa;
-  if (active) {
-    for (int k = t; k < g.nxh; k += pl.T) {
-      C ga = spec[a * g.pitch + k];
-      C gb = hasb ? spec[b * g.pitch + k] : mk<C>(T(0), T(0));
-      const bool selfm = (k == 0) || (2 * k == n);
-      if (selfm) {
-        ga.y = T(0);
-        gb.y = T(0);
+  {
+    C ga[kXHalfMax], gb[kXHalfMax];
+#pragma unroll
+    for (int c = 0; c < kXHalfMax; ++c) {
+      const int k = t + c * pl.T;
+      ga[c] = mk<C>(T(0), T(0));
+      gb[c] = mk<C>(T(0), T(0));
+      if (active && k < g.nxh) {
+        ga[c] = spec[a * g.pitch + k];
+        if (hasb) gb[c] = spec[b * g.pitch + k];
       }
-      sp[sa(k)] = mk<C>(ga.x - gb.y, ga.y + gb.x);
-      if (!selfm) sp[sa(n - k)] = mk<C>(ga.x + gb.y, gb.x - ga.y);
+    }
+#pragma unroll
+    for (int c = 0; c < kXHalfMax; ++c) {
+      const int k = t + c * pl.T;
+      if (active && k < g.nxh) {
+        C xa = ga[c], xb = gb[c];
+        const bool selfm = (k == 0) || (2 * k == n);
+        if (selfm) {
+          xa.y = T(0);
+          xb.y = T(0);
+        }
+        sp[sa(k)] = mk<C>(xa.x - xb.y, xa.y + xb.x);
+        if (!selfm) sp[sa(n - k)] = mk<C>(xa.x + xb.y, xb.x - xa.y);
+      }
     }
   }
   __syncthreads();
   fft_pencil<+1, C, SAPadded<PadG<T>::G>, false, false>(&pl, t, active, sp, sa, tw, nullptr, nullptr, 0, 0);
   Store st = st0;
-  if (active) {
-    for (int e = t; e < n; e += pl.T) {
-      const C v = sp[sa(e)];
-      st((int)a, e, v.x);
-      if (hasb) st((int)b, e, v.y);
+  {
+    C v[kFftEmax];
+#pragma unroll
+    for (int c = 0; c < kFftEmax; ++c) {
+      const int e = t + c * pl.T;
+      if (active && e < n) v[c] = sp[sa(e)];
+    }
+#pragma unroll
+    for (int c = 0; c < kFftEmax; ++c) {
+      const int e = t + c * pl.T;
+      if (active && e < n) {
+        st((int)a, e, v[c].x);
+        if (hasb) st((int)b, e, v[c].y);
+      }
     }
   }
   st.finish();
 }
 
 // ---------------------------------------------------------------------------
-// Y (AXIS=1) or Z (AXIS=2) C2C pass on the half spectrum.  blockDim = (P, T).
-// grid = (ceil(nxh/P), nz) for Y, (ceil(nxh/P), ny) for Z.
-// Op::pre(v, ix, iy, iz, idx) is applied on load and Op::post on store.
+// Tiled Y/Z passes.  A tile is P consecutive x' columns (P*sizeof(C) = 128 bytes) at
+// one outer index, all n elements along the transform axis.  blockDim = (P, T);
+// the grid is persistent (a few CTAs per SM) and walks tiles with stride gridDim.x.
 // ---------------------------------------------------------------------------
-template <typename T, int DIR, int AXIS, class Op>
-__global__ void k_pass_yz(Geom g, const __grid_constant__ FftPlan1D pl, const cplx_t<T>* __restrict__ twg,
-                          const cplx_t<T>* src, cplx_t<T>* dst, Op op, const int* __restrict__ done) {
-  using C = cplx_t<T>;
-  if (done != nullptr && *done) return;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  C* tw = reinterpret_cast<C*>(smraw);
-  const int n = pl.n;
-  C* sm = tw + n;
-  const int P = blockDim.x;
-  const int tid = threadIdx.x + threadIdx.y * blockDim.x;
-  for (int i = tid; i < n; i += blockDim.x * blockDim.y) tw[i] = twg[i];
-  __syncthreads();
-  const int px = threadIdx.x;
-  const int t = threadIdx.y;
-  const int col = blockIdx.x * P + px;
-  const bool active = col < g.nxh;
-  const int outer = blockIdx.y;
-  long long base, estride;
-  if (AXIS == 1) {
-    base = col + (long long)outer * g.pitch * g.ny;
-    estride = g.pitch;
-  } else {
-    base = col + (long long)outer * g.pitch;
-    estride = (long long)g.pitch * g.ny;
-  }
-  C* sp = sm + px;
-  SAStrided sa{P};
-  if constexpr (IsPlainOp<Op>::value) {
-    fft_pencil<DIR, C, SAStrided, true, true>(&pl, t, active, sp, sa, tw, src, dst, base, estride);
-  } else {
-    if (active) {
-      for (int e = t; e < n; e += pl.T) {
-        const long long idx = base + e * estride;
-        const C v = src[idx];
-        sp[sa(e)] = (AXIS == 1) ? op.pre(v, col, e, outer, idx) : op.pre(v, col, outer, e, idx);
-      }
-    }
-    __syncthreads();
-    fft_pencil<DIR, C, SAStrided, false, false>(&pl, t, active, sp, sa, tw, nullptr, nullptr, 0, 0);
-    if (active) {
-      for (int e = t; e < n; e += pl.T) {
-        const long long idx = base + e * estride;
-        const C v = sp[sa(e)];
-        dst[idx] = (AXIS == 1) ? op.post(v, col, e, outer, idx) : op.post(v, col, outer, e, idx);
-      }
-    }
+struct TileWalk {
+  int ntx;        // column tiles along x'
+  int ntiles;     // ntx * nouter
+  long long ostride;  // global stride of the outer index
+  long long estride;  // global stride along the transform axis
+};
+
+template <typename C>
+__device__ __forceinline__ void issue_tile(const C* __restrict__ src, C* buf, const Geom& g, const TileWalk& w,
+                                           int tile, int n, int P) {
+  const int tx = tile % w.ntx;
+  const int outer = tile / w.ntx;
+  const int col0 = tx * P;
+  const long long base = col0 + (long long)outer * w.ostride;
+  constexpr int kPer = 16 / (int)sizeof(C);  // complex values per 16-byte chunk
+  const int chunks = n * 8;                  // 8 chunks of 16 bytes per 128-byte row
+  const int nth = blockDim.x * blockDim.y;
+  for (int c = threadIdx.x + threadIdx.y * blockDim.x; c < chunks; c += nth) {
+    const int e = c >> 3, ch = c & 7;
+    const int col = col0 + ch * kPer;
+    const bool ok = col < g.nxh;
+    const C* gp = src + base + (long long)e * w.estride + (ok ? ch * kPer : 0);
+    cp_async16(buf + e * P + ch * kPer, gp, ok);
   }
 }
 
-// ---------------------------------------------------------------------------
-// Z forward -> Op::mid pointwise -> Z inverse, one pass.  blockDim = (P, T),
-// grid = (ceil(nxh/P), ny).
-// ---------------------------------------------------------------------------
-template <typename T, class Op>
-__global__ void k_z_fused(Geom g, const __grid_constant__ FftPlan1D pl, const cplx_t<T>* __restrict__ twg,
+template <typename T, int DIR, int AXIS, class Op>
+__global__ void k_pass_yz(Geom g, const __grid_constant__ FftPlan1D pl, TileWalk w, const cplx_t<T>* __restrict__ twg,
                           const cplx_t<T>* src, cplx_t<T>* dst, Op op, const int* __restrict__ done) {
   using C = cplx_t<T>;
   if (done != nullptr && *done) return;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* tw = reinterpret_cast<C*>(smraw);
   const int n = pl.n;
-  C* sm = tw + n;
   const int P = blockDim.x;
+  C* buf0 = tw + ((n + 7) & ~7);
+  C* buf1 = buf0 + (size_t)n * P;
   const int tid = threadIdx.x + threadIdx.y * blockDim.x;
   for (int i = tid; i < n; i += blockDim.x * blockDim.y) tw[i] = twg[i];
-  __syncthreads();
   const int px = threadIdx.x;
   const int t = threadIdx.y;
-  const int col = blockIdx.x * P + px;
-  const bool active = col < g.nxh;
-  const int iy = blockIdx.y;
-  const long long base = col + (long long)iy * g.pitch;
-  const long long estride = (long long)g.pitch * g.ny;
-  C* sp = sm + px;
   SAStrided sa{P};
-  fft_pencil<-1, C, SAStrided, true, false>(&pl, t, active, sp, sa, tw, src, nullptr, base, estride);
-  if (active) {
-    for (int e = t; e < n; e += pl.T) sp[sa(e)] = op.mid(sp[sa(e)], col, iy, e, base + e * estride);
+  int tile = blockIdx.x;
+  if (tile < w.ntiles) issue_tile(src, buf0, g, w, tile, n, P);
+  cp_async_commit();
+  for (int it = 0; tile < w.ntiles; tile += gridDim.x, ++it) {
+    C* cur = (it & 1) ? buf1 : buf0;
+    C* nxt = (it & 1) ? buf0 : buf1;
+    const int next = tile + gridDim.x;
+    if (next < w.ntiles) issue_tile(src, nxt, g, w, next, n, P);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    const int tx = tile % w.ntx, outer = tile / w.ntx;
+    const int col = tx * P + px;
+    const bool active = col < g.nxh;
+    const long long base = col + (long long)outer * w.ostride;
+    C* sp = cur + px;
+    if constexpr (IsPlainOp<Op>::value) {
+      fft_pencil<DIR, C, SAStrided, false, true>(&pl, t, active, sp, sa, tw, nullptr, dst, base, w.estride);
+    } else {
+      if (active) {
+        for (int e = t; e < n; e += pl.T) {
+          const long long idx = base + e * w.estride;
+          sp[sa(e)] = (AXIS == 1) ? op.pre(sp[sa(e)], col, e, outer, idx) : op.pre(sp[sa(e)], col, outer, e, idx);
+        }
+      }
+      __syncthreads();
+      fft_pencil<DIR, C, SAStrided, false, false>(&pl, t, active, sp, sa, tw, nullptr, nullptr, 0, 0);
+      if (active) {
+        for (int e = t; e < n; e += pl.T) {
+          const long long idx = base + e * w.estride;
+          const C v = sp[sa(e)];
+          dst[idx] = (AXIS == 1) ? op.post(v, col, e, outer, idx) : op.post(v, col, outer, e, idx);
+        }
+      }
+      __syncthreads();
+    }
   }
-  __syncthreads();
-  fft_pencil<+1, C, SAStrided, false, true>(&pl, t, active, sp, sa, tw, nullptr, dst, base, estride);
+  cp_async_wait<0>();
+}
+
+// Z forward -> Op::mid pointwise -> Z inverse, tiled like k_pass_yz (outer = y).
+template <typename T, class Op>
+__global__ void k_z_fused(Geom g, const __grid_constant__ FftPlan1D pl, TileWalk w, const cplx_t<T>* __restrict__ twg,
+                          const cplx_t<T>* src, cplx_t<T>* dst, Op op, const int* __restrict__ done) {
+  using C = cplx_t<T>;
+  if (done != nullptr && *done) return;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* tw = reinterpret_cast<C*>(smraw);
+  const int n = pl.n;
+  const int P = blockDim.x;
+  C* buf0 = tw + ((n + 7) & ~7);
+  C* buf1 = buf0 + (size_t)n * P;
+  const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+  for (int i = tid; i < n; i += blockDim.x * blockDim.y) tw[i] = twg[i];
+  const int px = threadIdx.x;
+  const int t = threadIdx.y;
+  SAStrided sa{P};
+  int tile = blockIdx.x;
+  if (tile < w.ntiles) issue_tile(src, buf0, g, w, tile, n, P);
+  cp_async_commit();
+  for (int it = 0; tile < w.ntiles; tile += gridDim.x, ++it) {
+    C* cur = (it & 1) ? buf1 : buf0;
+    C* nxt = (it & 1) ? buf0 : buf1;
+    const int next = tile + gridDim.x;
+    if (next < w.ntiles) issue_tile(src, nxt, g, w, next, n, P);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    const int tx = tile % w.ntx, iy = tile / w.ntx;
+    const int col = tx * P + px;
+    const bool active = col < g.nxh;
+    const long long base = col + (long long)iy * w.ostride;
+    C* sp = cur + px;
+    fft_pencil<-1, C, SAStrided, false, false>(&pl, t, active, sp, sa, tw, nullptr, nullptr, 0, 0);
+    if (active) {
+#pragma unroll 4
+      for (int e = t; e < n; e += pl.T) sp[sa(e)] = op.mid(sp[sa(e)], col, iy, e, base + e * w.estride);
+    }
+    __syncthreads();
+    fft_pencil<+1, C, SAStrided, false, true>(&pl, t, active, sp, sa, tw, nullptr, dst, base, w.estride);
+  }
+  cp_async_wait<0>();
 }
 
 }  // namespace qsm

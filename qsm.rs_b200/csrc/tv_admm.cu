@@ -1,0 +1,359 @@
+// TV-ADMM dipole inversion (src/inversion/tv.rs:63-97, src/inversion/admm.rs:76-178).
+//
+// The reference iteration is
+//   div = bdiv(g); x = Re IFFT(f_hat - rho*FFT(div)*inv_a); stop if relchange(x) < tol;
+//   v = grad x + u; z = shrink(v, lambda/rho); u = v - z; g = 2z - v.
+// Because the x-update is linear, x_i = x0 - y_i with x0 = Re IFFT(f_hat) (computed
+// once) and y_i = Re IFFT(rho*inv_a*FFT(div_i)).  One iteration is six kernels:
+//
+//   k_tv_step   : convergence test of the previous iterate (FP64 sums of
+//                 (x_{i-1}-x_{i-2})^2 and x_{i-1}^2, last-block reduction) fused with the
+//                 z/u update and the divergence (reads x0, y, u; writes u', div)
+//   X r2c (div) -> Y fwd -> Z fwd * rho*sym(inv_a) * Z inv -> Y inv -> X c2r (y_i)
+//
+// so the inverse X pass is a plain store.  A device-side state (iteration counter,
+// done flag) lets every kernel of a converged solve return immediately, so two
+// iterations are captured once as a CUDA graph and replayed without host syncs.
+#include "functors.cuh"
+#include "solvers.h"
+
+#include <algorithm>
+
+namespace qsm {
+
+template <typename S> __device__ __forceinline__ S sabs(S x) { return x < S(0) ? -x : x; }
+
+// inv_a = 1/(D^2 + rho*Lneg), 0 where |a| <= 1e-20 (src/inversion/admm.rs:164-168)
+template <typename S>
+__device__ __forceinline__ S admm_inv_a(const KSpaceT<S>& K, S kx, S ky, S kz, int ix, int iy, int iz, S rho) {
+  const S d = K.dipole(kx, ky, kz);
+  const S a = d * d + rho * K.lapneg(ix, iy, iz);
+  return sabs(a) > S(1e-20) ? S(1) / a : S(0);
+}
+
+// x0 = Re IFFT(F(f) * D * inv_a) (admm.rs:169-176), multiplier in double
+template <typename T> struct OpAdmmRhs {
+  using C = cplx_t<T>;
+  KSpace K;
+  double rho;
+  __device__ __forceinline__ C mid(C v, int ix, int iy, int iz, long long) const {
+    const KSpace& k = K;
+    const double r = rho;
+    const double m = K.sym(ix, iy, iz, [&](double kx, double ky, double kz, int a, int b, int c) {
+      return k.dipole(kx, ky, kz) * admm_inv_a<double>(k, kx, ky, kz, a, b, c, r);
+    });
+    return cscale(v, (T)m);
+  }
+};
+
+// per-iteration multiplier rho * sym(inv_a) (admm.rs:105-108), working precision
+template <typename T> struct OpAdmmMul {
+  using C = cplx_t<T>;
+  KSpaceT<T> K;
+  T rho;
+  __device__ __forceinline__ C mid(C v, int ix, int iy, int iz, long long) const {
+    const KSpaceT<T>& k = K;
+    const T r = rho;
+    const T ia = K.sym(ix, iy, iz, [&](T kx, T ky, T kz, int a, int b, int c) {
+      return admm_inv_a<T>(k, kx, ky, kz, a, b, c, r);
+    });
+    return cscale(v, r * ia);
+  }
+};
+
+template <typename T> struct StoreReal {
+  T* __restrict__ out;
+  int nx;
+  T scale;
+  __device__ __forceinline__ void operator()(int row, int e, T v) { out[(long long)row * nx + e] = v * scale; }
+  __device__ __forceinline__ void finish() {}
+};
+
+struct TvState {
+  int done;       // 1 once relative_change < tol
+  int k;          // iteration whose k_tv_step runs next (1-based)
+  unsigned counter;
+  int conv_iter;  // iteration that converged
+  double tol;
+  double rc;      // last relative change
+};
+
+// Convergence test of x_{k-1} (k >= 2) + z/u update + divergence, periodic BC
+// (src/utils/gradient.rs:21-108, src/utils/mod.rs:44-77, src/inversion/admm.rs:117-142).
+// x_j = x0 - y_j.  u is read from ui and written to uo; the backward neighbours' g
+// components are recomputed from x and ui there.
+template <typename T>
+__global__ void k_tv_step(int nx, int ny, int nz, T hx, T hy, T hz, T thr, const T* __restrict__ x0,
+                          const T* __restrict__ ycur, const T* __restrict__ yprev, const T* __restrict__ ui,
+                          T* __restrict__ uo, T* __restrict__ div, double2* __restrict__ partials, TvState* st,
+                          int check_only) {
+  if (st->done) return;
+  const int kiter = st->k;
+  const bool check = kiter >= 2;
+  const long long N = (long long)nx * ny * nz;
+  const long long sy = nx, sz = (long long)nx * ny;
+  double sd = 0.0, sx = 0.0;
+  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < N;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const T xc = x0[idx] - ycur[idx];
+    if (check) {
+      const T xp = x0[idx] - yprev[idx];
+      const double dd = (double)xc - (double)xp;
+      sd += dd * dd;
+      sx += (double)xc * (double)xc;
+    }
+    if (check_only) continue;
+    const int i = (int)(idx % nx);
+    const long long r = idx / nx;
+    const int j = (int)(r % ny);
+    const int k = (int)(r / ny);
+    const long long ip = (i + 1 < nx) ? idx + 1 : idx - (nx - 1);
+    const long long im = (i > 0) ? idx - 1 : idx + (nx - 1);
+    const long long jp = (j + 1 < ny) ? idx + sy : idx - (ny - 1) * sy;
+    const long long jm = (j > 0) ? idx - sy : idx + (ny - 1) * sy;
+    const long long kp = (k + 1 < nz) ? idx + sz : idx - (long long)(nz - 1) * sz;
+    const long long km = (k > 0) ? idx - sz : idx + (long long)(nz - 1) * sz;
+    const T xip = x0[ip] - ycur[ip], xjp = x0[jp] - ycur[jp], xkp = x0[kp] - ycur[kp];
+    const T xim = x0[im] - ycur[im], xjm = x0[jm] - ycur[jm], xkm = x0[km] - ycur[km];
+    const T vx = (xip - xc) * hx + ui[idx];
+    const T vy = (xjp - xc) * hy + ui[N + idx];
+    const T vz = (xkp - xc) * hz + ui[2 * N + idx];
+    const T zx = shrink(vx, thr), zy = shrink(vy, thr), zz = shrink(vz, thr);
+    uo[idx] = vx - zx;
+    uo[N + idx] = vy - zy;
+    uo[2 * N + idx] = vz - zz;
+    const T gx = T(2) * zx - vx, gy = T(2) * zy - vy, gz = T(2) * zz - vz;
+    const T vxm = (xc - xim) * hx + ui[im];
+    const T vym = (xc - xjm) * hy + ui[N + jm];
+    const T vzm = (xc - xkm) * hz + ui[2 * N + km];
+    const T gxm = T(2) * shrink(vxm, thr) - vxm;
+    const T gym = T(2) * shrink(vym, thr) - vym;
+    const T gzm = T(2) * shrink(vzm, thr) - vzm;
+    div[idx] = (gx - gxm) * hx + (gy - gym) * hy + (gz - gzm) * hz;
+  }
+  // deterministic two-level reduction: per-block partials, summed in a fixed order
+  // by the block that arrives last
+  __shared__ int am_last;
+  double a = sd, b = sx;
+  block_sum2(a, b);
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    partials[blockIdx.x] = make_double2(a, b);
+    __threadfence();
+    const unsigned prev = atomicAdd(&st->counter, 1u);
+    am_last = (prev == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (am_last) {
+    __threadfence();
+    double pa = 0.0, pb = 0.0;
+    for (int i = tid; i < (int)gridDim.x; i += blockDim.x) {
+      const double2 p = __ldcg(&partials[i]);
+      pa += p.x;
+      pb += p.y;
+    }
+    block_sum2(pa, pb);
+    if (tid == 0) {
+      if (check) {
+        const double rc = sqrt(pa) / (sqrt(pb) + 1e-20);  // src/utils/mod.rs:69-77
+        st->rc = rc;
+        if (rc < st->tol) {
+          st->done = 1;
+          st->conv_iter = kiter - 1;
+        }
+      }
+      st->k = kiter + 1;
+      st->counter = 0u;
+    }
+  }
+}
+
+template <typename T>
+__global__ void k_tv_out(long long N, const T* __restrict__ x0, const T* __restrict__ y,
+                         const uint8_t* __restrict__ mask, double* __restrict__ out) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
+    out[i] = mask[i] != 0 ? (double)(x0[i] - y[i]) : 0.0;  // apply_mask_zero, src/utils/mask.rs:47-53
+}
+
+template <typename T>
+void tv_admm_impl(qsm_ctx* ctx, const GridDims& d, const double* d_f, const uint8_t* d_mask, const double bdir[3],
+                  const qsm_tv_params& p, qsm_progress_fn progress, void* user, double* d_out) {
+  using C = cplx_t<T>;
+  Fft3<T> f = make_fft3<T>(ctx, d);
+  KSpace K64 = make_kspace(ctx, d, bdir);
+  KSpaceT<T> KT = make_kspace_t<T>(ctx, d, bdir);
+  const long long N = d.n;
+  const long long H = f.g.hsize();
+  const char* pre = sizeof(T) == 4 ? "tv32." : "tv64.";
+  auto nm = [&](const char* s) { return std::string(pre) + s; };
+  T* x0 = ws<T>(ctx, nm("x0"), (size_t)N);
+  T* yb[2] = {ws<T>(ctx, nm("y0"), (size_t)N), ws<T>(ctx, nm("y1"), (size_t)N)};
+  T* ub[2] = {ws<T>(ctx, nm("u0"), (size_t)(3 * N)), ws<T>(ctx, nm("u1"), (size_t)(3 * N))};
+  T* div = ws<T>(ctx, nm("div"), (size_t)N);
+  C* spec = ws<C>(ctx, nm("spec"), (size_t)H);
+  const unsigned sgrid = grid1d(N);
+  double2* partials = ws<double2>(ctx, nm("partials"), sgrid);
+  TvState* st = ws<TvState>(ctx, nm("state"), 1);
+  const int* done = &st->done;
+  const T scale = (T)(1.0 / (double)N);
+
+  // x0 = Re IFFT(F(f) * sym(D * inv_a)); x_0 = 0 means y_0 = x0
+  run_x_r2c<T>(ctx, f, spec, LoadCast<double, T>{d_f, d.nx}, nullptr);
+  run_yz<T, -1, 1>(ctx, f, spec, spec, OpId<T>{}, nullptr);
+  run_z_fused<T>(ctx, f, spec, spec, OpAdmmRhs<T>{K64, p.rho}, nullptr);
+  run_yz<T, +1, 1>(ctx, f, spec, spec, OpId<T>{}, nullptr);
+  run_x_c2r<T>(ctx, f, spec, StoreReal<T>{x0, d.nx, scale}, nullptr);
+  QSM_CUDA(cudaMemcpyAsync(yb[0], x0, sizeof(T) * N, cudaMemcpyDeviceToDevice, ctx->stream));
+  QSM_CUDA(cudaMemsetAsync(ub[0], 0, sizeof(T) * 3 * N, ctx->stream));
+  TvState init{};
+  init.k = 1;
+  init.tol = p.tol;
+  QSM_CUDA(cudaMemcpyAsync(st, &init, sizeof(TvState), cudaMemcpyHostToDevice, ctx->stream));
+
+  const T hx = (T)(1.0 / d.vsx), hy = (T)(1.0 / d.vsy), hz = (T)(1.0 / d.vsz);
+  const T thr = (T)(p.lambda / p.rho);
+  const OpAdmmMul<T> mul{KT, (T)p.rho};
+  // iteration i with parity q = i % 2: reads y_{i-1} = yb[1-q], y_{i-2} = yb[q],
+  // u = ub[1-q]; writes u' = ub[q], y_i = yb[q]
+  auto step = [&](int q, int check_only) {
+    LaunchScope ls(ctx, "tv_step");
+    k_tv_step<T><<<sgrid, 256, 0, ctx->stream>>>(d.nx, d.ny, d.nz, hx, hy, hz, thr, x0, yb[1 - q], yb[q], ub[1 - q],
+                                                 ub[q], div, partials, st, check_only);
+    ls.done();
+  };
+  auto one_iter = [&](int q) {
+    step(q, 0);
+    run_x_r2c<T>(ctx, f, spec, LoadCast<T, T>{div, d.nx}, done);
+    run_yz<T, -1, 1>(ctx, f, spec, spec, OpId<T>{}, done);
+    run_z_fused<T>(ctx, f, spec, spec, mul, done);
+    run_yz<T, +1, 1>(ctx, f, spec, spec, OpId<T>{}, done);
+    run_x_c2r<T>(ctx, f, spec, StoreReal<T>{yb[q], d.nx, scale}, done);
+  };
+
+  const size_t max_iter = p.max_iter;
+  const bool watch = (progress != nullptr) || (p.tol > 0.0);
+  TvState hs{};
+  size_t reported = 0;
+  auto poll = [&]() {
+    QSM_CUDA(cudaMemcpyAsync(&hs, st, sizeof(TvState), cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);
+    const size_t completed = hs.done ? (size_t)hs.conv_iter : (size_t)(hs.k - 1);
+    if (progress)
+      for (; reported < completed; ++reported) progress(user, reported + 1, max_iter);
+    return hs.done != 0;
+  };
+
+  bool converged = false;
+  if (ctx->profiling || max_iter < 2) {
+    // eager launches (per-kernel timing, or too short to be worth a graph)
+    for (size_t it = 1; it <= max_iter && !converged; ++it) {
+      one_iter((int)(it % 2));
+      if (watch && (it % 16 == 0)) converged = poll();
+    }
+  } else {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    const uint64_t l0 = ctx->launches;
+    QSM_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      one_iter(1);
+      one_iter(0);
+    } catch (...) {
+      cudaStreamEndCapture(ctx->stream, &graph);
+      if (graph) cudaGraphDestroy(graph);
+      throw;
+    }
+    QSM_CUDA(cudaStreamEndCapture(ctx->stream, &graph));
+    const uint64_t per_pair = ctx->launches - l0;
+    ctx->launches = l0;
+    cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) throw QsmError(QSM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+    const size_t pairs = max_iter / 2;
+    const size_t chunk = 8;  // graph launches (16 iterations) between host polls when watching
+    try {
+      size_t launched = 0;
+      while (launched < pairs && !converged) {
+        const size_t todo = watch ? std::min(chunk, pairs - launched) : (pairs - launched);
+        for (size_t c = 0; c < todo; ++c) {
+          QSM_CUDA(cudaGraphLaunch(exec, ctx->stream));
+          ctx->launches += per_pair;
+        }
+        launched += todo;
+        if (watch) converged = poll();
+      }
+      if (!converged && (max_iter % 2 == 1)) one_iter(1);
+    } catch (...) {
+      cudaGraphExecDestroy(exec);
+      throw;
+    }
+    cudaGraphExecDestroy(exec);
+  }
+  converged = poll();
+  size_t completed = converged ? (size_t)hs.conv_iter : max_iter;
+  if (!converged && max_iter >= 1 && p.tol > 0.0) {
+    // the reference also tests the last iterate (tv.rs:85-91)
+    step((int)((max_iter + 1) % 2), 1);
+    converged = poll();
+    completed = max_iter;
+  }
+  {
+    LaunchScope ls(ctx, "tv_out");
+    k_tv_out<T><<<grid1d(N), 256, 0, ctx->stream>>>(N, x0, yb[completed % 2], d_mask, d_out);
+    ls.done();
+  }
+  sync(ctx);
+  if (progress) {
+    for (; reported < completed; ++reported) progress(user, reported + 1, max_iter);
+    if (converged) progress(user, completed, completed);
+  }
+  ctx->tv_last_iters = completed;
+}
+
+void tv_device(qsm_ctx* ctx, const double* f, const uint8_t* m, const qsm_grid* grid, const double bdir[3],
+               const qsm_tv_params* p, qsm_progress_fn progress, void* user, double* out) {
+  GridDims d = check_grid(grid);
+  check_ptr(f, "local_field");
+  check_ptr(m, "mask");
+  check_ptr(out, "out");
+  check_ptr(p, "params");
+  check_bdir(bdir);
+  check_finite(p->lambda, "lambda");
+  check_finite(p->rho, "rho");
+  if (std::isnan(p->tol)) throw QsmError(QSM_ERR_INVALID_ARGUMENT, "tol is NaN");
+  if (ctx->precision == QSM_PRECISION_MIXED) tv_admm_impl<float>(ctx, d, f, m, bdir, *p, progress, user, out);
+  else tv_admm_impl<double>(ctx, d, f, m, bdir, *p, progress, user, out);
+}
+
+}  // namespace qsm
+
+using namespace qsm;
+
+extern "C" {
+
+qsm_status qsm_tv_admm_device(qsm_ctx* ctx, const double* d_local_field, const uint8_t* d_mask, const qsm_grid* grid,
+                              const double bdir[3], const qsm_tv_params* params, qsm_progress_fn progress, void* user,
+                              double* d_out_chi) {
+  return guarded(ctx, [&] {
+    tv_device(ctx, d_local_field, d_mask, grid, bdir, params, progress, user, d_out_chi);
+    sync(ctx);
+  });
+}
+
+qsm_status qsm_tv_admm(qsm_ctx* ctx, const double* local_field, const uint8_t* mask, const qsm_grid* grid,
+                       const double bdir[3], const qsm_tv_params* params, qsm_progress_fn progress, void* user,
+                       double* out_chi) {
+  return guarded(ctx, [&] {
+    GridDims d = check_grid(grid);
+    check_ptr(local_field, "local_field");
+    check_ptr(mask, "mask");
+    check_ptr(out_chi, "out_chi");
+    with_host_io(ctx, d.n, local_field, mask, out_chi, [&](const double* f, const uint8_t* m, double* o) {
+      tv_device(ctx, f, m, grid, bdir, params, progress, user, o);
+    });
+  });
+}
+
+size_t qsm_tv_last_iterations(const qsm_ctx* ctx) { return ctx ? ctx->tv_last_iters : 0; }
+
+}  // extern "C"
