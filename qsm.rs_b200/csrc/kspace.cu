@@ -2,6 +2,8 @@
 #include "launch.cuh"
 
 #include <cmath>
+#include <map>
+#include <mutex>
 
 namespace qsm {
 
@@ -93,6 +95,15 @@ template <typename S> KSpaceT<S> make_kspace_t(qsm_ctx* ctx, const GridDims& d, 
 
 template KSpaceT<float> make_kspace_t<float>(qsm_ctx*, const GridDims&, const double*);
 template KSpaceT<double> make_kspace_t<double>(qsm_ctx*, const GridDims&, const double*);
+
+size_t& smem_limit_slot(const void* func, int device) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> limits;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = limits.find({func, device});
+  if (it == limits.end()) it = limits.emplace(std::make_pair(func, device), (size_t)48 * 1024).first;
+  return it->second;
+}
 
 KSpace make_kspace(qsm_ctx* ctx, const GridDims& d, const double bdir[3]) {
   return make_kspace_t<double>(ctx, d, bdir);

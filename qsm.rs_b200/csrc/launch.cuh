@@ -34,9 +34,14 @@ template <typename T> Fft3<T> make_fft3(qsm_ctx* ctx, const GridDims& d) {
   return f;
 }
 
+// Raise a kernel's dynamic shared-memory limit when a launch needs more than the
+// default 48 KB (tracked per kernel function and device).
+size_t& smem_limit_slot(const void* func, int device);
 template <class K> void ensure_smem(K kernel, size_t bytes) {
   if (bytes > 227u * 1024u) throw QsmError(QSM_ERR_UNSUPPORTED_SIZE, "transform tile exceeds shared memory");
-  static size_t done = 48u * 1024u;  // one per kernel instantiation
+  int dev = 0;
+  QSM_CUDA(cudaGetDevice(&dev));
+  size_t& done = smem_limit_slot(reinterpret_cast<const void*>(kernel), dev);
   if (bytes > done) {
     QSM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
     done = bytes;

@@ -37,7 +37,7 @@ def rnd(grid, seed=0):
 
 # ---------------------------------------------------------------- transforms --
 FFT_SIZES = [(8, 6, 10), (16, 16, 16), (15, 9, 25), (64, 64, 64), (1, 7, 13), (22, 12, 11), (96, 100, 27),
-             (176, 4, 6), (256, 2, 3), (384, 3, 2), (2, 2, 2)]
+             (176, 4, 6), (256, 2, 3), (384, 3, 2), (2, 2, 2), (4, 256, 2), (2, 4, 256), (6, 5, 384)]
 
 
 @pytest.mark.parametrize("dims", FFT_SIZES)
@@ -49,7 +49,7 @@ def test_fft3d_real_matches_numpy_f64(ctx64, dims):
     assert np.linalg.norm(got - np.fft.fftn(x)) / np.linalg.norm(np.fft.fftn(x)) < 1e-12
 
 
-@pytest.mark.parametrize("dims", [(8, 6, 10), (64, 64, 64), (15, 9, 25), (176, 4, 6)])
+@pytest.mark.parametrize("dims", [(8, 6, 10), (64, 64, 64), (15, 9, 25), (176, 4, 6), (4, 256, 2), (2, 4, 256), (512, 2, 2)])
 def test_fft3d_real_matches_numpy_mixed(ctx32, dims):
     grid = Grid.new(*dims)
     x = rnd(grid, 2)
