@@ -82,72 +82,108 @@ struct TvState {
 // (src/utils/gradient.rs:21-108, src/utils/mod.rs:44-77, src/inversion/admm.rs:117-142).
 // x_j = x0 - y_j.  u is read from ui and written to uo; the backward neighbours' g
 // components are recomputed from x and ui there.
+//
+// blockDim = (32, 8): a warp spans 32 consecutive x, so x-neighbours come from
+// shuffles; each thread marches through `zchunk` planes keeping x at k-1, k, k+1 and
+// u_z at k-1 in registers.  grid = (ceil(nx/32), ceil(ny/8), ceil(nz/zchunk)).
+constexpr int kStepBX = 32, kStepBY = 8;
+
 template <typename T>
-__global__ void k_tv_step(int nx, int ny, int nz, T hx, T hy, T hz, T thr, const T* __restrict__ x0,
-                          const T* __restrict__ ycur, const T* __restrict__ yprev, const T* __restrict__ ui,
-                          T* __restrict__ uo, T* __restrict__ div, double2* __restrict__ partials, TvState* st,
-                          int check_only) {
+__global__ void __launch_bounds__(kStepBX* kStepBY)
+    k_tv_step(int nx, int ny, int nz, int zchunk, T hx, T hy, T hz, T thr, const T* __restrict__ x0,
+              const T* __restrict__ ycur, const T* __restrict__ yprev, const T* __restrict__ ui, T* __restrict__ uo,
+              T* __restrict__ div, double2* __restrict__ partials, TvState* st, int check_only) {
   if (st->done) return;
   const int kiter = st->k;
   const bool check = kiter >= 2;
   const long long N = (long long)nx * ny * nz;
-  const long long sy = nx, sz = (long long)nx * ny;
+  const long long sz = (long long)nx * ny;
+  const int lane = threadIdx.x;
+  const int i0 = blockIdx.x * kStepBX + lane;
+  const int j0 = blockIdx.y * kStepBY + threadIdx.y;
+  const bool in = i0 < nx && j0 < ny;
+  const int i = i0 < nx ? i0 : nx - 1;  // clamped for the shuffle partners
+  const int j = j0 < ny ? j0 : ny - 1;
+  const int ip = i + 1 < nx ? i + 1 : 0, im = i > 0 ? i - 1 : nx - 1;
+  const int jp = j + 1 < ny ? j + 1 : 0, jm = j > 0 ? j - 1 : ny - 1;
+  const int k0 = blockIdx.z * zchunk;
+  const int k1 = k0 + zchunk < nz ? k0 + zchunk : nz;
+  // x-neighbours through shuffles when the partner lane holds them
+  const bool shf_p = (lane < 31) && (i + 1 < nx) && (i0 < nx);
+  const bool shf_m = (lane > 0) && (i > 0) && (i0 < nx);
+  auto X = [&](long long q) -> T { return x0[q] - ycur[q]; };
+  const long long rowj = (long long)j * nx;
+  const int kmm = k0 > 0 ? k0 - 1 : nz - 1;
+  T x_km = X(kmm * sz + rowj + i);
+  T uz_km = check_only ? T(0) : ui[2 * N + kmm * sz + rowj + i];
+  T x_k = X(k0 * sz + rowj + i);
   double sd = 0.0, sx = 0.0;
-  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < N;
-       idx += (long long)gridDim.x * blockDim.x) {
-    const T xc = x0[idx] - ycur[idx];
-    if (check) {
-      const T xp = x0[idx] - yprev[idx];
-      const double dd = (double)xc - (double)xp;
+  for (int k = k0; k < k1; ++k) {
+    const int kp = k + 1 < nz ? k + 1 : 0;
+    const long long base = k * sz;
+    const long long c = base + rowj + i;
+    const T x_kp = X(kp * sz + rowj + i);
+    if (check && in) {
+      const T xp = x0[c] - yprev[c];
+      const double dd = (double)x_k - (double)xp;
       sd += dd * dd;
-      sx += (double)xc * (double)xc;
+      sx += (double)x_k * (double)x_k;
     }
-    if (check_only) continue;
-    const int i = (int)(idx % nx);
-    const long long r = idx / nx;
-    const int j = (int)(r % ny);
-    const int k = (int)(r / ny);
-    const long long ip = (i + 1 < nx) ? idx + 1 : idx - (nx - 1);
-    const long long im = (i > 0) ? idx - 1 : idx + (nx - 1);
-    const long long jp = (j + 1 < ny) ? idx + sy : idx - (ny - 1) * sy;
-    const long long jm = (j > 0) ? idx - sy : idx + (ny - 1) * sy;
-    const long long kp = (k + 1 < nz) ? idx + sz : idx - (long long)(nz - 1) * sz;
-    const long long km = (k > 0) ? idx - sz : idx + (long long)(nz - 1) * sz;
-    const T xip = x0[ip] - ycur[ip], xjp = x0[jp] - ycur[jp], xkp = x0[kp] - ycur[kp];
-    const T xim = x0[im] - ycur[im], xjm = x0[jm] - ycur[jm], xkm = x0[km] - ycur[km];
-    const T vx = (xip - xc) * hx + ui[idx];
-    const T vy = (xjp - xc) * hy + ui[N + idx];
-    const T vz = (xkp - xc) * hz + ui[2 * N + idx];
-    const T zx = shrink(vx, thr), zy = shrink(vy, thr), zz = shrink(vz, thr);
-    uo[idx] = vx - zx;
-    uo[N + idx] = vy - zy;
-    uo[2 * N + idx] = vz - zz;
-    const T gx = T(2) * zx - vx, gy = T(2) * zy - vy, gz = T(2) * zz - vz;
-    const T vxm = (xc - xim) * hx + ui[im];
-    const T vym = (xc - xjm) * hy + ui[N + jm];
-    const T vzm = (xc - xkm) * hz + ui[2 * N + km];
-    const T gxm = T(2) * shrink(vxm, thr) - vxm;
-    const T gym = T(2) * shrink(vym, thr) - vym;
-    const T gzm = T(2) * shrink(vzm, thr) - vzm;
-    div[idx] = (gx - gxm) * hx + (gy - gym) * hy + (gz - gzm) * hz;
+    if (!check_only) {
+      const T ux = ui[c], uy = ui[N + c], uz = ui[2 * N + c];
+      T xip = __shfl_down_sync(0xffffffffu, x_k, 1);
+      T xim = __shfl_up_sync(0xffffffffu, x_k, 1);
+      T uxm = __shfl_up_sync(0xffffffffu, ux, 1);
+      if (!shf_p) xip = X(base + rowj + ip);
+      if (!shf_m) {
+        xim = X(base + rowj + im);
+        uxm = ui[base + rowj + im];
+      }
+      const T xjp = X(base + (long long)jp * nx + i);
+      const long long cjm = base + (long long)jm * nx + i;
+      const T xjm = X(cjm);
+      const T uym = ui[N + cjm];
+      const T vx = (xip - x_k) * hx + ux;
+      const T vy = (xjp - x_k) * hy + uy;
+      const T vz = (x_kp - x_k) * hz + uz;
+      const T zx = shrink(vx, thr), zy = shrink(vy, thr), zz = shrink(vz, thr);
+      const T gx = T(2) * zx - vx, gy = T(2) * zy - vy, gz = T(2) * zz - vz;
+      const T vxm = (x_k - xim) * hx + uxm;
+      const T vym = (x_k - xjm) * hy + uym;
+      const T vzm = (x_k - x_km) * hz + uz_km;
+      const T gxm = T(2) * shrink(vxm, thr) - vxm;
+      const T gym = T(2) * shrink(vym, thr) - vym;
+      const T gzm = T(2) * shrink(vzm, thr) - vzm;
+      if (in) {
+        uo[c] = vx - zx;
+        uo[N + c] = vy - zy;
+        uo[2 * N + c] = vz - zz;
+        div[c] = (gx - gxm) * hx + (gy - gym) * hy + (gz - gzm) * hz;
+      }
+      uz_km = uz;
+    }
+    x_km = x_k;
+    x_k = x_kp;
   }
   // deterministic two-level reduction: per-block partials, summed in a fixed order
   // by the block that arrives last
   __shared__ int am_last;
   double a = sd, b = sx;
   block_sum2(a, b);
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x + kStepBX * threadIdx.y;
+  const int nblocks = gridDim.x * gridDim.y * gridDim.z;
+  const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
   if (tid == 0) {
-    partials[blockIdx.x] = make_double2(a, b);
+    partials[bid] = make_double2(a, b);
     __threadfence();
     const unsigned prev = atomicAdd(&st->counter, 1u);
-    am_last = (prev == gridDim.x - 1);
+    am_last = (prev == (unsigned)nblocks - 1);
   }
   __syncthreads();
   if (am_last) {
     __threadfence();
     double pa = 0.0, pb = 0.0;
-    for (int i = tid; i < (int)gridDim.x; i += blockDim.x) {
+    for (int i = tid; i < nblocks; i += kStepBX * kStepBY) {
       const double2 p = __ldcg(&partials[i]);
       pa += p.x;
       pb += p.y;
@@ -191,8 +227,12 @@ void tv_admm_impl(qsm_ctx* ctx, const GridDims& d, const double* d_f, const uint
   T* ub[2] = {ws<T>(ctx, nm("u0"), (size_t)(3 * N)), ws<T>(ctx, nm("u1"), (size_t)(3 * N))};
   T* div = ws<T>(ctx, nm("div"), (size_t)N);
   C* spec = ws<C>(ctx, nm("spec"), (size_t)H);
-  const unsigned sgrid = grid1d(N);
-  double2* partials = ws<double2>(ctx, nm("partials"), sgrid);
+  // stencil grid: 32x8 columns per block, z split into chunks so that ~3000 blocks run
+  const int gbx = (d.nx + kStepBX - 1) / kStepBX, gby = (d.ny + kStepBY - 1) / kStepBY;
+  int zchunk = (int)std::max<long long>(2, (long long)d.nz * gbx * gby / 3000);
+  if (zchunk > d.nz) zchunk = d.nz;
+  const dim3 sgrid(gbx, gby, (d.nz + zchunk - 1) / zchunk);
+  double2* partials = ws<double2>(ctx, nm("partials"), (size_t)sgrid.x * sgrid.y * sgrid.z);
   TvState* st = ws<TvState>(ctx, nm("state"), 1);
   const int* done = &st->done;
   const T scale = (T)(1.0 / (double)N);
@@ -217,7 +257,8 @@ void tv_admm_impl(qsm_ctx* ctx, const GridDims& d, const double* d_f, const uint
   // u = ub[1-q]; writes u' = ub[q], y_i = yb[q]
   auto step = [&](int q, int check_only) {
     LaunchScope ls(ctx, "tv_step");
-    k_tv_step<T><<<sgrid, 256, 0, ctx->stream>>>(d.nx, d.ny, d.nz, hx, hy, hz, thr, x0, yb[1 - q], yb[q], ub[1 - q],
+    k_tv_step<T><<<sgrid, dim3(kStepBX, kStepBY), 0, ctx->stream>>>(d.nx, d.ny, d.nz, zchunk, hx, hy, hz, thr, x0,
+                                                                    yb[1 - q], yb[q], ub[1 - q],
                                                  ub[q], div, partials, st, check_only);
     ls.done();
   };
