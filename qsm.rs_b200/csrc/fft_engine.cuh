@@ -220,6 +220,86 @@ __device__ __forceinline__ void fft_stage(C (&v)[EMAX], const FftPlan1D& pl, int
   __syncthreads();
 }
 
+// The same Stockham stage with every size known at compile time (radix R, span NS,
+// length N, threads per pencil TT): loop bounds, guards, j mod NS and the twiddle
+// strides fold into constants.  Used for the axis lengths of the benchmark volumes.
+template <int R, int NS, int N, int TT, int DIR, bool FIRST, bool LAST, typename C, class SA, class Fetch,
+          class Emit>
+__device__ __forceinline__ void fft_stage_fixed(C (&v)[kFftEmax], int t, bool active, C* sp, const SA& sa,
+                                                const C* tw, Fetch& fetch, Emit& emit) {
+  constexpr int NB = N / R;
+  constexpr int CM = (NB + TT - 1) / TT;
+  constexpr int TWS = N / (NS * R);
+  static_assert(CM * R <= kFftEmax, "stage does not fit the register budget");
+  if (active) {
+#pragma unroll
+    for (int c = 0; c < CM; ++c) {
+      const int j = t + c * TT;
+      if ((NB % TT == 0) || j < NB) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          if constexpr (FIRST) v[c * R + r] = fetch(j + r * NB);
+          else v[c * R + r] = sp[sa(j + r * NB)];
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (active) {
+#pragma unroll
+    for (int c = 0; c < CM; ++c) {
+      const int j = t + c * TT;
+      if ((NB % TT == 0) || j < NB) {
+        const int k = j % NS;
+        if constexpr (NS > 1) {
+#pragma unroll
+          for (int r = 1; r < R; ++r) {
+            const C w = tw[k * r * TWS];
+            v[c * R + r] = (DIR < 0) ? cmul(v[c * R + r], w) : cmulc(v[c * R + r], w);
+          }
+        }
+        Dft<R, DIR, C>::run(&v[c * R]);
+        const int base = (j - k) * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int e = base + r * NS;
+          if constexpr (LAST) emit(e, v[c * R + r]);
+          else sp[sa(e)] = v[c * R + r];
+        }
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// A compile-time plan: length N, TT threads per pencil, radices R0, R1[, R2].
+template <int N, int TT, int R0, int R1, int R2 = 1> struct FixedPlan {
+  static constexpr int n = N, T = TT;
+  static __host__ __device__ constexpr bool matches(const FftPlan1D& pl) {
+    return pl.n == N && pl.T == TT && pl.radix[0] == R0 && pl.radix[1] == R1 &&
+           (R2 == 1 ? pl.nstages == 2 : (pl.nstages == 3 && pl.radix[2] == R2));
+  }
+  template <int DIR, typename C, class SA, class Fetch, class Emit>
+  static __device__ __forceinline__ void run(int t, bool active, C* sp, const SA& sa, const C* tw, Fetch& fetch,
+                                             Emit& emit) {
+    C v[kFftEmax];
+    if constexpr (R2 == 1) {
+      fft_stage_fixed<R0, 1, N, TT, DIR, true, false>(v, t, active, sp, sa, tw, fetch, emit);
+      fft_stage_fixed<R1, R0, N, TT, DIR, false, true>(v, t, active, sp, sa, tw, fetch, emit);
+    } else {
+      fft_stage_fixed<R0, 1, N, TT, DIR, true, false>(v, t, active, sp, sa, tw, fetch, emit);
+      fft_stage_fixed<R1, R0, N, TT, DIR, false, false>(v, t, active, sp, sa, tw, fetch, emit);
+      fft_stage_fixed<R2, R0 * R1, N, TT, DIR, false, true>(v, t, active, sp, sa, tw, fetch, emit);
+    }
+  }
+};
+
+// Axis lengths with a compile-time transform (the host planner produces exactly
+// these plans for them; any other plan takes the runtime path).
+#define QSM_FIXED_PLANS(X)                                                                        \
+  X(64, 4, 16, 4, 1) X(96, 8, 16, 6, 1) X(128, 8, 16, 8, 1) X(160, 16, 16, 10, 1)                 \
+  X(176, 16, 16, 11, 1) X(192, 16, 16, 12, 1) X(256, 16, 16, 16, 1) X(384, 26, 16, 8, 3)
+
 // Full 1D transform of one pencil. DIR = -1 forward (exp(-2 pi i nk/n)), +1 inverse
 // (unnormalised).  tw points at the forward table W_n^k, k in [0, n).
 //
@@ -239,6 +319,13 @@ __device__ __noinline__ void fft_pencil(const FftPlan1D* plp, int t, bool active
     if constexpr (DST_G) gdst[base + e * stride] = v;
     else sp[sa(e)] = v;
   };
+#define QSM_TRY_FIXED(N_, T_, R0_, R1_, R2_)                                              \
+  if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(pl)) {                                    \
+    FixedPlan<N_, T_, R0_, R1_, R2_>::template run<DIR>(t, active, sp, sa, tw, fetch, emit); \
+    return;                                                                               \
+  }
+  QSM_FIXED_PLANS(QSM_TRY_FIXED)
+#undef QSM_TRY_FIXED
   constexpr int EMAX = kFftEmax;
   C v[EMAX];
   for (int s = 0; s < pl.nstages; ++s) {
