@@ -14,6 +14,7 @@
 // 423-479); the 3D passes built on this engine live in passes.cuh.
 #pragma once
 
+#include <type_traits>
 #include <utility>
 #include "common.cuh"
 #include "fft_plan.h"
@@ -319,13 +320,18 @@ __device__ __noinline__ void fft_pencil(const FftPlan1D* plp, int t, bool active
     if constexpr (DST_G) gdst[base + e * stride] = v;
     else sp[sa(e)] = v;
   };
-#define QSM_TRY_FIXED(N_, T_, R0_, R1_, R2_)                                              \
-  if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(pl)) {                                    \
-    FixedPlan<N_, T_, R0_, R1_, R2_>::template run<DIR>(t, active, sp, sa, tw, fetch, emit); \
-    return;                                                                               \
-  }
-  QSM_FIXED_PLANS(QSM_TRY_FIXED)
+  // Compile-time plans only for the contiguous (X) passes in single precision:
+  // inlining every plan into the strided Y/Z engine, or into the double-precision
+  // engine, raises the register count past the occupancy budget.
+  if constexpr (!std::is_same<SA, SAStrided>::value && sizeof(C) == 8) {
+#define QSM_TRY_FIXED(N_, T_, R0_, R1_, R2_)                                                \
+    if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(pl)) {                                    \
+      FixedPlan<N_, T_, R0_, R1_, R2_>::template run<DIR>(t, active, sp, sa, tw, fetch, emit); \
+      return;                                                                               \
+    }
+    QSM_FIXED_PLANS(QSM_TRY_FIXED)
 #undef QSM_TRY_FIXED
+  }
   constexpr int EMAX = kFftEmax;
   C v[EMAX];
   for (int s = 0; s < pl.nstages; ++s) {

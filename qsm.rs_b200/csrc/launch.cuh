@@ -127,8 +127,7 @@ template <class K> unsigned persistent_grid(qsm_ctx* ctx, K kernel, int threads,
   return (unsigned)g;
 }
 
-template <typename T> TileWalk tile_walk(const Fft3<T>& f, int axis) {
-  const int P = yz_cols<T>();
+template <typename T> TileWalk tile_walk(const Fft3<T>& f, int axis, int P) {
   TileWalk w;
   w.ntx = (f.g.nxh + P - 1) / P;
   if (axis == 1) {  // Y: outer = z
@@ -143,8 +142,27 @@ template <typename T> TileWalk tile_walk(const Fft3<T>& f, int axis) {
   return w;
 }
 
-template <typename T> inline size_t yz_smem(int n) {
-  return (size_t)(((n + 7) & ~7) + 2 * (size_t)n * yz_cols<T>()) * sizeof(cplx_t<T>);
+template <typename T> inline size_t yz_smem(int n, int P) {
+  return (size_t)(((n + 7) & ~7) + 2 * (size_t)n * P) * sizeof(cplx_t<T>);
+}
+
+// Tile width for a Y/Z pass: 128-byte rows, halved while the block (P x T threads)
+// does not fit on an SM (long axes: many threads, registers, shared memory).
+template <typename T, class K> int yz_tile_width(K kernel, int n, int Tn) {
+  constexpr int kMinP = 16 / (int)sizeof(cplx_t<T>) > 0 ? 16 / (int)sizeof(cplx_t<T>) : 1;
+  for (int P = yz_cols<T>(); P >= kMinP; P /= 2) {
+    if (P * Tn > 1024) continue;
+    const size_t smem = yz_smem<T>(n, P);
+    if (smem > 227u * 1024u) continue;
+    ensure_smem(kernel, smem);
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, P * Tn, smem) != cudaSuccess) {
+      (void)cudaGetLastError();
+      continue;
+    }
+    if (per_sm >= 1) return P;
+  }
+  throw QsmError(QSM_ERR_UNSUPPORTED_SIZE, "axis of length " + std::to_string(n) + " does not fit one tile");
 }
 
 // AXIS 1 = y, 2 = z; DIR -1 forward, +1 inverse.
@@ -152,12 +170,10 @@ template <typename T, int DIR, int AXIS, class Op>
 void run_yz(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst, const Op& op, const int* done) {
   const FftPlan1D& pl = (AXIS == 1) ? f.py : f.pz;
   const cplx_t<T>* tw = (AXIS == 1) ? f.twy : f.twz;
-  const int P = yz_cols<T>();
-  if (P * pl.T > 1024) throw QsmError(QSM_ERR_UNSUPPORTED_SIZE, "axis too long for one tile");
-  const size_t smem = yz_smem<T>(pl.n);
   auto kern = k_pass_yz<T, DIR, AXIS, Op>;
-  ensure_smem(kern, smem);
-  const TileWalk w = tile_walk(f, AXIS);
+  const int P = yz_tile_width<T>(kern, pl.n, pl.T);
+  const size_t smem = yz_smem<T>(pl.n, P);
+  const TileWalk w = tile_walk(f, AXIS, P);
   const unsigned grid = persistent_grid(ctx, kern, P * pl.T, smem, w.ntiles);
   LaunchScope ls(ctx, AXIS == 1 ? (DIR < 0 ? "fft_y_fwd" : "fft_y_inv") : (DIR < 0 ? "fft_z_fwd" : "fft_z_inv"));
   kern<<<grid, dim3(P, pl.T), smem, ctx->stream>>>(f.g, pl, w, tw, src, dst, op, done);
@@ -168,12 +184,10 @@ template <typename T, class Op>
 void run_z_fused(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst, const Op& op,
                  const int* done) {
   const FftPlan1D& pl = f.pz;
-  const int P = yz_cols<T>();
-  if (P * pl.T > 1024) throw QsmError(QSM_ERR_UNSUPPORTED_SIZE, "axis too long for one tile");
-  const size_t smem = yz_smem<T>(pl.n);
   auto kern = k_z_fused<T, Op>;
-  ensure_smem(kern, smem);
-  const TileWalk w = tile_walk(f, 2);
+  const int P = yz_tile_width<T>(kern, pl.n, pl.T);
+  const size_t smem = yz_smem<T>(pl.n, P);
+  const TileWalk w = tile_walk(f, 2, P);
   const unsigned grid = persistent_grid(ctx, kern, P * pl.T, smem, w.ntiles);
   LaunchScope ls(ctx, "fft_z_fused");
   kern<<<grid, dim3(P, pl.T), smem, ctx->stream>>>(f.g, pl, w, f.twz, src, dst, op, done);

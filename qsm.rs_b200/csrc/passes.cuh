@@ -199,8 +199,9 @@ __global__ void k_x_c2r(Geom g, const __grid_constant__ FftPlan1D pl, const cplx
 }
 
 // ---------------------------------------------------------------------------
-// Tiled Y/Z passes.  A tile is P consecutive x' columns (P*sizeof(C) = 128 bytes) at
-// one outer index, all n elements along the transform axis.  blockDim = (P, T);
+// Tiled Y/Z passes.  A tile is P consecutive x' columns (P*sizeof(C) = 128 bytes, or
+// narrower for long axes) at one outer index, all n elements along the transform
+// axis.  blockDim = (P, T);
 // the grid is persistent (a few CTAs per SM) and walks tiles with stride gridDim.x.
 // ---------------------------------------------------------------------------
 struct TileWalk {
@@ -218,10 +219,11 @@ __device__ __forceinline__ void issue_tile(const C* __restrict__ src, C* buf, co
   const int col0 = tx * P;
   const long long base = col0 + (long long)outer * w.ostride;
   constexpr int kPer = 16 / (int)sizeof(C);  // complex values per 16-byte chunk
-  const int chunks = n * 8;                  // 8 chunks of 16 bytes per 128-byte row
+  const int cpr = P / kPer;                  // 16-byte chunks per tile row
+  const int chunks = n * cpr;
   const int nth = blockDim.x * blockDim.y;
   for (int c = threadIdx.x + threadIdx.y * blockDim.x; c < chunks; c += nth) {
-    const int e = c >> 3, ch = c & 7;
+    const int e = c / cpr, ch = c - e * cpr;
     const int col = col0 + ch * kPer;
     const bool ok = col < g.nxh;
     const C* gp = src + base + (long long)e * w.estride + (ok ? ch * kPer : 0);
@@ -320,7 +322,7 @@ __global__ void k_z_fused(Geom g, const __grid_constant__ FftPlan1D pl, TileWalk
     C* sp = cur + px;
     fft_pencil<-1, C, SAStrided, false, false>(&pl, t, active, sp, sa, tw, nullptr, nullptr, 0, 0);
     if (active) {
-#pragma unroll 4
+#pragma unroll 1
       for (int e = t; e < n; e += pl.T) sp[sa(e)] = op.mid(sp[sa(e)], col, iy, e, base + e * w.estride);
     }
     __syncthreads();
