@@ -121,6 +121,20 @@ QSM_API qsm_status qsm_tkd(qsm_ctx* ctx, const double* local_field, const uint8_
                    const double bdir[3], const qsm_tkd_params* params, double* out_chi);
 QSM_API qsm_status qsm_tkd_device(qsm_ctx* ctx, const double* d_local_field, const uint8_t* d_mask, const qsm_grid* grid,
                           const double bdir[3], const qsm_tkd_params* params, double* d_out_chi);
+/* TKD in f64 that allocates no device memory (no counterpart in the reference).
+ * For callers that cannot call cudaMalloc: another allocator holds the GPU, a
+ * real-time loop must avoid cudaMalloc's implicit synchronisation, or a fixed memory
+ * budget applies.  Same result as qsm_tkd_device in f64, without a context: pointers
+ * are device pointers on the current device, work runs on `stream` (a cudaStream_t,
+ * NULL = default stream) and the call returns after the stream has finished.  Scratch
+ * is a 48 MiB array in the library's own device memory (held by every GPU that loads
+ * the library); volumes whose scratch exceeds it (above about 160^3) return
+ * QSM_ERR_UNSUPPORTED_SIZE.  Calls share that array, so calls that overlap on the GPU
+ * race and must be serialised by the caller.  The first call on a device resolves
+ * the array's address and should come before any stream capture. */
+QSM_API qsm_status qsm_tkd_device_noalloc(const double* d_local_field, const uint8_t* d_mask, const qsm_grid* grid,
+                                          const double bdir[3], const qsm_tkd_params* params, double* d_out_chi,
+                                          void* stream);
 /* inversion::tsvd — src/inversion/tkd.rs:105-153. */
 QSM_API qsm_status qsm_tsvd(qsm_ctx* ctx, const double* local_field, const uint8_t* mask, const qsm_grid* grid,
                     const double bdir[3], const qsm_tkd_params* params, double* out_chi);

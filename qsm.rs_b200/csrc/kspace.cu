@@ -96,6 +96,15 @@ template <typename S> KSpaceT<S> make_kspace_t(qsm_ctx* ctx, const GridDims& d, 
 template KSpaceT<float> make_kspace_t<float>(qsm_ctx*, const GridDims&, const double*);
 template KSpaceT<double> make_kspace_t<double>(qsm_ctx*, const GridDims&, const double*);
 
+// Host copy of one per-axis k-space table: "freq", "lap" or "poi" (as uploaded by
+// make_kspace_t), for callers that place the tables in memory they manage.
+std::vector<double> kspace_axis_table(const char* what, int n, double vs) {
+  const std::string w(what);
+  if (w == "freq") return fftfreq(n, vs);
+  if (w == "lap") return lapneg_axis(n, vs);
+  return poisson_axis(n, vs);
+}
+
 size_t& smem_limit_slot(const void* func, int device) {
   static std::mutex mu;
   static std::map<std::pair<const void*, int>, size_t> limits;

@@ -103,6 +103,8 @@ _SIGS = [
                           C.POINTER(QsmTkdParams), c_double_p]),
     ("qsm_tkd_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(QsmGrid), c_double_p,
                                  C.POINTER(QsmTkdParams), C.c_void_p]),
+    ("qsm_tkd_device_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(QsmGrid), c_double_p,
+                                         C.POINTER(QsmTkdParams), C.c_void_p, C.c_void_p]),
     ("qsm_tsvd", C.c_int, [C.c_void_p, c_double_p, c_u8_p, C.POINTER(QsmGrid), c_double_p,
                            C.POINTER(QsmTkdParams), c_double_p]),
     ("qsm_tsvd_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(QsmGrid), c_double_p,
