@@ -180,6 +180,42 @@ void run_yz(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst
   ls.done();
 }
 
+template <typename T> inline size_t zm_smem(int n, int P) {
+  return yz_smem<T>(n, P) + 2 * (((size_t)n * P + 3) & ~(size_t)3) * sizeof(T);
+}
+
+// Tile width of the multiplier-array Z pass, 0 when no width fits (very long axes).
+template <typename T> int zm_tile_width(int n, int Tn) {
+  auto kern = k_z_fused_m<T>;
+  for (int p = yz_cols<T>(); p >= 16 / (int)sizeof(T); p /= 2) {
+    if (p * Tn > 1024 || zm_smem<T>(n, p) > 227u * 1024u) continue;
+    ensure_smem(kern, zm_smem<T>(n, p));
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, p * Tn, zm_smem<T>(n, p)) != cudaSuccess) {
+      (void)cudaGetLastError();
+      continue;
+    }
+    if (per_sm >= 1) return p;
+  }
+  return 0;
+}
+
+// Z fused pass with a precomputed real multiplier array (spectrum layout).
+template <typename T>
+void run_z_fused_m(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst, const T* mult,
+                   const int* done) {
+  const FftPlan1D& pl = f.pz;
+  auto kern = k_z_fused_m<T>;
+  const int P = zm_tile_width<T>(pl.n, pl.T);
+  if (P == 0) throw QsmError(QSM_ERR_UNSUPPORTED_SIZE, "z axis does not fit one multiplier tile");
+  const size_t smem = zm_smem<T>(pl.n, P);
+  const TileWalk w = tile_walk(f, 2, P);
+  const unsigned grid = persistent_grid(ctx, kern, P * pl.T, smem, w.ntiles);
+  LaunchScope ls(ctx, "fft_z_fused");
+  kern<<<grid, dim3(P, pl.T), smem, ctx->stream>>>(f.g, pl, w, f.twz, src, dst, mult, done);
+  ls.done();
+}
+
 template <typename T, class Op>
 void run_z_fused(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst, const Op& op,
                  const int* done) {

@@ -231,8 +231,13 @@ __device__ __forceinline__ void issue_tile(const C* __restrict__ src, C* buf, co
   }
 }
 
+// Register cap of the tiled Y/Z kernels: three 256-thread CTAs per SM in single
+// precision, three 128-thread CTAs in double.
+template <typename T> struct YzRegCap { static constexpr int value = sizeof(T) == 4 ? 80 : 128; };
+
 template <typename T, int DIR, int AXIS, class Op>
-__global__ void k_pass_yz(Geom g, const __grid_constant__ FftPlan1D pl, TileWalk w, const cplx_t<T>* __restrict__ twg,
+__global__ void __maxnreg__(YzRegCap<T>::value)
+    k_pass_yz(Geom g, const __grid_constant__ FftPlan1D pl, TileWalk w, const cplx_t<T>* __restrict__ twg,
                           const cplx_t<T>* src, cplx_t<T>* dst, Op op, const int* __restrict__ done) {
   using C = cplx_t<T>;
   if (done != nullptr && *done) return;
@@ -287,9 +292,87 @@ __global__ void k_pass_yz(Geom g, const __grid_constant__ FftPlan1D pl, TileWalk
   cp_async_wait<0>();
 }
 
+// Real multiplier tile (same tile walk, element size sizeof(T)), 16-byte chunks.
+template <typename T>
+__device__ __forceinline__ void issue_mtile(const T* __restrict__ src, T* buf, const Geom& g, const TileWalk& w,
+                                            int tile, int n, int P) {
+  const int tx = tile % w.ntx;
+  const int outer = tile / w.ntx;
+  const int col0 = tx * P;
+  const long long base = col0 + (long long)outer * w.ostride;
+  constexpr int kPer = 16 / (int)sizeof(T);
+  const int cpr = P / kPer;
+  const int chunks = n * cpr;
+  const int nth = blockDim.x * blockDim.y;
+  for (int c = threadIdx.x + threadIdx.y * blockDim.x; c < chunks; c += nth) {
+    const int e = c / cpr, ch = c - e * cpr;
+    const int col = col0 + ch * kPer;
+    const bool ok = col < g.nxh;
+    const T* gp = src + base + (long long)e * w.estride + (ok ? ch * kPer : 0);
+    cp_async16(buf + e * P + ch * kPer, gp, ok);
+  }
+}
+
+// Z forward -> multiply by a precomputed real multiplier -> Z inverse.  The
+// multiplier (spectrum layout, real) is staged with the spectrum tile, so the
+// pointwise step is one shared-memory read per element.  Needs P*sizeof(T) >= 16.
+template <typename T>
+__global__ void __maxnreg__(YzRegCap<T>::value) k_z_fused_m(Geom g, const __grid_constant__ FftPlan1D pl, TileWalk w,
+                            const cplx_t<T>* __restrict__ twg, const cplx_t<T>* src, cplx_t<T>* dst,
+                            const T* __restrict__ mult, const int* __restrict__ done) {
+  using C = cplx_t<T>;
+  if (done != nullptr && *done) return;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* tw = reinterpret_cast<C*>(smraw);
+  const int n = pl.n;
+  const int P = blockDim.x;
+  C* buf0 = tw + ((n + 7) & ~7);
+  C* buf1 = buf0 + (size_t)n * P;
+  T* mb0 = reinterpret_cast<T*>(buf1 + (size_t)n * P);
+  T* mb1 = mb0 + (((size_t)n * P + 3) & ~(size_t)3);
+  const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+  for (int i = tid; i < n; i += blockDim.x * blockDim.y) tw[i] = twg[i];
+  const int px = threadIdx.x;
+  const int t = threadIdx.y;
+  SAStrided sa{P};
+  int tile = blockIdx.x;
+  if (tile < w.ntiles) {
+    issue_tile(src, buf0, g, w, tile, n, P);
+    issue_mtile(mult, mb0, g, w, tile, n, P);
+  }
+  cp_async_commit();
+  for (int it = 0; tile < w.ntiles; tile += gridDim.x, ++it) {
+    C* cur = (it & 1) ? buf1 : buf0;
+    C* nxt = (it & 1) ? buf0 : buf1;
+    T* mcur = (it & 1) ? mb1 : mb0;
+    T* mnxt = (it & 1) ? mb0 : mb1;
+    const int next = tile + gridDim.x;
+    if (next < w.ntiles) {
+      issue_tile(src, nxt, g, w, next, n, P);
+      issue_mtile(mult, mnxt, g, w, next, n, P);
+    }
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    const int tx = tile % w.ntx, iy = tile / w.ntx;
+    const int col = tx * P + px;
+    const bool active = col < g.nxh;
+    const long long base = col + (long long)iy * w.ostride;
+    C* sp = cur + px;
+    fft_pencil<-1, C, SAStrided, false, false>(&pl, t, active, sp, sa, tw, nullptr, nullptr, 0, 0);
+    if (active) {
+      for (int e = t; e < n; e += pl.T) sp[sa(e)] = cscale(sp[sa(e)], mcur[e * P + px]);
+    }
+    __syncthreads();
+    fft_pencil<+1, C, SAStrided, false, true>(&pl, t, active, sp, sa, tw, nullptr, dst, base, w.estride);
+  }
+  cp_async_wait<0>();
+}
+
 // Z forward -> Op::mid pointwise -> Z inverse, tiled like k_pass_yz (outer = y).
 template <typename T, class Op>
-__global__ void k_z_fused(Geom g, const __grid_constant__ FftPlan1D pl, TileWalk w, const cplx_t<T>* __restrict__ twg,
+__global__ void __maxnreg__(YzRegCap<T>::value)
+    k_z_fused(Geom g, const __grid_constant__ FftPlan1D pl, TileWalk w, const cplx_t<T>* __restrict__ twg,
                           const cplx_t<T>* src, cplx_t<T>* dst, Op op, const int* __restrict__ done) {
   using C = cplx_t<T>;
   if (done != nullptr && *done) return;

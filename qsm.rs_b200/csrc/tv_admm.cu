@@ -61,6 +61,27 @@ template <typename T> struct OpAdmmMul {
   }
 };
 
+// Per-iteration multiplier rho*sym(inv_a) as a real half-spectrum array (spectrum
+// layout, padding columns 0), evaluated once per solve in double.
+template <typename T>
+__global__ void k_admm_mult(Geom g, KSpace K, double rho, T* __restrict__ out) {
+  const long long H = g.hsize();
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < H; i += (long long)gridDim.x * blockDim.x) {
+    const int ix = (int)(i % g.pitch);
+    const long long r = i / g.pitch;
+    const int iy = (int)(r % g.ny);
+    const int iz = (int)(r / g.ny);
+    double m = 0.0;
+    if (ix < g.nxh) {
+      const KSpace& k = K;
+      m = rho * K.sym(ix, iy, iz, [&](double kx, double ky, double kz, int a, int b, int c) {
+        return admm_inv_a<double>(k, kx, ky, kz, a, b, c, rho);
+      });
+    }
+    out[i] = (T)m;
+  }
+}
+
 template <typename T> struct StoreReal {
   T* __restrict__ out;
   int nx;
@@ -253,6 +274,15 @@ void tv_admm_impl(qsm_ctx* ctx, const GridDims& d, const double* d_f, const uint
   const T hx = (T)(1.0 / d.vsx), hy = (T)(1.0 / d.vsy), hz = (T)(1.0 / d.vsz);
   const T thr = (T)(p.lambda / p.rho);
   const OpAdmmMul<T> mul{KT, (T)p.rho};
+  // precomputed multiplier tiles need P*sizeof(T) >= 16 (always true for the
+  // 128-byte tiles; narrow tiles of very long z axes use the in-kernel multiplier)
+  T* mult = ws<T>(ctx, nm("mult"), (size_t)H);
+  {
+    LaunchScope ls(ctx, "admm_mult");
+    k_admm_mult<T><<<grid1d(H), 256, 0, ctx->stream>>>(f.g, K64, p.rho, mult);
+    ls.done();
+  }
+  const bool use_mult = zm_tile_width<T>(d.nz, f.pz.T) > 0;
   // iteration i with parity q = i % 2: reads y_{i-1} = yb[1-q], y_{i-2} = yb[q],
   // u = ub[1-q]; writes u' = ub[q], y_i = yb[q]
   auto step = [&](int q, int check_only) {
@@ -266,7 +296,8 @@ void tv_admm_impl(qsm_ctx* ctx, const GridDims& d, const double* d_f, const uint
     step(q, 0);
     run_x_r2c<T>(ctx, f, spec, LoadCast<T, T>{div, d.nx}, done);
     run_yz<T, -1, 1>(ctx, f, spec, spec, OpId<T>{}, done);
-    run_z_fused<T>(ctx, f, spec, spec, mul, done);
+    if (use_mult) run_z_fused_m<T>(ctx, f, spec, spec, mult, done);
+    else run_z_fused<T>(ctx, f, spec, spec, mul, done);
     run_yz<T, +1, 1>(ctx, f, spec, spec, OpId<T>{}, done);
     run_x_c2r<T>(ctx, f, spec, StoreReal<T>{yb[q], d.nx, scale}, done);
   };
