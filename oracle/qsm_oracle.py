@@ -568,3 +568,375 @@ def cg_solve(a_op, b, x0, tol, max_iter, progress=None):
         p = r + beta * p
         rsold = rsnew
     return x
+
+
+# ---------------------------------------------------------------------------
+# iLSQR (src/inversion/ilsqr.rs)
+# ---------------------------------------------------------------------------
+@dataclass
+class IlsqrParams:  # src/inversion/ilsqr.rs:20-34
+    tol: float = 0.01
+    max_iter: int = 50
+
+
+def lsqr_real(apply_a, apply_at, b, tol, max_iter):
+    """Real LSQR, relative-residual stop (src/inversion/ilsqr.rs:62-148)."""
+    u = np.array(b, dtype=np.float64)
+    beta = float(np.linalg.norm(u))
+    if beta > 0:
+        u = u * (1.0 / beta)
+    v = apply_at(u)
+    alpha = float(np.linalg.norm(v))
+    if alpha > 0:
+        v = v * (1.0 / alpha)
+    w = v.copy()
+    x = np.zeros_like(v)
+    phi_bar, rho_bar, bnorm = beta, alpha, beta
+    for _ in range(max_iter):
+        u_new = apply_a(v) - alpha * u
+        beta = float(np.linalg.norm(u_new))
+        if beta > 0:
+            u_new = u_new * (1.0 / beta)
+        u = u_new
+        v_new = apply_at(u) - beta * v
+        alpha = float(np.linalg.norm(v_new))
+        if alpha > 0:
+            v_new = v_new * (1.0 / alpha)
+        v = v_new
+        rho = math.sqrt(rho_bar * rho_bar + beta * beta)
+        c, s = rho_bar / rho, beta / rho
+        theta = s * alpha
+        rho_bar = -c * alpha
+        phi = c * phi_bar
+        phi_bar *= s
+        t1, t2 = phi / rho, -theta / rho
+        x = x + t1 * w
+        w = v + t2 * w
+        if phi_bar / (bnorm + 1e-20) < tol:
+            break
+    return x
+
+
+def lsqr_complex(apply_a, apply_ah, b, tol, max_iter, return_iters=False):
+    """Complex LSQR stopping on ||r||/||b|| <= tol (src/inversion/ilsqr.rs:177-321)."""
+    u = np.array(b, dtype=np.complex128)
+    beta = float(np.linalg.norm(u))
+    if beta > 0:
+        u = u * (1.0 / beta)
+    v = apply_ah(u)
+    alpha = float(np.linalg.norm(v))
+    if alpha > 0:
+        v = v * (1.0 / alpha)
+    w = v.copy()
+    x = np.zeros_like(v)
+    phi_bar, rho_bar, bnorm = beta, alpha, beta
+    it_done = 0
+    if alpha * beta == 0.0:
+        return (x, 0) if return_iters else x
+    for it in range(max_iter):
+        u_new = apply_a(v) - alpha * u
+        beta = float(np.linalg.norm(u_new))
+        if beta > 0:
+            u_new = u_new * (1.0 / beta)
+        u = u_new
+        v_new = apply_ah(u) - beta * v
+        alpha = float(np.linalg.norm(v_new))
+        if alpha > 0:
+            v_new = v_new * (1.0 / alpha)
+        v = v_new
+        rho = math.sqrt(rho_bar * rho_bar + beta * beta)
+        c, s = rho_bar / rho, beta / rho
+        theta = s * alpha
+        rho_bar = -c * alpha
+        phi = c * phi_bar
+        phi_bar *= s
+        t1, t2 = phi / rho, -theta / rho
+        x = x + t1 * w
+        w = v + t2 * w
+        it_done = it + 1
+        if phi_bar / (bnorm + 1e-20) <= tol:
+            break
+    return (x, it_done) if return_iters else x
+
+
+def lsmr(apply_a, apply_at, b, n, atol, btol, max_iter, return_iters=False):
+    """LSMR, undamped, Fong & Saunders tests 1-3 with conlim 1e8 (src/inversion/ilsqr.rs:344-517)."""
+    u = np.array(b, dtype=np.float64)
+    beta = float(np.linalg.norm(u))
+    if beta > 0:
+        u = u * (1.0 / beta)
+    v = apply_at(u)
+    alpha = float(np.linalg.norm(v))
+    if alpha > 0:
+        v = v * (1.0 / alpha)
+    alpha_bar, zeta_bar = alpha, alpha * beta
+    rho, rho_bar, c_bar, s_bar = 1.0, 1.0, 1.0, 0.0
+    h = v.copy()
+    h_bar = np.zeros(n)
+    x = np.zeros(n)
+    normb, betadd, betad, rhodold, tautildeold, thetatilde, zeta, d = beta, beta, 0.0, 1.0, 0.0, 0.0, 0.0, 0.0
+    norm_a2 = alpha * alpha
+    maxrbar, minrbar = 0.0, 1e100
+    ctol = 1.0 / 1e8
+    it_done = 0
+    if alpha * beta == 0.0:
+        return (x, 0) if return_iters else x
+    for it in range(max_iter):
+        u_new = apply_a(v) - alpha * u
+        beta = float(np.linalg.norm(u_new))
+        if beta > 0:
+            u_new = u_new * (1.0 / beta)
+        u = u_new
+        v_new = apply_at(u) - beta * v
+        alpha = float(np.linalg.norm(v_new))
+        if alpha > 0:
+            v_new = v_new * (1.0 / alpha)
+        v = v_new
+        rho_old = rho
+        rho = math.sqrt(alpha_bar * alpha_bar + beta * beta)
+        c, s = alpha_bar / rho, beta / rho
+        theta_new = s * alpha
+        alpha_bar = c * alpha
+        rho_bar_old, zeta_old = rho_bar, zeta
+        theta_bar = s_bar * rho
+        rho_temp = c_bar * rho
+        rho_bar = math.sqrt(rho_temp * rho_temp + theta_new * theta_new)
+        c_bar, s_bar = rho_temp / rho_bar, theta_new / rho_bar
+        zeta = c_bar * zeta_bar
+        zeta_bar *= -s_bar
+        h_bar = h - (theta_bar * rho / (rho_old * rho_bar_old)) * h_bar
+        x = x + (zeta / (rho * rho_bar)) * h_bar
+        h = v - (theta_new / rho) * h
+        betaacute = betadd
+        betahat = c * betaacute
+        betadd = -s * betaacute
+        thetatildeold = thetatilde
+        rhotildeold = math.sqrt(rhodold * rhodold + theta_bar * theta_bar)
+        ctildeold, stildeold = rhodold / rhotildeold, theta_bar / rhotildeold
+        thetatilde = stildeold * rho_bar
+        rhodold = ctildeold * rho_bar
+        betad = -stildeold * betad + ctildeold * betahat
+        tautildeold = (zeta_old - thetatildeold * tautildeold) / rhotildeold
+        taud = (zeta - thetatilde * tautildeold) / rhodold
+        normr = math.sqrt(d + (betad - taud) ** 2 + betadd * betadd)
+        norm_a2 += beta * beta
+        norm_a = math.sqrt(norm_a2)
+        norm_a2 += alpha * alpha
+        maxrbar = max(maxrbar, rho_bar_old)
+        if it > 0:
+            minrbar = min(minrbar, rho_bar_old)
+        cond_a = max(maxrbar, rho_temp) / min(minrbar, rho_temp)
+        norm_ar = abs(zeta_bar)
+        normx = float(np.linalg.norm(x))
+        test1 = normr / (normb + 1e-20)
+        test2 = norm_ar / ((norm_a * normr) + 1e-20)
+        test3 = 1.0 / (cond_a + 1e-20)
+        rtol = btol + atol * norm_a * normx / (normb + 1e-20)
+        it_done = it + 1
+        if test3 <= ctol or test2 <= atol or test1 <= rtol:
+            break
+    return (x, it_done) if return_iters else x
+
+
+def prctile(sorted_vals, p):
+    """Linear-interpolation percentile of a sorted array (src/inversion/ilsqr.rs:937-946)."""
+    n = len(sorted_vals)
+    if n == 0:
+        return 0.0
+    if n == 1:
+        return float(sorted_vals[0])
+    h = (p / 100.0) * (n - 1)
+    lo = int(math.floor(h))
+    hi = min(lo + 1, n - 1)
+    frac = h - lo
+    return float(sorted_vals[lo] + frac * (sorted_vals[hi] - sorted_vals[lo]))
+
+
+def _lap1_axis(f, m, axis, h):
+    """Mask-adaptive second difference along one axis (src/inversion/ilsqr.rs:571-669)."""
+    n = f.shape[axis]
+    fm = np.moveaxis(f, axis, -1)
+    mm = np.moveaxis(m, axis, -1)
+    out = np.zeros_like(fm)
+    for c in range(n):
+        # stencil selector: interior -> 2*mask[+1] + mask[-1]; first -> 2; last -> 1
+        if 1 <= c <= n - 2:
+            sel = 2 * mm[..., c + 1].astype(np.int64) + mm[..., c - 1].astype(np.int64)
+        else:
+            sel = np.full(fm.shape[:-1], 2 if c == 0 else (1 if c == n - 1 else 0), dtype=np.int64)
+        val = np.zeros(fm.shape[:-1])
+        central = sel == 3
+        if central.any():
+            val = np.where(central, fm[..., c - 1] - 2.0 * fm[..., c] + fm[..., c + 1] if 1 <= c <= n - 2 else 0.0, val)
+        fwd = sel == 2
+        if fwd.any() and c + 1 < n:
+            o4 = (c + 3 < n)
+            m2 = mm[..., c + 2] != 0 if c + 2 < n else np.zeros(fm.shape[:-1], bool)
+            m3 = mm[..., c + 3] != 0 if c + 3 < n else np.zeros(fm.shape[:-1], bool)
+            v4 = (2.0 * fm[..., c] - 5.0 * fm[..., c + 1] + 4.0 * fm[..., c + 2] - fm[..., c + 3]) if o4 else 0.0
+            v2 = (fm[..., c] - 2.0 * fm[..., c + 1] + fm[..., c + 2]) if c + 2 < n else 0.0
+            v1 = fm[..., c + 1] - fm[..., c]
+            fv = np.where(o4 & m2 & m3, v4, np.where((c + 2 < n) & m2, v2, v1))
+            val = np.where(fwd, fv, val)
+        bwd = sel == 1
+        if bwd.any() and c - 1 >= 0:
+            m2 = mm[..., c - 2] != 0 if c - 2 >= 0 else np.zeros(fm.shape[:-1], bool)
+            m3 = mm[..., c - 3] != 0 if c - 3 >= 0 else np.zeros(fm.shape[:-1], bool)
+            v4 = (-fm[..., c - 3] + 4.0 * fm[..., c - 2] - 5.0 * fm[..., c - 1] + 2.0 * fm[..., c]) if c - 3 >= 0 else 0.0
+            v2 = (fm[..., c - 2] - 2.0 * fm[..., c - 1] + fm[..., c]) if c - 2 >= 0 else 0.0
+            v1 = fm[..., c - 1] - fm[..., c]
+            bv = np.where((c - 3 >= 0) & m3 & m2, v4, np.where((c - 2 >= 0) & m2, v2, v1))
+            val = np.where(bwd, bv, val)
+        out[..., c] = val
+    return np.moveaxis(out, -1, axis) * h
+
+
+def ilsqr_laplacian(f, mask, grid: Grid):
+    """Mask-adaptive Laplacian, zero outside the mask (src/inversion/ilsqr.rs:528-566)."""
+    vsx, vsy, vsz = grid.voxel_size
+    m = (mask != 0)
+    lap = np.zeros(grid.shape)
+    lap += _lap1_axis(f, mask, 2, 1.0 / (vsx * vsx))
+    lap += _lap1_axis(f, mask, 1, 1.0 / (vsy * vsy))
+    lap += _lap1_axis(f, mask, 0, 1.0 / (vsz * vsz))
+    return np.where(m, lap, 0.0)
+
+
+def _percentile_weights(vals, mask, pmin, pmax, extra_mask_multiply=False):
+    sel = np.sort(vals[mask != 0])
+    w = np.zeros(vals.shape)
+    if sel.size == 0:
+        return w
+    tmin, tmax = prctile(sel, pmin), prctile(sel, pmax)
+    rng = tmax - tmin
+    inner = np.where(rng > 1e-10, (tmax - vals) / (rng if rng != 0 else 1.0), 0.0)
+    ww = np.where(vals < tmin, 1.0, np.where(vals > tmax, 0.0, inner))
+    if extra_mask_multiply:
+        ww = ww * mask.astype(np.float64)
+    return np.where(mask != 0, ww, 0.0)
+
+
+def laplacian_weights_ilsqr(f, mask, grid: Grid, pmin=60.0, pmax=99.9):
+    """Equation 7 weights (src/inversion/ilsqr.rs:672-719)."""
+    return _percentile_weights(ilsqr_laplacian(f, mask, grid), mask, pmin, pmax)
+
+
+def dipole_kspace_weights_ilsqr(d, n_exp=0.001, pa=1.0, pb=30.0):
+    """|D|^n normalised by percentiles over all values (src/inversion/ilsqr.rs:724-760)."""
+    w = np.abs(d) ** n_exp
+    vals = np.sort(w.ravel())
+    lo, hi = prctile(vals, pa), prctile(vals, pb)
+    rng = hi - lo
+    if rng > 1e-20:
+        w = (w - lo) / rng
+    return np.clip(w, 0.0, 1.0)
+
+
+def fgrad_masked(f, mask, grid: Grid):
+    """Mask-adaptive forward/backward gradient (src/inversion/ilsqr.rs:767-823)."""
+    vsx, vsy, vsz = grid.voxel_size
+    m = mask != 0
+    out = []
+    for axis, h in ((2, 1.0 / vsx), (1, 1.0 / vsy), (0, 1.0 / vsz)):
+        n = f.shape[axis]
+        fp = np.roll(f, -1, axis)
+        fmn = np.roll(f, 1, axis)
+        mp = np.roll(m, -1, axis)
+        mmn = np.roll(m, 1, axis)
+        idx = np.arange(n).reshape([-1 if a == axis else 1 for a in range(3)])
+        can_f = (idx < n - 1) & mp
+        can_b = (idx > 0) & mmn
+        g = np.where(can_f, h * (fp - f), np.where(can_b, h * (f - fmn), 0.0))
+        out.append(np.where(m, g, 0.0))
+    return tuple(out)
+
+
+def lsqr_step(f, mask, grid: Grid, d):
+    """Step 1 (src/inversion/ilsqr.rs:953-1030)."""
+    w = laplacian_weights_ilsqr(f, mask, grid)
+    b = fft3d((w * f).astype(np.complex128)) * d
+
+    def apply_a(x):
+        x3 = x.reshape(grid.shape)
+        r = ifft3d(d * x3).real
+        return (fft3d((w * r).astype(np.complex128)) * d).ravel()
+
+    x = lsqr_complex(apply_a, apply_a, b.ravel(), 0.01, 50)
+    xi = ifft3d(x.reshape(grid.shape))
+    return np.where(mask != 0, xi.real, 0.0)
+
+
+def fastqsm_step(f, mask, grid: Grid, d):
+    """Step 2 (src/inversion/ilsqr.rs:1037-1167)."""
+    F = fft3d(f.astype(np.complex128))
+    x = F * np.sign(d)
+    wfs = dipole_kspace_weights_ilsqr(d)
+    h = fft_real_kernel(smv_kernel(grid, 3.0))
+    filt = wfs + h * (1.0 - wfs)
+    xf = ifft3d(x * wfs + x * h * (1.0 - wfs))
+    xf = np.where(mask != 0, xf.real, 0.0).astype(np.complex128)
+    xf = fft3d(xf)
+    xf2 = ifft3d(xf * wfs + xf * h * (1.0 - wfs))
+    x_fs = np.where(mask != 0, xf2.real, 0.0)
+    t0 = 1.0 / 8.0
+    with np.errstate(divide="ignore"):
+        inv_d = np.where(np.abs(d) < t0, np.sign(d) / t0, 1.0 / d)
+    # Rust f64::signum(0.0) = 1.0 (src/inversion/ilsqr.rs:1129)
+    inv_d = np.where((np.abs(d) < t0) & (d == 0.0), np.copysign(1.0, d) / t0, inv_d)
+    x_tkd = np.where(mask != 0, ifft3d(F * inv_d).real, 0.0)
+    n_all = float(f.size)
+    s_fs, s_tkd = float(x_fs.sum()), float(x_tkd.sum())
+    s_fs2, s_ft = float((x_fs * x_fs).sum()), float((x_fs * x_tkd).sum())
+    det = s_fs2 * n_all - s_fs * s_fs
+    if abs(det) > 1e-20:
+        a = (n_all * s_ft - s_fs * s_tkd) / det
+        bb = (s_fs2 * s_tkd - s_fs * s_ft) / det
+    else:
+        a, bb = 1.0, 0.0
+    del filt
+    return np.where(mask != 0, a * x_fs + bb, 0.0)
+
+
+def susceptibility_artifacts_step(x0, xfs, mask, grid: Grid, d, tol, maxit):
+    """Step 3 (src/inversion/ilsqr.rs:1174-1289)."""
+    gx, gy, gz = fgrad_masked(xfs, mask, grid)
+    wx = _percentile_weights(gx, mask, 50.0, 70.0, True)
+    wy = _percentile_weights(gy, mask, 50.0, 70.0, True)
+    wz = _percentile_weights(gz, mask, 50.0, 70.0, True)
+    mic = (np.abs(d) < 0.1).astype(np.float64)
+    dx, dy, dz = fgrad(x0, grid)
+    b = np.concatenate([(wx * dx).ravel(), (wy * dy).ravel(), (wz * dz).ravel()])
+    n = x0.size
+
+    def apply_a(xin):
+        xr = ifft3d(fft3d(xin.reshape(grid.shape).astype(np.complex128)) * mic).real
+        ax, ay, az = fgrad(xr, grid)
+        return np.concatenate([(wx * ax).ravel(), (wy * ay).ravel(), (wz * az).ravel()])
+
+    def apply_at(yin):
+        yx, yy, yz = (yin[i * n:(i + 1) * n].reshape(grid.shape) for i in range(3))
+        dv = bdiv(wx * yx, wy * yy, wz * yz, grid)
+        return ifft3d(fft3d((-dv).astype(np.complex128)) * mic).real.ravel()
+
+    xsa = lsmr(apply_a, apply_at, b, n, tol, tol, maxit)
+    return np.where(mask.ravel() != 0, xsa, 0.0).reshape(grid.shape)
+
+
+def ilsqr(field_, mask, grid: Grid, bdir, params: IlsqrParams = IlsqrParams(), progress=None):
+    """iLSQR: (chi, xsa, xfs, xlsqr) (src/inversion/ilsqr.rs:1307-1351)."""
+    f = _vol(field_, grid)
+    m = _vol(mask, grid, np.uint8)
+    d = dipole_kernel(grid, bdir)
+    if progress:
+        progress(1, 4)
+    xlsqr = lsqr_step(f, m, grid, d)
+    if progress:
+        progress(2, 4)
+    xfs = fastqsm_step(f, m, grid, d)
+    if progress:
+        progress(3, 4)
+    xsa = susceptibility_artifacts_step(xlsqr, xfs, m, grid, d, params.tol, params.max_iter)
+    if progress:
+        progress(4, 4)
+    chi = np.where(m != 0, xlsqr - xsa, 0.0)
+    return chi, xsa, xfs, xlsqr
