@@ -32,6 +32,11 @@ import numpy as np  # noqa: E402
 DIMS = (256, 256, 176)
 ITERS = 250
 METRIC = "TV-ADMM volumes/s at 256x256x176 (250 iterations)"
+# DRAM bytes (read + write) per launch of the dominant kernels, from one ncu --set full
+# capture of this workload (profiles/tv_admm_256x256x176_kernels.md); ncu flushes the
+# caches before each replay, so these are cold-cache figures.
+NCU_TRAFFIC = {"tv_step": 441453056, "fft_z_fused": 77602560}
+NCU_TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/tv_admm_256x256x176_kernels.md"
 UNIT = "volumes/s"
 
 
@@ -351,7 +356,8 @@ def main():
     dom = max((n for n in kernels if n in model), key=lambda n: kernels[n]["total_ms"])
     iter_bytes = 20 * N * 4
     roofline = {"bound": "hbm", "achieved": kernels[dom]["gbs"], "peak": peak, "unit": "GB/s",
-                "frac": round(kernels[dom]["gbs"] / peak, 3), "traffic": None, "kernel": dom,
+                "frac": round(kernels[dom]["gbs"] / peak, 3), "traffic": NCU_TRAFFIC.get(dom), "kernel": dom,
+                "traffic_source": NCU_TRAFFIC_SOURCE if dom in NCU_TRAFFIC else None,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
                 "fallback 6.65 TB/s",
                 "iteration_model_gbs": round(iter_bytes / (ms_step / ITERS / 1e3) / 1e9, 1),
