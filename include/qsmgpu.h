@@ -98,12 +98,16 @@ typedef struct { double lambda; int reg; } qsm_tikhonov_params;
 typedef struct { double threshold, radius; } qsm_sharp_params;
 /* VsharpParams — src/bgremove/vsharp.rs:22-40 (0.05, 12.0, 1.0). */
 typedef struct { double threshold, max_radius, min_radius; } qsm_vsharp_params;
+/* IlsqrParams — src/inversion/ilsqr.rs:20-34 (tol 0.01, max_iter 50: the LSMR step's
+ * tolerance and iteration cap). */
+typedef struct { double tol; size_t max_iter; } qsm_ilsqr_params;
 
 QSM_API void qsm_tv_params_default(qsm_tv_params* p);
 QSM_API void qsm_tkd_params_default(qsm_tkd_params* p);
 QSM_API void qsm_tikhonov_params_default(qsm_tikhonov_params* p);
 QSM_API void qsm_sharp_params_default(qsm_sharp_params* p);
 QSM_API void qsm_vsharp_params_default(qsm_vsharp_params* p);
+QSM_API void qsm_ilsqr_params_default(qsm_ilsqr_params* p);
 
 /* -------------------------------------------------------- dipole inversion -- */
 /* inversion::tv_admm — src/inversion/tv.rs:63-97 (+ admm.rs:76-178). */
@@ -141,6 +145,17 @@ QSM_API qsm_status qsm_tsvd(qsm_ctx* ctx, const double* local_field, const uint8
 QSM_API qsm_status qsm_tsvd_device(qsm_ctx* ctx, const double* d_local_field, const uint8_t* d_mask,
                            const qsm_grid* grid, const double bdir[3], const qsm_tkd_params* params,
                            double* d_out_chi);
+/* inversion::ilsqr — src/inversion/ilsqr.rs:1307-1351, returning (chi, xsa, xfs, xlsqr).
+ * out_xsa, out_xfs and out_xlsqr may be NULL when the caller does not need them.  Progress
+ * is (1,4) .. (4,4) as in the reference.  Every axis length must be >= 2 (the reference's
+ * one-sided Laplacian stencils read outside a length-1 axis). */
+QSM_API qsm_status qsm_ilsqr(qsm_ctx* ctx, const double* local_field, const uint8_t* mask, const qsm_grid* grid,
+                             const double bdir[3], const qsm_ilsqr_params* params, qsm_progress_fn progress,
+                             void* user, double* out_chi, double* out_xsa, double* out_xfs, double* out_xlsqr);
+QSM_API qsm_status qsm_ilsqr_device(qsm_ctx* ctx, const double* d_local_field, const uint8_t* d_mask,
+                                    const qsm_grid* grid, const double bdir[3], const qsm_ilsqr_params* params,
+                                    qsm_progress_fn progress, void* user, double* d_out_chi, double* d_out_xsa,
+                                    double* d_out_xfs, double* d_out_xlsqr);
 /* inversion::tikhonov — src/inversion/tikhonov.rs:62-138. */
 QSM_API qsm_status qsm_tikhonov(qsm_ctx* ctx, const double* local_field, const uint8_t* mask, const qsm_grid* grid,
                         const double bdir[3], const qsm_tikhonov_params* params, double* out_chi);
@@ -212,6 +227,7 @@ typedef struct {
   qsm_tkd_params tsvd;
   qsm_tikhonov_params tikhonov;
   qsm_tv_params tv;
+  qsm_ilsqr_params ilsqr;
 } qsm_inversion_config;
 
 /* BgRemovalAlgorithm — src/pipeline/config.rs:33-42, same variant order.  Variants
@@ -247,6 +263,15 @@ QSM_API qsm_status qsm_run_bg_removal(qsm_ctx* ctx, const double* field_ppm, siz
                               const qsm_scan_metadata* metadata, const qsm_bg_removal_config* config,
                               qsm_progress_fn progress, void* user, double* out_local_field,
                               uint8_t* out_eroded_mask);
+
+/* ------------------------------------------------------ order statistics -- */
+/* prctile (src/inversion/ilsqr.rs:937-946) of the values d_vals[i] with d_mask[i] != 0
+ * (all n values when d_mask is NULL), for each of the np percents in p; results in
+ * out[0..np) on the host.  The reference sorts the selected values; this computes the
+ * same order statistics by radix selection.  Returns 0 for an empty selection, as the
+ * reference's prctile does. */
+QSM_API qsm_status qsm_prctile_device(qsm_ctx* ctx, const double* d_vals, const uint8_t* d_mask, size_t n,
+                                      const double* p, size_t np, double* out);
 
 /* ---------------------------------------------------------- FFT primitives -- */
 /* Forward 3D transform of a real volume, returned as the full complex spectrum

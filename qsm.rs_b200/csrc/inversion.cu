@@ -198,6 +198,7 @@ void qsm_inversion_config_default(qsm_inversion_config* c) {
   qsm_tkd_params_default(&c->tsvd);
   qsm_tikhonov_params_default(&c->tikhonov);
   qsm_tv_params_default(&c->tv);
+  qsm_ilsqr_params_default(&c->ilsqr);
 }
 
 qsm_status qsm_run_dipole_inversion(qsm_ctx* ctx, const double* local_field_ppm, size_t len, const uint8_t* mask,
@@ -235,6 +236,11 @@ qsm_status qsm_run_dipole_inversion(qsm_ctx* ctx, const double* local_field_ppm,
       case QSM_INV_TV:
         with_host_io(ctx, d.n, local_field_ppm, mask, out_chi, [&](const double* f, const uint8_t* m, double* o) {
           tv_device(ctx, f, m, &g, b, &cfg->tv, progress, user, o);
+        });
+        break;
+      case QSM_INV_ILSQR:  // src/pipeline/inversion.rs:100-105: chi of the 4-tuple
+        with_host_io(ctx, d.n, local_field_ppm, mask, out_chi, [&](const double* f, const uint8_t* m, double* o) {
+          ilsqr_device(ctx, f, m, &g, b, &cfg->ilsqr, progress, user, o, nullptr, nullptr, nullptr);
         });
         break;
       case QSM_INV_TGV:

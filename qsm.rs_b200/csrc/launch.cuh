@@ -107,6 +107,38 @@ void run_x_c2r(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* spec, const Stor
   ls.done();
 }
 
+// Transform bundle for full complex spectra (complex-to-complex along x too): every
+// x column is valid, rows padded to a multiple of 4 values.
+template <typename T> Fft3<T> make_fft3_full(qsm_ctx* ctx, const GridDims& d) {
+  Fft3<T> f = make_fft3<T>(ctx, d);
+  f.g.nxh = d.nx;
+  f.g.pitch = (d.nx + 3) / 4 * 4;
+  return f;
+}
+
+// Identity pointwise hook of k_x_full.
+template <typename T> struct MidId {
+  __device__ __forceinline__ cplx_t<T> operator()(cplx_t<T> v, int, int) const { return v; }
+};
+
+// X pass over full complex rows: load -> FFT(D1) -> mid -> FFT(D2) -> store.
+template <typename T, int D1, int D2, class Load, class Mid, class Store>
+void run_x_full(qsm_ctx* ctx, const Fft3<T>& f, const Load& ld, const Mid& mid, const Store& st, const int* done,
+                const char* name) {
+  using C = cplx_t<T>;
+  if ((f.px.n + f.px.T - 1) / f.px.T > kFftEmax)
+    throw QsmError(QSM_ERR_UNSUPPORTED_SIZE, "x length outside the per-thread register budget");
+  const int Tt = x_block_t(f.px.T);
+  const int P = x_pencils_per_block<T>(f.px.T);
+  const size_t smem = (size_t)(f.px.n + P * x_rowlen<T>(f.px.n)) * sizeof(C);
+  auto kern = k_x_full<T, D1, D2, Load, Mid, Store>;
+  ensure_smem(kern, smem);
+  const long long blocks = ((long long)f.g.nrows() + P - 1) / P;
+  LaunchScope ls(ctx, name);
+  kern<<<(unsigned)blocks, dim3(Tt, P), smem, ctx->stream>>>(f.g, f.px, f.twx, ld, mid, st, done);
+  ls.done();
+}
+
 template <typename T> inline int yz_cols() { return sizeof(T) == 4 ? 16 : 8; }
 
 inline int sm_count(qsm_ctx* ctx) {
@@ -177,6 +209,25 @@ void run_yz(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst
   const unsigned grid = persistent_grid(ctx, kern, P * pl.T, smem, w.ntiles);
   LaunchScope ls(ctx, AXIS == 1 ? (DIR < 0 ? "fft_y_fwd" : "fft_y_inv") : (DIR < 0 ? "fft_z_fwd" : "fft_z_inv"));
   kern<<<grid, dim3(P, pl.T), smem, ctx->stream>>>(f.g, pl, w, tw, src, dst, op, done);
+  ls.done();
+}
+
+// Y/Z pass with an FP64 accumulation in its post hook (k_pass_yz_acc).  `partials`
+// holds at least kMaxPersistentBlocks doubles; `counter` is 0 between launches.
+constexpr int kMaxPersistentBlocks = 4096;
+template <typename T, int DIR, int AXIS, class Op>
+void run_yz_acc(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst, const Op& op,
+                double* partials, unsigned* counter, const int* done, const char* name) {
+  const FftPlan1D& pl = (AXIS == 1) ? f.py : f.pz;
+  const cplx_t<T>* tw = (AXIS == 1) ? f.twy : f.twz;
+  auto kern = k_pass_yz_acc<T, DIR, AXIS, Op>;
+  const int P = yz_tile_width<T>(kern, pl.n, pl.T);
+  const size_t smem = yz_smem<T>(pl.n, P);
+  const TileWalk w = tile_walk(f, AXIS, P);
+  unsigned grid = persistent_grid(ctx, kern, P * pl.T, smem, w.ntiles);
+  if (grid > (unsigned)kMaxPersistentBlocks) grid = kMaxPersistentBlocks;
+  LaunchScope ls(ctx, name);
+  kern<<<grid, dim3(P, pl.T), smem, ctx->stream>>>(f.g, pl, w, tw, src, dst, op, partials, counter, done);
   ls.done();
 }
 

@@ -122,6 +122,68 @@ __global__ void k_x_r2c(Geom g, const __grid_constant__ FftPlan1D pl, const cplx
 }
 
 // ---------------------------------------------------------------------------
+// X pass over full complex rows (complex-to-complex spectra: [nz][ny][pitch] with all
+// nx columns valid).  Per row: load -> FFT(D1) -> mid -> FFT(D2) -> store, where a
+// direction of 0 skips that transform.  One row per pencil; blockDim = (Tb, P).
+//   Load : C operator()(int row, int e)
+//   Mid  : C operator()(C v, int row, int e)
+//   Store: void operator()(int row, int e, C v); void finish()
+// ---------------------------------------------------------------------------
+template <typename T, int D1, int D2, class Load, class Mid, class Store>
+__global__ void k_x_full(Geom g, const __grid_constant__ FftPlan1D pl, const cplx_t<T>* __restrict__ twg, Load ld,
+                         Mid mid, Store st0, const int* __restrict__ done) {
+  using C = cplx_t<T>;
+  if (done != nullptr && *done) return;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* tw = reinterpret_cast<C*>(smraw);
+  const int n = pl.n;
+  const int rowlen = x_rowlen<T>(n);
+  C* sm = tw + n;
+  const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+  for (int i = tid; i < n; i += blockDim.x * blockDim.y) tw[i] = twg[i];
+  const int t = threadIdx.x;
+  const long long row = (long long)blockIdx.x * blockDim.y + threadIdx.y;
+  const bool active = row < g.nrows() && t < pl.T;
+  C* sp = sm + threadIdx.y * rowlen;
+  SAPadded<PadG<T>::G> sa;
+  {
+    C v[kFftEmax];
+#pragma unroll
+    for (int c = 0; c < kFftEmax; ++c) {
+      const int e = t + c * pl.T;
+      v[c] = mk<C>(T(0), T(0));
+      if (active && e < n) v[c] = ld((int)row, e);
+    }
+#pragma unroll
+    for (int c = 0; c < kFftEmax; ++c) {
+      const int e = t + c * pl.T;
+      if (active && e < n) sp[sa(e)] = v[c];
+    }
+  }
+  __syncthreads();
+  if constexpr (D1 != 0) fft_pencil<D1, C, SAPadded<PadG<T>::G>, false, false>(&pl, t, active, sp, sa, tw, nullptr, nullptr, 0, 0);
+  if (active)
+    for (int e = t; e < n; e += pl.T) sp[sa(e)] = mid(sp[sa(e)], (int)row, e);
+  __syncthreads();
+  if constexpr (D2 != 0) fft_pencil<D2, C, SAPadded<PadG<T>::G>, false, false>(&pl, t, active, sp, sa, tw, nullptr, nullptr, 0, 0);
+  Store st = st0;
+  {
+    C v[kFftEmax];
+#pragma unroll
+    for (int c = 0; c < kFftEmax; ++c) {
+      const int e = t + c * pl.T;
+      if (active && e < n) v[c] = sp[sa(e)];
+    }
+#pragma unroll
+    for (int c = 0; c < kFftEmax; ++c) {
+      const int e = t + c * pl.T;
+      if (active && e < n) st((int)row, e, v[c]);
+    }
+  }
+  st.finish();
+}
+
+// ---------------------------------------------------------------------------
 // X inverse: half spectrum -> real rows.  blockDim = (Tb, P) as for k_x_r2c.
 // A thread loads at most 9 half-spectrum entries per row (nx/2+1 <= 9T), issued as
 // one batch; the results are handed to the store functor in one unrolled batch.
@@ -290,6 +352,134 @@ __global__ void __maxnreg__(YzRegCap<T>::value)
     }
   }
   cp_async_wait<0>();
+}
+
+// ------------------------------------------------------------- reductions --
+// Sum K doubles over a block of any shape (partial last warp included); the result
+// is valid in thread 0.  Fixed order for a fixed block shape.
+template <int K> __device__ __forceinline__ void block_sum_any(double (&a)[K]) {
+  __shared__ double red[K][32];
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int nth = blockDim.x * blockDim.y * blockDim.z;
+  const int lane = tid & 31, wid = tid >> 5;
+  const int wsz = imin(32, nth - (wid << 5));
+  const unsigned m = wsz == 32 ? 0xffffffffu : ((1u << wsz) - 1u);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const double b = __shfl_down_sync(m, a[k], o);
+      if (lane + o < wsz) a[k] += b;
+    }
+  }
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < K; ++k) red[k][wid] = a[k];
+  __syncthreads();
+  const int nw = (nth + 31) >> 5;
+  if (wid == 0) {  // warp 0 itself may be partial (blocks of fewer than 32 threads)
+#pragma unroll
+    for (int k = 0; k < K; ++k) a[k] = lane < nw ? red[k][lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        const double b = __shfl_down_sync(m, a[k], o);
+        if (lane + o < wsz) a[k] += b;
+      }
+    }
+  }
+}
+
+// Deterministic grid-wide sum: every block passes its K values; the block that
+// arrives last sums the per-block partials in block order and returns true with the
+// totals valid in its thread 0.  `counter` must be 0 on entry and is reset.
+template <int K>
+__device__ __forceinline__ bool grid_sum_last(double (&a)[K], double* __restrict__ partials, unsigned* counter) {
+  __shared__ int am_last;
+  block_sum_any<K>(a);
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int nth = blockDim.x * blockDim.y * blockDim.z;
+  const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
+  const unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+  if (tid == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) partials[(size_t)bid * K + k] = a[k];
+    __threadfence();
+    const unsigned prev = atomicAdd(counter, 1u);
+    am_last = (prev == nblocks - 1);
+  }
+  __syncthreads();
+  if (!am_last) return false;
+  __threadfence();
+#pragma unroll
+  for (int k = 0; k < K; ++k) a[k] = 0.0;
+  for (unsigned b = tid; b < nblocks; b += nth)
+#pragma unroll
+    for (int k = 0; k < K; ++k) a[k] += __ldcg(&partials[(size_t)b * K + k]);
+  block_sum_any<K>(a);
+  if (tid == 0) *counter = 0u;
+  return true;
+}
+
+// Y/Z pass whose post hook also accumulates one FP64 value per element
+// (post(v, ix, iy, iz, idx, acc) returns the value to store).  The block that
+// finishes last reduces the sums and runs op.last(total) on its thread 0.
+template <typename T, int DIR, int AXIS, class Op>
+__global__ void __maxnreg__(YzRegCap<T>::value)
+    k_pass_yz_acc(Geom g, const __grid_constant__ FftPlan1D pl, TileWalk w, const cplx_t<T>* __restrict__ twg,
+                  const cplx_t<T>* src, cplx_t<T>* dst, Op op, double* __restrict__ partials, unsigned* counter,
+                  const int* __restrict__ done) {
+  using C = cplx_t<T>;
+  if (done != nullptr && *done) return;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* tw = reinterpret_cast<C*>(smraw);
+  const int n = pl.n;
+  const int P = blockDim.x;
+  C* buf0 = tw + ((n + 7) & ~7);
+  C* buf1 = buf0 + (size_t)n * P;
+  const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+  for (int i = tid; i < n; i += blockDim.x * blockDim.y) tw[i] = twg[i];
+  const int px = threadIdx.x;
+  const int t = threadIdx.y;
+  SAStrided sa{P};
+  double acc[1] = {0.0};
+  int tile = blockIdx.x;
+  if (tile < w.ntiles) issue_tile(src, buf0, g, w, tile, n, P);
+  cp_async_commit();
+  for (int it = 0; tile < w.ntiles; tile += gridDim.x, ++it) {
+    C* cur = (it & 1) ? buf1 : buf0;
+    C* nxt = (it & 1) ? buf0 : buf1;
+    const int next = tile + gridDim.x;
+    if (next < w.ntiles) issue_tile(src, nxt, g, w, next, n, P);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    const int tx = tile % w.ntx, outer = tile / w.ntx;
+    const int col = tx * P + px;
+    const bool active = col < g.nxh;
+    const long long base = col + (long long)outer * w.ostride;
+    C* sp = cur + px;
+    if (active) {
+      for (int e = t; e < n; e += pl.T) {
+        const long long idx = base + e * w.estride;
+        sp[sa(e)] = (AXIS == 1) ? op.pre(sp[sa(e)], col, e, outer, idx) : op.pre(sp[sa(e)], col, outer, e, idx);
+      }
+    }
+    __syncthreads();
+    fft_pencil<DIR, C, SAStrided, false, false>(&pl, t, active, sp, sa, tw, nullptr, nullptr, 0, 0);
+    if (active) {
+      for (int e = t; e < n; e += pl.T) {
+        const long long idx = base + e * w.estride;
+        const C v = sp[sa(e)];
+        dst[idx] = (AXIS == 1) ? op.post(v, col, e, outer, idx, acc[0]) : op.post(v, col, outer, e, idx, acc[0]);
+      }
+    }
+    __syncthreads();
+  }
+  cp_async_wait<0>();
+  if (grid_sum_last<1>(acc, partials, counter) && tid == 0) op.last(acc[0]);
 }
 
 // Real multiplier tile (same tile walk, element size sizeof(T)), 16-byte chunks.

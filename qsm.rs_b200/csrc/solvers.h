@@ -15,6 +15,10 @@ void tkd_device(qsm_ctx* ctx, const double* f, const uint8_t* m, const qsm_grid*
                 const qsm_tkd_params* p, double* out, int tsvd);
 void tikhonov_device(qsm_ctx* ctx, const double* f, const uint8_t* m, const qsm_grid* grid, const double bdir[3],
                      const qsm_tikhonov_params* p, double* out);
+// xsa, xfs, xlsqr may be null
+void ilsqr_device(qsm_ctx* ctx, const double* f, const uint8_t* m, const qsm_grid* grid, const double bdir[3],
+                  const qsm_ilsqr_params* p, qsm_progress_fn progress, void* user, double* chi, double* xsa,
+                  double* xfs, double* xlsqr);
 
 // Stage a host volume (and optional mask) on the device, run, copy the result back.
 template <class Run>

@@ -57,6 +57,10 @@ class QsmVsharpParams(C.Structure):
     _fields_ = [("threshold", C.c_double), ("max_radius", C.c_double), ("min_radius", C.c_double)]
 
 
+class QsmIlsqrParams(C.Structure):
+    _fields_ = [("tol", C.c_double), ("max_iter", C.c_size_t)]
+
+
 class QsmScanMetadata(C.Structure):
     _fields_ = [("nx", C.c_size_t), ("ny", C.c_size_t), ("nz", C.c_size_t),
                 ("vsx", C.c_double), ("vsy", C.c_double), ("vsz", C.c_double),
@@ -65,7 +69,7 @@ class QsmScanMetadata(C.Structure):
 
 class QsmInversionConfig(C.Structure):
     _fields_ = [("algorithm", C.c_int), ("tkd", QsmTkdParams), ("tsvd", QsmTkdParams),
-                ("tikhonov", QsmTikhonovParams), ("tv", QsmTvParams)]
+                ("tikhonov", QsmTikhonovParams), ("tv", QsmTvParams), ("ilsqr", QsmIlsqrParams)]
 
 
 class QsmBgRemovalConfig(C.Structure):
@@ -90,6 +94,15 @@ _SIGS = [
                                         C.POINTER(C.c_uint64), C.POINTER(C.c_double)]),
     ("qsm_grid_supported", C.c_int, [C.POINTER(QsmGrid)]),
     ("qsm_tv_params_default", None, [C.POINTER(QsmTvParams)]),
+    ("qsm_ilsqr_params_default", None, [C.POINTER(QsmIlsqrParams)]),
+    ("qsm_prctile_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, c_double_p, C.c_size_t,
+                                     c_double_p]),
+    ("qsm_ilsqr", C.c_int, [C.c_void_p, c_double_p, c_u8_p, C.POINTER(QsmGrid), c_double_p,
+                            C.POINTER(QsmIlsqrParams), PROGRESS_FN, C.c_void_p, c_double_p, c_double_p, c_double_p,
+                            c_double_p]),
+    ("qsm_ilsqr_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(QsmGrid), c_double_p,
+                                   C.POINTER(QsmIlsqrParams), PROGRESS_FN, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_void_p]),
     ("qsm_tkd_params_default", None, [C.POINTER(QsmTkdParams)]),
     ("qsm_tikhonov_params_default", None, [C.POINTER(QsmTikhonovParams)]),
     ("qsm_sharp_params_default", None, [C.POINTER(QsmSharpParams)]),

@@ -47,6 +47,17 @@ class TikhonovParams:
         return _lib.QsmTikhonovParams(self.lambda_, int(self.reg))
 
 
+@dataclass
+class IlsqrParams:
+    """src/inversion/ilsqr.rs:20-34."""
+
+    tol: float = 0.01
+    max_iter: int = 50
+
+    def _c(self):
+        return _lib.QsmIlsqrParams(self.tol, int(self.max_iter))
+
+
 def _closed(fn_name, local_field, mask, grid: Grid, bdir, params, ctx):
     c = _ctx(ctx)
     f = _as_f64(local_field, grid, "local_field")
@@ -137,4 +148,50 @@ def dipole_forward(chi, grid: Grid, bdir=(0.0, 0.0, 1.0), *, ctx: Optional[Conte
     b, _keep = _bdir(bdir)
     g = grid._c()
     _check(c, c._lib.qsm_dipole_forward(c.handle, _ptr_d(x), C.byref(g), b, _ptr_d(out)))
+    return out
+
+
+def ilsqr(local_field, mask, grid: Grid, bdir=(0.0, 0.0, 1.0), params: IlsqrParams = IlsqrParams(),
+          progress: Optional[Callable[[int, int], None]] = None, *, ctx: Optional[Context] = None):
+    """inversion::ilsqr (src/inversion/ilsqr.rs:1307-1351) -> (chi, xsa, xfs, xlsqr).
+
+    progress(step, 4) is called before each of the three steps and after the last one.
+    """
+    c = _ctx(ctx)
+    f = _as_f64(local_field, grid, "local_field")
+    m = _as_u8(mask, "mask")
+    _check_len(f, grid, "local_field")
+    _check_len(m, grid, "mask")
+    outs = [np.empty_like(f) for _ in range(4)]
+    b, _keep = _bdir(bdir)
+    g = grid._c()
+    p = params._c()
+    cb, _cbkeep = _progress(progress)
+    st = c._lib.qsm_ilsqr(c.handle, _ptr_d(f), _ptr_u8(m), C.byref(g), b, C.byref(p), cb, None,
+                          *[_ptr_d(o) for o in outs])
+    _check(c, st)
+    return tuple(outs)
+
+
+def ilsqr_device(ctx: Context, d_local_field: int, d_mask: int, grid: Grid, bdir, params: IlsqrParams,
+                 d_chi: int, d_xsa: int = 0, d_xfs: int = 0, d_xlsqr: int = 0, progress=None):
+    """Device-pointer variant; the last three outputs are optional (0 = not wanted)."""
+    b, _keep = _bdir(bdir)
+    g = grid._c()
+    p = params._c()
+    cb, _cbkeep = _progress(progress)
+    st = ctx._lib.qsm_ilsqr_device(ctx.handle, C.c_void_p(d_local_field), C.c_void_p(d_mask), C.byref(g), b,
+                                   C.byref(p), cb, None, C.c_void_p(d_chi), C.c_void_p(d_xsa or None),
+                                   C.c_void_p(d_xfs or None), C.c_void_p(d_xlsqr or None))
+    _check(ctx, st)
+
+
+def prctile_device(ctx: Context, d_vals: int, d_mask: int, n: int, percents):
+    """prctile (src/inversion/ilsqr.rs:937-946) of device values where mask != 0 (all when
+    d_mask is 0), one result per percent."""
+    p = np.ascontiguousarray(np.asarray(percents, dtype=np.float64))
+    out = np.zeros_like(p)
+    st = ctx._lib.qsm_prctile_device(ctx.handle, C.c_void_p(d_vals), C.c_void_p(d_mask or None), int(n), _ptr_d(p),
+                                     p.size, _ptr_d(out))
+    _check(ctx, st)
     return out

@@ -64,9 +64,13 @@ def test_host_only_entry_points(lib):
     k = _lib.QsmTikhonovParams()
     lib.qsm_tikhonov_params_default(C.byref(k))
     assert (k.lambda_, k.reg) == (0.01, 0)
+    il = _lib.QsmIlsqrParams()
+    lib.qsm_ilsqr_params_default(C.byref(il))
+    assert (il.tol, il.max_iter) == (0.01, 50)  # src/inversion/ilsqr.rs:27-34
     ic = _lib.QsmInversionConfig()
     lib.qsm_inversion_config_default(C.byref(ic))
     assert ic.algorithm == 4  # Rts, src/pipeline/config.rs:251
+    assert (ic.ilsqr.tol, ic.ilsqr.max_iter) == (0.01, 50)
     bc = _lib.QsmBgRemovalConfig()
     lib.qsm_bg_removal_config_default(C.byref(bc))
     assert bc.algorithm == 0  # Vsharp

@@ -234,3 +234,139 @@ def test_nyquist_symmetrised_multiplier_matches_c2c():
     # the unsymmetrised half-spectrum product would differ
     half = np.fft.irfftn(np.fft.rfftn(x) * M[:, :, :5], s=grid.shape, axes=(0, 1, 2))
     assert np.abs(half - ref).max() > 1e-3
+
+
+# ---------------------------------------------------------------------------- iLSQR --
+def test_lsqr_real_diagonal():
+    """src/inversion/ilsqr.rs:1357-1372: diag(1..10) x = 2*diag -> x = 2."""
+    d = np.arange(1, 11, dtype=np.float64)
+    x = O.lsqr_real(lambda v: v * d, lambda v: v * d, d * 2.0, 1e-10, 100)
+    assert np.all(np.abs(x - 2.0) < 1e-6)
+
+
+def test_norm_and_sign_known_answers():
+    """src/inversion/ilsqr.rs:1374-1385: norm([3,4]) = 5; sign([-2,0,3]) = [-1,0,1]."""
+    assert abs(float(np.linalg.norm([3.0, 4.0])) - 5.0) < 1e-10
+    assert list(np.sign([-2.0, 0.0, 3.0])) == [-1.0, 0.0, 1.0]
+
+
+def test_lsqr_complex_relres_stop():
+    """src/inversion/ilsqr.rs:1387-1432: diag(1,10,100,1000), tol 1e-6 -> relres <= 10*tol."""
+    d = np.array([1.0, 10.0, 100.0, 1000.0])
+    b = (d * d).astype(np.complex128)
+    x = O.lsqr_complex(lambda v: v * d, lambda v: v * d, b, 1e-6, 200)
+    assert np.linalg.norm(x * d - b) / np.linalg.norm(b) <= 1e-5
+
+
+def test_lsqr_complex_diagonal():
+    """src/inversion/ilsqr.rs:1434-1465: diag(1,2,3), x = [1+i, 2+i, 3+i]."""
+    d = np.array([1.0, 2.0, 3.0])
+    e = np.array([1 + 1j, 2 + 1j, 3 + 1j])
+    x = O.lsqr_complex(lambda v: v * d, lambda v: v * d, e * d, 1e-10, 100)
+    assert np.all(np.abs(x.real - e.real) < 1e-6) and np.all(np.abs(x.imag - e.imag) < 1e-6)
+
+
+def test_lsmr_identity():
+    """src/inversion/ilsqr.rs:1467-1492: identity, b = [3,5,7]: finite, residual < ||b||."""
+    b = np.array([3.0, 5.0, 7.0])
+    x = O.lsmr(lambda v: v.copy(), lambda v: v.copy(), b, 3, 1e-6, 1e-6, 200)
+    assert x.shape == (3,) and np.all(np.isfinite(x))
+    assert np.linalg.norm(x - b) < np.linalg.norm(b)
+    np.testing.assert_allclose(x, b, atol=1e-12)  # one iteration solves the identity exactly
+
+
+def test_prctile_linear_interpolation():
+    """src/inversion/ilsqr.rs:937-946 (MATLAB-style linear interpolation)."""
+    v = np.sort(np.array([4.0, 1.0, 3.0, 2.0, 5.0]))
+    assert O.prctile(v, 50.0) == 3.0
+    assert O.prctile(v, 10.0) == 1.4
+    assert O.prctile(v, 100.0) == 5.0
+    assert O.prctile(np.array([7.0]), 30.0) == 7.0 and O.prctile(np.array([]), 30.0) == 0.0
+    r = np.random.default_rng(0).standard_normal(1001)
+    for p in (1.0, 30.0, 60.0, 99.9):
+        assert abs(O.prctile(np.sort(r), p) - np.percentile(r, p)) < 1e-12
+
+
+def _sphere44():
+    n = 4
+    mask = np.zeros((n, n, n), np.uint8)
+    f = np.zeros((n, n, n))
+    k, j, i = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    r2 = (i - 1.5) ** 2 + (j - 1.5) ** 2 + (k - 1.5) ** 2
+    mask[r2 < 2.5] = 1
+    f[r2 < 2.5] = 5.0
+    return f, mask
+
+
+def test_laplacian_weights_known_properties():
+    """src/inversion/ilsqr.rs:1494-1536: constant field in a 4^3 sphere, weights in [0,1],
+    0 outside the mask."""
+    f, mask = _sphere44()
+    w = O.laplacian_weights_ilsqr(f, mask, g(4), 10.0, 90.0)
+    assert np.all(np.isfinite(w)) and np.all((w >= 0) & (w <= 1))
+    assert np.all(w[mask == 0] == 0.0)
+    # the Laplacian of a constant is zero everywhere, so every weight is 0 (range <= 1e-10)
+    assert np.all(O.ilsqr_laplacian(f, mask, g(4)) == 0.0)
+
+
+def test_lap1_stencils_follow_mask():
+    """src/inversion/ilsqr.rs:583-669: central / 4th-order one-sided / 2nd-order / first
+    difference chosen by the mask, checked on a 1-D profile along x."""
+    grid = O.Grid.new(8, 1, 1)
+    x = np.arange(8, dtype=np.float64)
+    f = (x ** 3).reshape(1, 1, 8)
+    m = np.ones((1, 1, 8), np.uint8)
+    lap = O._lap1_axis(f, m, 2, 1.0).ravel()
+    # interior central difference of x^3 is 6x; the ends use the 4th-order one-sided forms
+    np.testing.assert_allclose(lap[1:7], 6.0 * x[1:7])
+    assert lap[0] == 2 * 0 - 5 * 1 + 4 * 8 - 27 and lap[7] == -(4 ** 3) + 4 * 125 - 5 * 216 + 2 * 343
+    m2 = m.copy()
+    m2[0, 0, 5] = 0  # voxel 4 loses its forward neighbour: backward 4th order
+    lap2 = O._lap1_axis(f, m2, 2, 1.0).ravel()
+    assert lap2[4] == -(1 ** 3) + 4 * 8 - 5 * 27 + 2 * 64
+    assert grid.n_total() == 8
+
+
+def test_dipole_kspace_weights_known_properties():
+    """src/inversion/ilsqr.rs:1538-1559."""
+    d = np.array([0.0, 0.01, 0.1, 0.3, 0.5, 0.7, 1.0, -0.5, -1.0, 0.0])
+    w = O.dipole_kspace_weights_ilsqr(d, 1.0, 1.0, 90.0)
+    assert np.all((w >= 0) & (w <= 1))
+    assert w[0] <= 1e-10 and w[6] > 0.5 and w[8] > 0.5
+
+
+def test_gradient_weights_known_properties():
+    """src/inversion/ilsqr.rs:1561-1600: linear field in x, full mask."""
+    n = 4
+    f = np.tile(np.arange(n, dtype=np.float64), (n, n, 1))
+    mask = np.ones((n, n, n), np.uint8)
+    gx, gy, gz = O.fgrad_masked(f, mask, g(n))
+    for comp in (gx, gy, gz):
+        w = O._percentile_weights(comp, mask, 10.0, 90.0, True)
+        assert np.all(np.isfinite(w)) and np.all((w >= 0) & (w <= 1))
+    assert np.all(gx == 1.0) and np.all(gy == 0.0) and np.all(gz == 0.0)
+
+
+def ilsqr_small_case():
+    """The 8^3 sphere case of src/inversion/ilsqr.rs:1602-1681."""
+    n = 8
+    c = (n - 1) / 2.0
+    k, j, i = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    di, dj, dk = i - c, j - c, k - c
+    r2 = di * di + dj * dj + dk * dk
+    mask = (r2 < 9.0).astype(np.uint8)
+    field = np.where(mask > 0, 0.01 * (dk * dk - di * di - dj * dj) / (r2 + 1.0), 0.0)
+    return field, mask
+
+
+def test_ilsqr_small():
+    """src/inversion/ilsqr.rs:1602-1681: finite, zero outside the mask, not all zero inside."""
+    field, mask = ilsqr_small_case()
+    seen = []
+    chi, xsa, xfs, xlsqr = O.ilsqr(field, mask, g(8), (0, 0, 1), O.IlsqrParams(0.1, 5),
+                                   progress=lambda a, b: seen.append((a, b)))
+    assert chi.shape == field.shape and np.all(np.isfinite(chi))
+    assert np.all(chi[mask == 0] == 0.0)
+    assert np.abs(chi[mask > 0]).sum() > 0.0
+    assert seen == [(1, 4), (2, 4), (3, 4), (4, 4)]  # src/inversion/ilsqr.rs:1324-1343
+    np.testing.assert_array_equal(chi, np.where(mask > 0, xlsqr - xsa, 0.0))
