@@ -98,6 +98,13 @@ typedef struct { double lambda; int reg; } qsm_tikhonov_params;
 typedef struct { double threshold, radius; } qsm_sharp_params;
 /* VsharpParams — src/bgremove/vsharp.rs:22-40 (0.05, 12.0, 1.0). */
 typedef struct { double threshold, max_radius, min_radius; } qsm_vsharp_params;
+/* TgvParams — src/inversion/tgv.rs:39-76 (alpha1 5e-4, alpha0 1.5e-3, 1000 iterations,
+ * 3 erosions, step 3, 3 T, TE 20 ms, tol 1e-5); single precision like the reference. */
+typedef struct {
+  float alpha1, alpha0;
+  size_t iterations, erosions;
+  float step_size, fieldstrength, te, tol;
+} qsm_tgv_params;
 /* IlsqrParams — src/inversion/ilsqr.rs:20-34 (tol 0.01, max_iter 50: the LSMR step's
  * tolerance and iteration cap). */
 typedef struct { double tol; size_t max_iter; } qsm_ilsqr_params;
@@ -108,6 +115,7 @@ QSM_API void qsm_tikhonov_params_default(qsm_tikhonov_params* p);
 QSM_API void qsm_sharp_params_default(qsm_sharp_params* p);
 QSM_API void qsm_vsharp_params_default(qsm_vsharp_params* p);
 QSM_API void qsm_ilsqr_params_default(qsm_ilsqr_params* p);
+QSM_API void qsm_tgv_params_default(qsm_tgv_params* p);
 
 /* -------------------------------------------------------- dipole inversion -- */
 /* inversion::tv_admm — src/inversion/tv.rs:63-97 (+ admm.rs:76-178). */
@@ -156,6 +164,21 @@ QSM_API qsm_status qsm_ilsqr_device(qsm_ctx* ctx, const double* d_local_field, c
                                     const qsm_grid* grid, const double bdir[3], const qsm_ilsqr_params* params,
                                     qsm_progress_fn progress, void* user, double* d_out_chi, double* d_out_xsa,
                                     double* d_out_xfs, double* d_out_xlsqr);
+/* inversion::tgv_qsm — src/inversion/tgv.rs:1045-1299: susceptibility (ppm) from WRAPPED
+ * phase, parameters before the field direction as in the reference.  Progress is
+ * (iter, iterations) for every iteration started, then (final_iter, iterations).  The
+ * iterations always run in float (the reference's arithmetic), whatever the context's
+ * precision.  A mask that is empty after the erosions returns QSM_ERR_INVALID_ARGUMENT
+ * (the reference panics on it). */
+QSM_API qsm_status qsm_tgv_qsm(qsm_ctx* ctx, const double* phase, const uint8_t* mask, const qsm_grid* grid,
+                               const qsm_tgv_params* params, const double b0_dir[3], qsm_progress_fn progress,
+                               void* user, double* out_chi);
+QSM_API qsm_status qsm_tgv_qsm_device(qsm_ctx* ctx, const double* d_phase, const uint8_t* d_mask,
+                                      const qsm_grid* grid, const qsm_tgv_params* params, const double b0_dir[3],
+                                      qsm_progress_fn progress, void* user, double* d_out_chi);
+/* inversion::tgv::compute_oblique_stencil — src/inversion/tgv.rs:272-479 (host only):
+ * out_stencil[(di*3 + dj)*3 + dk] for offsets di, dj, dk in {-1, 0, 1} shifted by one. */
+QSM_API qsm_status qsm_tgv_oblique_stencil(const double res[3], const double b0_dir[3], float out_stencil[27]);
 /* inversion::tikhonov — src/inversion/tikhonov.rs:62-138. */
 QSM_API qsm_status qsm_tikhonov(qsm_ctx* ctx, const double* local_field, const uint8_t* mask, const qsm_grid* grid,
                         const double bdir[3], const qsm_tikhonov_params* params, double* out_chi);

@@ -940,3 +940,403 @@ def ilsqr(field_, mask, grid: Grid, bdir, params: IlsqrParams = IlsqrParams(), p
         progress(4, 4)
     chi = np.where(m != 0, xlsqr - xsa, 0.0)
     return chi, xsa, xfs, xlsqr
+
+
+# ---------------------------------------------------------------------------
+# TGV-QSM (src/inversion/tgv.rs), single precision like the reference
+# ---------------------------------------------------------------------------
+F32 = np.float32
+
+
+@dataclass
+class TgvParams:  # src/inversion/tgv.rs:39-76
+    alpha1: float = 0.0005
+    alpha0: float = 0.0015
+    iterations: int = 1000
+    erosions: int = 3
+    step_size: float = 3.0
+    fieldstrength: float = 3.0
+    te: float = 0.020
+    tol: float = 1e-5
+
+
+def erode_mask(mask: np.ndarray, iterations: int = 1) -> np.ndarray:
+    """6-connected erosion, boundary voxels removed (src/utils/mask.rs:59-92)."""
+    cur = (np.asarray(mask) != 0).astype(np.uint8)
+    for _ in range(iterations):
+        keep = cur.copy()
+        inner = np.zeros_like(cur, dtype=bool)
+        inner[1:-1, 1:-1, 1:-1] = True
+        nb = np.ones_like(cur, dtype=bool)
+        for ax in range(3):
+            for sh in (1, -1):
+                nb &= np.roll(cur, sh, axis=ax) != 0
+        keep[(cur != 0) & ~(inner & nb)] = 0
+        cur = keep
+    return cur
+
+
+def tgv_bounding_box(mask: np.ndarray, padding: int):
+    """BoundingBox::from_mask (src/inversion/tgv.rs:110-144): (lo, hi) per axis in (x, y, z)."""
+    nz, ny, nx = mask.shape
+    idx = np.nonzero(mask)
+    if len(idx[0]) == 0:
+        lo = [nx, ny, nz]
+        hi = [0, 0, 0]
+    else:
+        lo = [int(idx[2].min()), int(idx[1].min()), int(idx[0].min())]
+        hi = [int(idx[2].max()), int(idx[1].max()), int(idx[0].max())]
+    dims = (nx, ny, nz)
+    lo = [max(v - padding, 0) for v in lo]
+    hi = [min(v + padding + 1, d) for v, d in zip(hi, dims)]
+    return lo, hi
+
+
+def _dst_sin_table(n):
+    """src/inversion/tgv.rs:481-491."""
+    scale = math.pi / (n + 1.0)
+    j = np.arange(n, dtype=np.float64) + 1.0
+    return np.sin(np.outer(j, j) * scale)
+
+
+def _dst3d(a, s):
+    """Separable DST-I along x, y, z (src/inversion/tgv.rs:494-540); a is (z, y, x)."""
+    a = np.einsum("zyj,jk->zyk", a, s)
+    a = np.einsum("zjx,jk->zkx", a, s)
+    return np.einsum("jyx,jk->kyx", a, s)
+
+
+def _jacobi_pinv_solve(g, h):
+    """solve_symmetric_pseudoinverse (src/inversion/tgv.rs:558-654): cyclic Jacobi, then
+    eigenvalues below 1e-10 * max |lambda| dropped."""
+    n = len(h)
+    a = [list(map(float, row)) for row in g]
+    v = [[1.0 if i == j else 0.0 for j in range(n)] for i in range(n)]
+    for _ in range(100):
+        max_off = 0.0
+        for i in range(n):
+            for j in range(i + 1, n):
+                max_off = max(max_off, abs(a[i][j]))
+        if max_off < 1e-15:
+            break
+        for p in range(n):
+            for q in range(p + 1, n):
+                if abs(a[p][q]) < 1e-15:
+                    continue
+                app, aqq, apq = a[p][p], a[q][q], a[p][q]
+                tau = (aqq - app) / (2.0 * apq)
+                t = 1.0 / (tau + math.sqrt(1.0 + tau * tau)) if tau >= 0.0 else -1.0 / (-tau + math.sqrt(1.0 + tau * tau))
+                c = 1.0 / math.sqrt(1.0 + t * t)
+                s = t * c
+                for i in range(n):
+                    if i == p or i == q:
+                        continue
+                    aip, aiq = a[i][p], a[i][q]
+                    a[i][p] = c * aip - s * aiq
+                    a[p][i] = a[i][p]
+                    a[i][q] = s * aip + c * aiq
+                    a[q][i] = a[i][q]
+                a[p][p] = c * c * app - 2.0 * c * s * apq + s * s * aqq
+                a[q][q] = s * s * app + 2.0 * c * s * apq + c * c * aqq
+                a[p][q] = 0.0
+                a[q][p] = 0.0
+                for i in range(n):
+                    vip, viq = v[i][p], v[i][q]
+                    v[i][p] = c * vip - s * viq
+                    v[i][q] = s * vip + c * viq
+    ev = [a[i][i] for i in range(n)]
+    thr = 1e-10 * max(abs(e) for e in ev)
+    vth = [sum(v[j][i] * h[j] for j in range(n)) for i in range(n)]
+    vth = [vth[i] / ev[i] if abs(ev[i]) > thr else 0.0 for i in range(n)]
+    return [sum(v[i][j] * vth[j] for j in range(n)) for i in range(n)]
+
+
+def tgv_oblique_stencil(res, b0):
+    """compute_oblique_stencil (src/inversion/tgv.rs:272-479): least-squares fit of 13
+    centrosymmetric stencil pairs to the dipole field on a 64^3 grid through DST-I
+    Poisson solves, resolution-weighted, centre = -sum(others).  Returns st[di][dj][dk]
+    as float32."""
+    n, mid = 64, 32
+    dx, dy, dz = (float(F32(r)) for r in res)
+    bf = [F32(c) for c in b0]
+    bn = math.sqrt(float(bf[0] * bf[0] + bf[1] * bf[1] + bf[2] * bf[2]))  # f32 sum, f64 sqrt
+    bd = (float(bf[0]) / bn, float(bf[1]) / bn, float(bf[2]) / bn)
+    z, y, x = np.meshgrid(np.arange(n) - mid, np.arange(n) - mid, np.arange(n) - mid, indexing="ij")
+    x, y, z = x.astype(np.float64), y.astype(np.float64), z.astype(np.float64)
+    r = np.sqrt(x * x + y * y + z * z)
+    valid = r >= 4.0
+    with np.errstate(invalid="ignore", divide="ignore"):
+        xz = (bd[0] * x + bd[1] * y + bd[2] * z) / r
+        kappa = (3.0 * xz * xz - 1.0) / (4.0 * math.pi * r * r * r)
+    c2 = (2.0 * np.sin(math.pi * (np.arange(n) + 1.0) / (2.0 * (n + 1.0)))) ** 2
+    lam = c2[None, None, :] + c2[None, :, None] + c2[:, None, None]
+    s = _dst_sin_table(n)
+    iscale = (2.0 / (n + 1.0)) ** 3
+    pos = [(di, dj, dk) for dk in (-1, 0, 1) for dj in (-1, 0, 1) for di in (-1, 0, 1) if (di, dj, dk) != (0, 0, 0)]
+    rows = []
+    for p in range(13):
+        di, dj, dk = pos[p]
+        delta = np.zeros((n, n, n))
+        delta[mid + dk, mid + dj, mid + di] = 1.0
+        delta[mid - dk, mid - dj, mid - di] += 1.0
+        delta[mid, mid, mid] = -2.0
+        fd = _dst3d(delta, s) / -lam
+        rows.append(_dst3d(fd, s)[valid] * iscale)
+    dv = kappa[valid]
+    g = [[float(np.dot(rows[i], rows[j])) for j in range(13)] for i in range(13)]
+    h = [float(np.dot(rows[i], dv)) for i in range(13)]
+    yv = _jacobi_pinv_solve(g, h)
+    st = np.zeros((3, 3, 3), dtype=F32)
+    for p in range(13):
+        di, dj, dk = pos[p]
+        st[di + 1, dj + 1, dk + 1] = F32(yv[p])
+        di2, dj2, dk2 = pos[25 - p]
+        st[di2 + 1, dj2 + 1, dk2 + 1] = F32(yv[p])
+    for dk in (-1, 0, 1):
+        for dj in (-1, 0, 1):
+            for di in (-1, 0, 1):
+                if (di, dj, dk) == (0, 0, 0):
+                    continue
+                i2, j2, k2 = di * di, dj * dj, dk * dk
+                w = (i2 / (dx * dx) + j2 / (dy * dy) + k2 / (dz * dz)) / (i2 + j2 + k2)
+                st[di + 1, dj + 1, dk + 1] = F32(st[di + 1, dj + 1, dk + 1] * F32(w))
+    total = F32(0.0)
+    for dk in range(3):
+        for dj in range(3):
+            for di in range(3):
+                if not (di == 1 and dj == 1 and dk == 1):
+                    total = F32(total + st[di, dj, dk])
+    st[1, 1, 1] = -total
+    return st
+
+
+def _tgv_lap_neumann(a, mask, h2):
+    """apply_laplacian_inplace (src/inversion/tgv.rs:780-824): Neumann BC, 0 outside the mask."""
+    hx2, hy2, hz2 = h2
+    two = F32(2.0)
+
+    def nb(axis, sh):
+        b = np.roll(a, sh, axis=axis)
+        edge = [slice(None)] * 3
+        edge[axis] = 0 if sh == 1 else -1
+        b[tuple(edge)] = a[tuple(edge)]
+        return b
+
+    out = (hx2 * (nb(2, 1) - two * a + nb(2, -1)) + hy2 * (nb(1, 1) - two * a + nb(1, -1))
+           + hz2 * (nb(0, 1) - two * a + nb(0, -1)))
+    return np.where(mask != 0, out, F32(0)).astype(F32)
+
+
+def _tgv_apply_stencil(x, st, mask):
+    """apply_stencil (src/inversion/tgv.rs:667-713): 27-point, 0 outside the mask and on the
+    sub-volume's faces; summed in dk, dj, di order."""
+    nz, ny, nx = x.shape
+    out = np.zeros_like(x)
+    if nz < 3 or ny < 3 or nx < 3:
+        return out
+    acc = np.zeros((nz - 2, ny - 2, nx - 2), dtype=F32)
+    for dk in range(3):
+        for dj in range(3):
+            for di in range(3):
+                acc = (acc + st[di, dj, dk] * x[dk:nz - 2 + dk, dj:ny - 2 + dj, di:nx - 2 + di]).astype(F32)
+    out[1:-1, 1:-1, 1:-1] = acc
+    return np.where(mask != 0, out, F32(0)).astype(F32)
+
+
+def _fgrad_f32(x, h):
+    """fgrad_inplace_f32 (src/utils/gradient.rs:222-257): forward differences, 0 on the last slice."""
+    out = []
+    for axis, hh in ((2, h[0]), (1, h[1]), (0, h[2])):
+        g = np.zeros_like(x)
+        sl = [slice(None)] * 3
+        sp = [slice(None)] * 3
+        sl[axis] = slice(0, -1)
+        sp[axis] = slice(1, None)
+        g[tuple(sl)] = (x[tuple(sp)] - x[tuple(sl)]) * hh
+        out.append(g)
+    return out
+
+
+def _bwd(a, axis):
+    """a[i-1] along axis with 0 for i = 0."""
+    b = np.zeros_like(a)
+    sl = [slice(None)] * 3
+    sp = [slice(None)] * 3
+    sl[axis] = slice(1, None)
+    sp[axis] = slice(0, -1)
+    b[tuple(sl)] = a[tuple(sp)]
+    return b
+
+
+def _symgrad_f32(wx, wy, wz, h):
+    """symgrad_inplace_f32 (src/utils/gradient.rs:300-372)."""
+    half = F32(0.5)
+    dxx, dyx, dzx = _fgrad_f32(wx, h)  # d/dx, d/dy, d/dz of wx
+    dxy, dyy, dzy = _fgrad_f32(wy, h)
+    dxz, dyz, dzz = _fgrad_f32(wz, h)
+    sxx = dxx
+    sxy = (dxy * half + dyx * half).astype(F32)
+    sxz = (dxz * half + dzx * half).astype(F32)
+    syy = dyy
+    syz = (dyz * half + dzy * half).astype(F32)
+    szz = dzz
+    return sxx, sxy, sxz, syy, syz, szz
+
+
+def _symdiv_f32(sxx, sxy, sxz, syy, syz, szz, h):
+    """symdiv_inplace_f32 (src/utils/gradient.rs:380-432): backward differences, zero BC."""
+    hx, hy, hz = h
+
+    def row(a, b, c):
+        return ((a - _bwd(a, 2)) * hx + (b - _bwd(b, 1)) * hy + (c - _bwd(c, 0)) * hz).astype(F32)
+
+    return row(sxx, sxy, sxz), row(sxy, syy, syz), row(sxz, syz, szz)
+
+
+def _bdiv_masked_f32(gx, gy, gz, mask, h):
+    """bdiv_masked_inplace_f32 (src/utils/gradient.rs:497-565)."""
+    m = (mask != 0).astype(F32)
+    hx, hy, hz = h
+    tx = m * gx * hx - _bwd(m, 2) * _bwd(gx, 2) * hx
+    ty = m * gy * hy - _bwd(m, 1) * _bwd(gy, 1) * hy
+    tz = m * gz * hz - _bwd(m, 0) * _bwd(gz, 0) * hz
+    return np.where(mask != 0, (tx + ty + tz), F32(0)).astype(F32)
+
+
+def tgv_qsm(phase, mask, grid: Grid, params: TgvParams = TgvParams(), b0=(0.0, 0.0, 1.0), progress=None):
+    """tgv_qsm (src/inversion/tgv.rs:1045-1299) in float32."""
+    ph = _vol(phase, grid).astype(F32)
+    m_in = _vol(mask, grid, np.uint8)
+    vs = tuple(F32(v) for v in grid.voxel_size)
+    b0f = tuple(F32(v) for v in b0)
+    me = m_in.copy()
+    for _ in range(params.erosions):
+        me = erode_mask(me, 1)
+    m0 = erode_mask(me, 1)
+    lo, hi = tgv_bounding_box(m0, 2)
+    sl = (slice(lo[2], hi[2]), slice(lo[1], hi[1]), slice(lo[0], hi[0]))
+    phs, m0s, mes = ph[sl], m0[sl], me[sl]
+    hx2, hy2, hz2 = (F32(1.0) / (v * v) for v in vs)
+    h = tuple(F32(1.0) / v for v in vs)
+    # compute_phase_laplacian (tgv.rs:716-738) with the clamped 7-point Laplacian (:741-777)
+    sp, cp = np.sin(phs).astype(F32), np.cos(phs).astype(F32)
+    centre = F32(-2.0) * (hx2 + hy2 + hz2)
+
+    def lap_clamped(a):
+        def nb(axis, sh):
+            b = np.roll(a, sh, axis=axis)
+            edge = [slice(None)] * 3
+            edge[axis] = 0 if sh == 1 else -1
+            b[tuple(edge)] = a[tuple(edge)]
+            return b
+        return (centre * a + hx2 * (nb(2, 1) + nb(2, -1)) + hy2 * (nb(1, 1) + nb(1, -1))
+                + hz2 * (nb(0, 1) + nb(0, -1))).astype(F32)
+
+    lphi = np.where(m0s != 0, lap_clamped(sp) * cp - lap_clamped(cp) * sp, F32(0)).astype(F32)
+    cnt = int((m0s != 0).sum())
+    if cnt > 0:
+        s = F32(0.0)
+        for v in lphi[m0s != 0]:
+            s = F32(s + v)
+        mean = F32(s / F32(cnt))
+        lphi = np.where(m0s != 0, lphi - mean, lphi).astype(F32)
+    st = tgv_oblique_stencil(vs, b0f)
+    gns = F32(4.0) * (F32(1.0) / (vs[0] * vs[0]) + F32(1.0) / (vs[1] * vs[1]) + F32(1.0) / (vs[2] * vs[2]))
+    gn = F32(np.sqrt(gns))
+    wave = F32(0.0)
+    for v in st.ravel():  # [[[f32; 3]; 3]; 3] flattened with the last index fastest
+        wave = F32(wave + abs(v))
+    ns = _tgv_operator_norm_sqr(gn, gns, wave)
+    tau = F32(F32(1.0) / F32(np.sqrt(ns)))
+    sigma = tau
+    sstep, tstep = F32(sigma * F32(params.step_size)), F32(tau * F32(params.step_size))
+    a0, a1 = F32(params.alpha0), F32(params.alpha1)
+    shp = lphi.shape
+    z = lambda: np.zeros(shp, F32)
+    chi, chi_, chi_prev, phi, phi_ = z(), z(), z(), z(), z()
+    w = [z(), z(), z()]
+    w_ = [z(), z(), z()]
+    eta = z()
+    p = [z(), z(), z()]
+    q = [z() for _ in range(6)]
+    in0, inm = m0s != 0, mes != 0
+    final_iter = params.iterations
+    for it in range(params.iterations):
+        if progress:
+            progress(it, params.iterations)
+        if it > 0 and it % 100 == 0:
+            d = F32(0.0)
+            nrm = F32(0.0)
+            for a, b in zip(chi[in0], chi_prev[in0]):
+                dd = F32(a - b)
+                d = F32(d + dd * dd)
+                nrm = F32(nrm + a * a)
+            rc = F32(np.sqrt(d / nrm)) if nrm > 1e-10 else F32(1.0)
+            if rc < F32(params.tol):
+                final_iter = it
+                break
+            chi_prev = chi.copy()
+        t1 = _tgv_lap_neumann(phi_, m0s, (hx2, hy2, hz2))
+        t2 = _tgv_apply_stencil(chi_, st, m0s)
+        eta = np.where(in0, eta + sigma * (-t1 + t2 - lphi), eta).astype(F32)
+        g = _fgrad_f32(chi_, h)
+        s0 = np.where(in0, sstep, F32(0)).astype(F32)
+        s1 = np.where(inm, sstep, F32(0)).astype(F32)
+        upd = in0 | inm
+        for c in range(3):
+            p[c] = np.where(upd, p[c] + (s0 * g[c] - s1 * w_[c]), p[c]).astype(F32)
+        nrm3 = np.sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]).astype(F32)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            sc = np.where(upd & (nrm3 > a1), a1 / nrm3, F32(1.0)).astype(F32)
+        for c in range(3):
+            p[c] = np.where(upd & (nrm3 > a1), p[c] * sc, p[c]).astype(F32)
+        sg = _symgrad_f32(w_[0], w_[1], w_[2], h)
+        for c in range(6):
+            q[c] = np.where(in0, q[c] + sstep * sg[c], q[c]).astype(F32)
+        fro = np.sqrt(q[0] * q[0] + q[3] * q[3] + q[5] * q[5]
+                      + F32(2.0) * (q[1] * q[1] + q[2] * q[2] + q[4] * q[4])).astype(F32)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            sc = np.where(in0 & (fro > a0), a0 / fro, F32(1.0)).astype(F32)
+        for c in range(6):
+            q[c] = np.where(in0 & (fro > a0), q[c] * sc, q[c]).astype(F32)
+        phi, phi_ = phi_, phi
+        chi, chi_ = chi_, chi
+        w, w_ = w_, w
+        t1 = np.where(in0, eta, F32(0)).astype(F32)
+        t2 = _tgv_lap_neumann(t1, m0s, (hx2, hy2, hz2))
+        den = (F32(1.0) + np.where(inm, tau, F32(0))).astype(F32)
+        phi = ((phi_ + tau * t2) / den).astype(F32)
+        t1 = _bdiv_masked_f32(p[0], p[1], p[2], m0s, h)
+        t2 = _tgv_apply_stencil(np.where(in0, eta, F32(0)).astype(F32), st, m0s)
+        chi = (chi_ + tstep * (t1 - t2)).astype(F32)
+        qm = [np.where(in0, qc, F32(0)).astype(F32) for qc in q]
+        dq = _symdiv_f32(*qm, h)
+        w = [np.where(inm, w_[c] + tstep * (p[c] + dq[c]), w_[c]).astype(F32) for c in range(3)]
+        phi_ = (F32(2.0) * phi - phi_).astype(F32)
+        chi_ = (F32(2.0) * chi - chi_).astype(F32)
+        w_ = [(F32(2.0) * w[c] - w_[c]).astype(F32) for c in range(3)]
+    if progress:
+        progress(final_iter, params.iterations)
+    gamma = F32(42.5781)
+    scale = F32(F32(1.0) / (F32(2.0) * F32(math.pi) * F32(params.te) * F32(params.fieldstrength) * gamma))
+    out = np.zeros(grid.shape, dtype=F32)
+    out[sl] = np.where(inm, chi * scale, F32(0))
+    return out.astype(np.float64)
+
+
+def _tgv_operator_norm_sqr(g, g2, w):
+    """compute_operator_norm_sqr (src/inversion/tgv.rs:839-876): 20 power iterations in f32."""
+    g4, g2w, g2w2, g21 = F32(g2 * g2), F32(g2 * w), F32(g2 + w * w), F32(g2 + F32(1.0))
+    v = [F32(1.0)] * 3
+    for _ in range(20):
+        y0 = F32(g4 * v[0] + g2w * v[1])
+        y1 = F32(g2w * v[0] + g2w2 * v[1] + g * v[2])
+        y2 = F32(g * v[1] + g21 * v[2])
+        nrm = F32(np.sqrt(F32(y0 * y0 + y1 * y1 + y2 * y2)))
+        if nrm < 1e-10:
+            break
+        v = [F32(y0 / nrm), F32(y1 / nrm), F32(y2 / nrm)]
+    y0 = F32(g4 * v[0] + g2w * v[1])
+    y1 = F32(g2w * v[0] + g2w2 * v[1] + g * v[2])
+    y2 = F32(g * v[1] + g21 * v[2])
+    return F32(v[0] * y0 + v[1] * y1 + v[2] * y2)

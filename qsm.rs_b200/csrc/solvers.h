@@ -19,6 +19,8 @@ void tikhonov_device(qsm_ctx* ctx, const double* f, const uint8_t* m, const qsm_
 void ilsqr_device(qsm_ctx* ctx, const double* f, const uint8_t* m, const qsm_grid* grid, const double bdir[3],
                   const qsm_ilsqr_params* p, qsm_progress_fn progress, void* user, double* chi, double* xsa,
                   double* xfs, double* xlsqr);
+void tgv_device(qsm_ctx* ctx, const double* phase, const uint8_t* mask, const qsm_grid* grid, const qsm_tgv_params* p,
+                const double b0[3], qsm_progress_fn progress, void* user, double* out);
 
 // Stage a host volume (and optional mask) on the device, run, copy the result back.
 template <class Run>

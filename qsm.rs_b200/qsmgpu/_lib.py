@@ -61,6 +61,11 @@ class QsmIlsqrParams(C.Structure):
     _fields_ = [("tol", C.c_double), ("max_iter", C.c_size_t)]
 
 
+class QsmTgvParams(C.Structure):
+    _fields_ = [("alpha1", C.c_float), ("alpha0", C.c_float), ("iterations", C.c_size_t), ("erosions", C.c_size_t),
+                ("step_size", C.c_float), ("fieldstrength", C.c_float), ("te", C.c_float), ("tol", C.c_float)]
+
+
 class QsmScanMetadata(C.Structure):
     _fields_ = [("nx", C.c_size_t), ("ny", C.c_size_t), ("nz", C.c_size_t),
                 ("vsx", C.c_double), ("vsy", C.c_double), ("vsz", C.c_double),
@@ -95,6 +100,12 @@ _SIGS = [
     ("qsm_grid_supported", C.c_int, [C.POINTER(QsmGrid)]),
     ("qsm_tv_params_default", None, [C.POINTER(QsmTvParams)]),
     ("qsm_ilsqr_params_default", None, [C.POINTER(QsmIlsqrParams)]),
+    ("qsm_tgv_params_default", None, [C.POINTER(QsmTgvParams)]),
+    ("qsm_tgv_qsm", C.c_int, [C.c_void_p, c_double_p, c_u8_p, C.POINTER(QsmGrid), C.POINTER(QsmTgvParams),
+                              c_double_p, PROGRESS_FN, C.c_void_p, c_double_p]),
+    ("qsm_tgv_qsm_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(QsmGrid),
+                                     C.POINTER(QsmTgvParams), c_double_p, PROGRESS_FN, C.c_void_p, C.c_void_p]),
+    ("qsm_tgv_oblique_stencil", C.c_int, [c_double_p, c_double_p, C.POINTER(C.c_float)]),
     ("qsm_prctile_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, c_double_p, C.c_size_t,
                                      c_double_p]),
     ("qsm_ilsqr", C.c_int, [C.c_void_p, c_double_p, c_u8_p, C.POINTER(QsmGrid), c_double_p,

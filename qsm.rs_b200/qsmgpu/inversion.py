@@ -195,3 +195,63 @@ def prctile_device(ctx: Context, d_vals: int, d_mask: int, n: int, percents):
                                      p.size, _ptr_d(out))
     _check(ctx, st)
     return out
+
+
+@dataclass
+class TgvParams:
+    """src/inversion/tgv.rs:39-76."""
+
+    alpha1: float = 0.0005
+    alpha0: float = 0.0015
+    iterations: int = 1000
+    erosions: int = 3
+    step_size: float = 3.0
+    fieldstrength: float = 3.0
+    te: float = 0.020
+    tol: float = 1e-5
+
+    def _c(self):
+        return _lib.QsmTgvParams(self.alpha1, self.alpha0, int(self.iterations), int(self.erosions), self.step_size,
+                                 self.fieldstrength, self.te, self.tol)
+
+
+def tgv_qsm(phase, mask, grid: Grid, params: TgvParams = TgvParams(), b0_dir=(0.0, 0.0, 1.0),
+            progress: Optional[Callable[[int, int], None]] = None, *, ctx: Optional[Context] = None):
+    """inversion::tgv_qsm (src/inversion/tgv.rs:1045-1299): chi (ppm) from wrapped phase.
+    Parameters come before the field direction, as in the reference."""
+    c = _ctx(ctx)
+    f = _as_f64(phase, grid, "phase")
+    m = _as_u8(mask, "mask")
+    _check_len(f, grid, "phase")
+    _check_len(m, grid, "mask")
+    out = np.empty_like(f)
+    b, _keep = _bdir(b0_dir)
+    g = grid._c()
+    p = params._c()
+    cb, _cbkeep = _progress(progress)
+    st = c._lib.qsm_tgv_qsm(c.handle, _ptr_d(f), _ptr_u8(m), C.byref(g), C.byref(p), b, cb, None, _ptr_d(out))
+    _check(c, st)
+    return out
+
+
+def tgv_qsm_device(ctx: Context, d_phase: int, d_mask: int, grid: Grid, params: TgvParams, b0_dir, d_out: int,
+                   progress=None):
+    b, _keep = _bdir(b0_dir)
+    g = grid._c()
+    p = params._c()
+    cb, _cbkeep = _progress(progress)
+    st = ctx._lib.qsm_tgv_qsm_device(ctx.handle, C.c_void_p(d_phase), C.c_void_p(d_mask), C.byref(g), C.byref(p), b,
+                                     cb, None, C.c_void_p(d_out))
+    _check(ctx, st)
+
+
+def tgv_oblique_stencil(res=(1.0, 1.0, 1.0), b0_dir=(0.0, 0.0, 1.0)):
+    """compute_oblique_stencil (src/inversion/tgv.rs:272-479) -> float32 array st[di, dj, dk]."""
+    from . import _lib as L
+    lib = L.load()
+    r = (C.c_double * 3)(*res)
+    b = (C.c_double * 3)(*b0_dir)
+    out = (C.c_float * 27)()
+    if lib.qsm_tgv_oblique_stencil(r, b, out) != 0:
+        raise RuntimeError("qsm_tgv_oblique_stencil failed")
+    return np.frombuffer(out, dtype=np.float32).reshape(3, 3, 3).copy()

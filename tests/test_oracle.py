@@ -370,3 +370,67 @@ def test_ilsqr_small():
     assert np.abs(chi[mask > 0]).sum() > 0.0
     assert seen == [(1, 4), (2, 4), (3, 4), (4, 4)]  # src/inversion/ilsqr.rs:1324-1343
     np.testing.assert_array_equal(chi, np.where(mask > 0, xlsqr - xsa, 0.0))
+
+
+# ------------------------------------------------------------------------------ TGV --
+def test_tgv_erode_mask():
+    """src/inversion/tgv.rs:1335-1347: 5^3 all-ones mask, one erosion keeps the centre."""
+    e = O.erode_mask(np.ones((5, 5, 5), np.uint8), 1)
+    assert e[2, 2, 2] == 1 and e[0, 0, 0] == 0 and e.sum() == 27
+
+
+def test_tgv_bounding_box():
+    """src/inversion/tgv.rs:1356-1377: 3..7 cube, padding 1 -> [2, 8)."""
+    m = np.zeros((10, 10, 10), np.uint8)
+    m[3:7, 3:7, 3:7] = 1
+    lo, hi = O.tgv_bounding_box(m, 1)
+    assert lo[:2] == [2, 2] and hi[:2] == [8, 8]
+
+
+def test_tgv_oblique_stencil_properties():
+    """src/inversion/tgv.rs:1439-1490: sum ~0, centre = -sum(others), anisotropic case."""
+    st = O.tgv_oblique_stencil((1.0, 1.0, 1.0), (0.0, 0.0, 1.0))
+    assert abs(float(st.astype(np.float64).sum())) < 1e-4
+    off = float(st.sum() - st[1, 1, 1])
+    assert abs(float(st[1, 1, 1]) + off) < 1e-6
+    st2 = O.tgv_oblique_stencil((1.0, 1.0, 2.0), (0.2, 0.3, 0.9))
+    assert abs(float(st2.astype(np.float64).sum())) < 1e-4
+    # centrosymmetric pairs share their coefficient
+    np.testing.assert_array_equal(st2, st2[::-1, ::-1, ::-1])
+
+
+def test_tgv_phase_laplacian_of_constant():
+    """src/inversion/tgv.rs:1319-1333: constant phase -> Laplacian ~0 (through tgv_qsm's
+    first step: a constant phase gives chi = 0)."""
+    n = 8
+    mask = np.ones((n, n, n), np.uint8)
+    out = O.tgv_qsm(np.ones((n, n, n)), mask, O.Grid.new(n, n, n), O.TgvParams(iterations=3, erosions=1))
+    assert np.all(np.abs(out) < 1e-12)
+
+
+def _tgv_small_case():
+    n = 12
+    c = 6.0
+    k, j, i = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    mask = (np.sqrt((i - c) ** 2 + (j - c) ** 2 + (k - c) ** 2) < 4.0).astype(np.uint8)
+    phase = np.where(mask > 0, 0.1 * k, 0.0)
+    return phase, mask
+
+
+def test_tgv_qsm_small():
+    """src/inversion/tgv.rs:1379-1437: 12^3 sphere, z ramp, 10 iterations, 1 erosion."""
+    phase, mask = _tgv_small_case()
+    r = O.tgv_qsm(phase, mask, O.Grid.new(12, 12, 12), O.TgvParams(iterations=10, erosions=1))
+    assert r.shape == (12, 12, 12) and np.all(np.isfinite(r)) and np.any(np.abs(r) > 1e-20)
+
+
+def test_tgv_convergence_progress():
+    """src/inversion/tgv.rs:1562-1599: zero phase, tol 1.1 -> stops at the first check
+    (iteration 100); progress is 0..100 then (100, 1000)."""
+    _, mask = _tgv_small_case()
+    seen = []
+    r = O.tgv_qsm(np.zeros(mask.shape), mask, O.Grid.new(12, 12, 12), O.TgvParams(iterations=1000, erosions=1,
+                                                                                   tol=1.1),
+                  progress=lambda a, b: seen.append((a, b)))
+    assert seen[:101] == [(t, 1000) for t in range(101)] and seen[101:] == [(100, 1000)]
+    assert np.all(r == 0.0)
