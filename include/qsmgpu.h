@@ -105,6 +105,8 @@ typedef struct {
   size_t iterations, erosions;
   float step_size, fieldstrength, te, tol;
 } qsm_tgv_params;
+/* ResharpParams — src/bgremove/resharp.rs:22-45 (radius 6 mm, tik_reg 1e-4, tol 1e-6, 30). */
+typedef struct { double radius, tik_reg, tol; size_t max_iter; } qsm_resharp_params;
 /* IlsqrParams — src/inversion/ilsqr.rs:20-34 (tol 0.01, max_iter 50: the LSMR step's
  * tolerance and iteration cap). */
 typedef struct { double tol; size_t max_iter; } qsm_ilsqr_params;
@@ -115,6 +117,7 @@ QSM_API void qsm_tikhonov_params_default(qsm_tikhonov_params* p);
 QSM_API void qsm_sharp_params_default(qsm_sharp_params* p);
 QSM_API void qsm_vsharp_params_default(qsm_vsharp_params* p);
 QSM_API void qsm_ilsqr_params_default(qsm_ilsqr_params* p);
+QSM_API void qsm_resharp_params_default(qsm_resharp_params* p);
 QSM_API void qsm_tgv_params_default(qsm_tgv_params* p);
 
 /* -------------------------------------------------------- dipole inversion -- */
@@ -218,6 +221,31 @@ QSM_API qsm_status qsm_vsharp_with_radii_device(qsm_ctx* ctx, const double* d_fi
                                         double threshold, qsm_progress_fn progress, void* user,
                                         double* d_out_local, uint8_t* d_out_mask);
 
+/* bgremove::resharp — src/bgremove/resharp.rs:58-125: Tikhonov-regularised SHARP solved
+ * by conjugate gradients on (H^T H + tik_reg I) x = H^T H field. */
+QSM_API qsm_status qsm_resharp(qsm_ctx* ctx, const double* field, const uint8_t* mask, const qsm_grid* grid,
+                               const qsm_resharp_params* params, qsm_progress_fn progress, void* user,
+                               double* out_local, uint8_t* out_mask);
+QSM_API qsm_status qsm_resharp_device(qsm_ctx* ctx, const double* d_field, const uint8_t* d_mask,
+                                      const qsm_grid* grid, const qsm_resharp_params* params,
+                                      qsm_progress_fn progress, void* user, double* d_out_local,
+                                      uint8_t* d_out_mask);
+
+/* ------------------------------------------------------------------ solvers -- */
+/* solvers::cg_solve_with_progress — src/solvers/cg.rs:34-101 — for one fixed operator
+ * (closures cannot cross the C ABI):
+ *   A x = Re IFFT(K * FFT(w * Re IFFT(K * FFT(x)))) + lambda * x,
+ * the normal operator of H x = w * IFFT(K * FFT(x)).  d_kernel_spectrum holds K as
+ * nx*ny*nz real values in natural FFT order (the reference's fft_real_kernel output);
+ * K must be even (K(k) = K(-k)), as every real symmetric image-space kernel's is; the
+ * GPU applies (K(k) + K(-k))/2.  d_weight (w) may be NULL for w = 1, d_x0 NULL for a
+ * zero start.  Same stopping rules as the reference: |p.Ap| < 1e-20 or
+ * ||r|| < tol ||b||; progress(iter, max_iter) for every iteration begun. */
+QSM_API qsm_status qsm_cg_kspace_normal_device(qsm_ctx* ctx, const qsm_grid* grid, const double* d_kernel_spectrum,
+                                               const double* d_weight, double lambda, const double* d_b,
+                                               const double* d_x0, double tol, size_t max_iter,
+                                               qsm_progress_fn progress, void* user, double* d_x);
+
 /* ----------------------------------------------------------------- pipeline -- */
 /* InversionAlgorithm — src/pipeline/config.rs:47-58, same variant order.  Variants
  * this library does not compute return QSM_ERR_INVALID_CONFIG; Tgv and Qsmart return
@@ -271,6 +299,7 @@ typedef struct {
   int algorithm;
   qsm_vsharp_params vsharp;
   qsm_sharp_params sharp;
+  qsm_resharp_params resharp;
 } qsm_bg_removal_config;
 
 QSM_API void qsm_inversion_config_default(qsm_inversion_config* c);

@@ -1340,3 +1340,36 @@ def _tgv_operator_norm_sqr(g, g2, w):
     y1 = F32(g2w * v[0] + g2w2 * v[1] + g * v[2])
     y2 = F32(g * v[1] + g21 * v[2])
     return F32(v[0] * y0 + v[1] * y1 + v[2] * y2)
+
+
+# ---------------------------------------------------------------------------
+# RESHARP (src/bgremove/resharp.rs) on CG (src/solvers/cg.rs)
+# ---------------------------------------------------------------------------
+@dataclass
+class ResharpParams:  # src/bgremove/resharp.rs:22-45
+    radius: float = 6.0
+    tik_reg: float = 1e-4
+    tol: float = 1e-6
+    max_iter: int = 30
+
+
+def apply_ht_h(dker, w, x):
+    """Re IFFT(DKER * FFT(w * IFFT(DKER * FFT(x)))) with the complex intermediate kept
+    (src/bgremove/resharp.rs:133-153)."""
+    t = ifft3d(fft3d(x.astype(np.complex128)) * dker) * w
+    return ifft3d(fft3d(t) * dker).real
+
+
+def resharp(field_, mask, grid: Grid, params: ResharpParams = ResharpParams(), progress=None):
+    """src/bgremove/resharp.rs:58-125 -> (local_field, eroded_mask)."""
+    f = _vol(field_, grid)
+    m = _vol(mask, grid, np.uint8)
+    s_fft = fft_real_kernel(smv_kernel(grid, params.radius))
+    dker = 1.0 - s_fft
+    eroded = erode_mask_smv(m, s_fft, 1.0 - math.sqrt(1e-7))
+    w = eroded.astype(np.float64)
+    b = apply_ht_h(dker, w, f)
+    lam = params.tik_reg
+    x = cg_solve(lambda v: (apply_ht_h(dker, w, v.reshape(grid.shape)) + lam * v.reshape(grid.shape)).ravel(),
+                 b.ravel(), np.zeros(f.size), params.tol, params.max_iter, progress)
+    return np.where(eroded.ravel() == 1, x, 0.0).reshape(grid.shape), eroded

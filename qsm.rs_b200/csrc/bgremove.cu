@@ -6,6 +6,7 @@
 // (FP64 transform error ~1e-15) whatever the context precision; field filtering runs
 // in the working precision.
 #include "functors.cuh"
+#include "solvers.h"
 
 #include <algorithm>
 #include <cstring>
@@ -508,6 +509,7 @@ void qsm_bg_removal_config_default(qsm_bg_removal_config* c) {
   c->algorithm = QSM_BG_VSHARP;
   qsm_vsharp_params_default(&c->vsharp);
   qsm_sharp_params_default(&c->sharp);
+  qsm_resharp_params_default(&c->resharp);
 }
 
 qsm_status qsm_run_bg_removal(qsm_ctx* ctx, const double* field_ppm, size_t len, const uint8_t* mask,
@@ -534,6 +536,12 @@ qsm_status qsm_run_bg_removal(qsm_ctx* ctx, const double* field_ppm, size_t len,
                       });
         break;
       }
+      case QSM_BG_RESHARP:
+        with_host_io2(ctx, d, field_ppm, mask, out_local, out_mask,
+                      [&](const double* f, const uint8_t* m, double* o, uint8_t* om) {
+                        resharp_device(ctx, f, m, d, &cfg->resharp, progress, user, o, om);
+                      });
+        break;
       case QSM_BG_SHARP:
         with_host_io2(ctx, d, field_ppm, mask, out_local, out_mask,
                       [&](const double* f, const uint8_t* m, double* o, uint8_t* om) {

@@ -19,6 +19,9 @@ void tikhonov_device(qsm_ctx* ctx, const double* f, const uint8_t* m, const qsm_
 void ilsqr_device(qsm_ctx* ctx, const double* f, const uint8_t* m, const qsm_grid* grid, const double bdir[3],
                   const qsm_ilsqr_params* p, qsm_progress_fn progress, void* user, double* chi, double* xsa,
                   double* xfs, double* xlsqr);
+void resharp_device(qsm_ctx* ctx, const double* field, const uint8_t* mask, const GridDims& d,
+                    const qsm_resharp_params* p, qsm_progress_fn progress, void* user, double* out_local,
+                    uint8_t* out_mask);
 void tgv_device(qsm_ctx* ctx, const double* phase, const uint8_t* mask, const qsm_grid* grid, const qsm_tgv_params* p,
                 const double b0[3], qsm_progress_fn progress, void* user, double* out);
 

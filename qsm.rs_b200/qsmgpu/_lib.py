@@ -57,6 +57,10 @@ class QsmVsharpParams(C.Structure):
     _fields_ = [("threshold", C.c_double), ("max_radius", C.c_double), ("min_radius", C.c_double)]
 
 
+class QsmResharpParams(C.Structure):
+    _fields_ = [("radius", C.c_double), ("tik_reg", C.c_double), ("tol", C.c_double), ("max_iter", C.c_size_t)]
+
+
 class QsmIlsqrParams(C.Structure):
     _fields_ = [("tol", C.c_double), ("max_iter", C.c_size_t)]
 
@@ -78,7 +82,8 @@ class QsmInversionConfig(C.Structure):
 
 
 class QsmBgRemovalConfig(C.Structure):
-    _fields_ = [("algorithm", C.c_int), ("vsharp", QsmVsharpParams), ("sharp", QsmSharpParams)]
+    _fields_ = [("algorithm", C.c_int), ("vsharp", QsmVsharpParams), ("sharp", QsmSharpParams),
+                ("resharp", QsmResharpParams)]
 
 
 # (name, restype, argtypes)
@@ -100,6 +105,14 @@ _SIGS = [
     ("qsm_grid_supported", C.c_int, [C.POINTER(QsmGrid)]),
     ("qsm_tv_params_default", None, [C.POINTER(QsmTvParams)]),
     ("qsm_ilsqr_params_default", None, [C.POINTER(QsmIlsqrParams)]),
+    ("qsm_resharp_params_default", None, [C.POINTER(QsmResharpParams)]),
+    ("qsm_resharp", C.c_int, [C.c_void_p, c_double_p, c_u8_p, C.POINTER(QsmGrid), C.POINTER(QsmResharpParams),
+                              PROGRESS_FN, C.c_void_p, c_double_p, c_u8_p]),
+    ("qsm_resharp_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(QsmGrid),
+                                     C.POINTER(QsmResharpParams), PROGRESS_FN, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("qsm_cg_kspace_normal_device", C.c_int, [C.c_void_p, C.POINTER(QsmGrid), C.c_void_p, C.c_void_p, C.c_double,
+                                              C.c_void_p, C.c_void_p, C.c_double, C.c_size_t, PROGRESS_FN,
+                                              C.c_void_p, C.c_void_p]),
     ("qsm_tgv_params_default", None, [C.POINTER(QsmTgvParams)]),
     ("qsm_tgv_qsm", C.c_int, [C.c_void_p, c_double_p, c_u8_p, C.POINTER(QsmGrid), C.POINTER(QsmTgvParams),
                               c_double_p, PROGRESS_FN, C.c_void_p, c_double_p]),

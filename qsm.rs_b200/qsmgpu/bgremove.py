@@ -23,6 +23,19 @@ class SharpParams:
 
 
 @dataclass
+class ResharpParams:
+    """src/bgremove/resharp.rs:22-45."""
+
+    radius: float = 6.0
+    tik_reg: float = 1e-4
+    tol: float = 1e-6
+    max_iter: int = 30
+
+    def _c(self):
+        return _lib.QsmResharpParams(self.radius, self.tik_reg, self.tol, int(self.max_iter))
+
+
+@dataclass
 class VsharpParams:
     """src/bgremove/vsharp.rs:22-40."""
 
@@ -85,3 +98,28 @@ def vsharp_with_radii(field, mask, grid: Grid, radii: Sequence[float], threshold
     _check(c, c._lib.qsm_vsharp_with_radii(c.handle, _ptr_d(f), _ptr_u8(m), C.byref(g), _ptr_d(r), r.size,
                                            float(threshold), cb, None, _ptr_d(out), _ptr_u8(om)))
     return out, om
+
+
+def resharp(field, mask, grid: Grid, params: ResharpParams = ResharpParams(),
+            progress: Optional[Callable[[int, int], None]] = None, *, ctx: Optional[Context] = None):
+    """bgremove::resharp (src/bgremove/resharp.rs:58-125) -> (local_field, eroded_mask)."""
+    c = _ctx(ctx)
+    f, m, out, om = _io(field, mask, grid)
+    g = grid._c()
+    p = params._c()
+    cb, _keep = _progress(progress)
+    _check(c, c._lib.qsm_resharp(c.handle, _ptr_d(f), _ptr_u8(m), C.byref(g), C.byref(p), cb, None, _ptr_d(out),
+                                 _ptr_u8(om)))
+    return out, om
+
+
+def cg_kspace_normal_device(ctx: Context, grid: Grid, d_kernel_spectrum: int, d_weight: int, lam: float, d_b: int,
+                            d_x0: int, tol: float, max_iter: int, d_x: int, progress=None):
+    """solvers::cg_solve_with_progress (src/solvers/cg.rs:34-101) for
+    A x = Re IFFT(K FFT(w Re IFFT(K FFT(x)))) + lam x; device pointers as ints (0 = NULL)."""
+    g = grid._c()
+    cb, _keep = _progress(progress)
+    _check(ctx, ctx._lib.qsm_cg_kspace_normal_device(ctx.handle, C.byref(g), C.c_void_p(d_kernel_spectrum),
+                                                     C.c_void_p(d_weight or None), float(lam), C.c_void_p(d_b),
+                                                     C.c_void_p(d_x0 or None), float(tol), int(max_iter), cb, None,
+                                                     C.c_void_p(d_x)))

@@ -10,7 +10,7 @@ import numpy as np
 from . import _lib
 from . import Context, _ctx, _check, _ptr_d, _ptr_u8, _progress
 from .inversion import IlsqrParams, TkdParams, TikhonovParams, TvParams
-from .bgremove import SharpParams, VsharpParams
+from .bgremove import ResharpParams, SharpParams, VsharpParams
 
 # InversionAlgorithm, src/pipeline/config.rs:47-58
 TKD, TSVD, TIKHONOV, TV, RTS, NLTV, MEDI, ILSQR, TGV, QSMART = range(10)
@@ -57,9 +57,10 @@ class BgRemovalConfig:
     algorithm: int = VSHARP
     vsharp: VsharpParams = field(default_factory=VsharpParams)
     sharp: SharpParams = field(default_factory=SharpParams)
+    resharp: ResharpParams = field(default_factory=ResharpParams)
 
     def _c(self):
-        return _lib.QsmBgRemovalConfig(self.algorithm, self.vsharp._c(), self.sharp._c())
+        return _lib.QsmBgRemovalConfig(self.algorithm, self.vsharp._c(), self.sharp._c(), self.resharp._c())
 
 
 @dataclass

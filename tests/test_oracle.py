@@ -434,3 +434,16 @@ def test_tgv_convergence_progress():
                   progress=lambda a, b: seen.append((a, b)))
     assert seen[:101] == [(t, 1000) for t in range(101)] and seen[101:] == [(100, 1000)]
     assert np.all(r == 0.0)
+
+
+def test_resharp_reference_tests():
+    """src/bgremove/resharp.rs:159-190: zero field -> ~0; ramp field -> finite, eroded mask
+    not empty."""
+    n = 16
+    grid = O.Grid.new(n, n, n)
+    p = O.ResharpParams(2.0, 1e-4, 1e-6, 50)
+    local, _ = O.resharp(np.zeros((n, n, n)), np.ones((n, n, n), np.uint8), grid, p)
+    assert np.all(np.abs(local) < 1e-8)
+    field = (np.arange(n ** 3, dtype=np.float64) * 0.01).reshape(n, n, n)
+    local, eroded = O.resharp(field, np.ones((n, n, n), np.uint8), grid, p)
+    assert np.all(np.isfinite(local)) and eroded.sum() > 0
