@@ -325,6 +325,22 @@ QSM_API qsm_status qsm_run_bg_removal(qsm_ctx* ctx, const double* field_ppm, siz
 QSM_API qsm_status qsm_prctile_device(qsm_ctx* ctx, const double* d_vals, const uint8_t* d_mask, size_t n,
                                       const double* p, size_t np, double* out);
 
+/* QsmReference — src/pipeline/config.rs:69-72. */
+typedef enum { QSM_REFERENCE_MEAN = 0, QSM_REFERENCE_NONE = 1 } qsm_reference;
+
+/* pipeline::referencing::apply_reference — src/pipeline/referencing.rs:12-43 (host
+ * pointers, n values): Mean subtracts the mean over mask > 0; both zero outside it. */
+QSM_API qsm_status qsm_apply_reference(qsm_ctx* ctx, const double* chi, const uint8_t* mask, size_t n, int method,
+                                       double* out);
+
+/* pipeline::run_tgv — src/pipeline/inversion.rs:124-157 for a single echo: wrapped phase ->
+ * tgv_qsm -> apply_reference.  `phases` holds n_echoes pointers to `len` values each;
+ * more than one echo needs field mapping, which this library does not provide, and
+ * returns QSM_ERR_INVALID_CONFIG.  len != nx*ny*nz -> QSM_ERR_DIMENSION_MISMATCH. */
+QSM_API qsm_status qsm_run_tgv(qsm_ctx* ctx, const double* const* phases, size_t n_echoes, size_t len,
+                               const uint8_t* mask, const qsm_scan_metadata* metadata, const qsm_tgv_params* params,
+                               int reference, qsm_progress_fn progress, void* user, double* out_chi);
+
 /* ---------------------------------------------------------- FFT primitives -- */
 /* Forward 3D transform of a real volume, returned as the full complex spectrum
  * (interleaved re, im; nx*ny*nz complex values) — src/fft.rs:412-430 fft3d on real

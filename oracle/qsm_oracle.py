@@ -1373,3 +1373,11 @@ def resharp(field_, mask, grid: Grid, params: ResharpParams = ResharpParams(), p
     x = cg_solve(lambda v: (apply_ht_h(dker, w, v.reshape(grid.shape)) + lam * v.reshape(grid.shape)).ravel(),
                  b.ravel(), np.zeros(f.size), params.tol, params.max_iter, progress)
     return np.where(eroded.ravel() == 1, x, 0.0).reshape(grid.shape), eroded
+
+
+def apply_reference(chi, mask, method="mean"):
+    """src/pipeline/referencing.rs:12-43: Mean subtracts the masked mean; zero outside."""
+    x = np.asarray(chi, dtype=np.float64)
+    m = np.asarray(mask) > 0
+    mu = float(x[m].sum()) / int(m.sum()) if (method == "mean" and m.any()) else 0.0
+    return np.where(m, x - mu, 0.0)

@@ -197,9 +197,56 @@ template <typename T, class K> int yz_tile_width(K kernel, int n, int Tn) {
   throw QsmError(QSM_ERR_UNSUPPORTED_SIZE, "axis of length " + std::to_string(n) + " does not fit one tile");
 }
 
+// Compile-time Y/Z kernels (float, 16-column tiles) for the axis lengths of
+// QSM_FIXED_PLANS; returns false when the plan is not one of them.
+constexpr int kFxCols = 16;
+template <class K> bool fx_launch_ok(qsm_ctx* ctx, K kern, int threads, size_t smem, unsigned* grid, long long work) {
+  if (smem > 227u * 1024u) return false;
+  ensure_smem(kern, smem);
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  if (per_sm < 1) return false;
+  long long g = (long long)per_sm * sm_count(ctx);
+  if (g > work) g = work;
+  *grid = (unsigned)(g < 1 ? 1 : g);
+  return true;
+}
+
+template <typename T, int DIR, int AXIS>
+bool run_yz_fixed(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst, const int* done) {
+  if constexpr (!std::is_same<T, float>::value) {
+    return false;
+  } else {
+    const FftPlan1D& pl = (AXIS == 1) ? f.py : f.pz;
+    const cplx_t<T>* tw = (AXIS == 1) ? f.twy : f.twz;
+#define QSM_TRY_YZ(N_, T_, R0_, R1_, R2_)                                                         \
+    if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(pl) && kFxCols * T_ <= 1024) {                   \
+      using FP = FixedPlan<N_, T_, R0_, R1_, R2_>;                                                \
+      auto kern = k_pass_yz_fx<T, DIR, FP, kFxCols>;                                              \
+      const size_t smem = yz_smem<T>(N_, kFxCols);                                                \
+      const TileWalk w = tile_walk(f, AXIS, kFxCols);                                             \
+      unsigned grid = 0;                                                                          \
+      if (!fx_launch_ok(ctx, kern, kFxCols * T_, smem, &grid, w.ntiles)) return false;            \
+      LaunchScope ls(ctx, AXIS == 1 ? (DIR < 0 ? "fft_y_fwd" : "fft_y_inv") : (DIR < 0 ? "fft_z_fwd" : "fft_z_inv")); \
+      kern<<<grid, dim3(kFxCols, T_), smem, ctx->stream>>>(f.g, w, tw, src, dst, done);          \
+      ls.done();                                                                                  \
+      return true;                                                                                \
+    }
+    QSM_FIXED_PLANS(QSM_TRY_YZ)
+#undef QSM_TRY_YZ
+    return false;
+  }
+}
+
 // AXIS 1 = y, 2 = z; DIR -1 forward, +1 inverse.
 template <typename T, int DIR, int AXIS, class Op>
 void run_yz(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst, const Op& op, const int* done) {
+  if constexpr (IsPlainOp<Op>::value) {
+    if (run_yz_fixed<T, DIR, AXIS>(ctx, f, src, dst, done)) return;
+  }
   const FftPlan1D& pl = (AXIS == 1) ? f.py : f.pz;
   const cplx_t<T>* tw = (AXIS == 1) ? f.twy : f.twz;
   auto kern = k_pass_yz<T, DIR, AXIS, Op>;
@@ -256,6 +303,24 @@ template <typename T>
 void run_z_fused_m(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst, const T* mult,
                    const int* done) {
   const FftPlan1D& pl = f.pz;
+  if constexpr (std::is_same<T, float>::value) {
+#define QSM_TRY_ZM(N_, T_, R0_, R1_, R2_)                                                         \
+    if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(pl) && kFxCols * T_ <= 1024) {                   \
+      using FP = FixedPlan<N_, T_, R0_, R1_, R2_>;                                                \
+      auto kfx = k_z_fused_m_fx<T, FP, kFxCols>;                                                  \
+      const size_t smem = zm_smem<T>(N_, kFxCols);                                                \
+      const TileWalk w = tile_walk(f, 2, kFxCols);                                                \
+      unsigned grid = 0;                                                                          \
+      if (fx_launch_ok(ctx, kfx, kFxCols * T_, smem, &grid, w.ntiles)) {                          \
+        LaunchScope ls(ctx, "fft_z_fused");                                                       \
+        kfx<<<grid, dim3(kFxCols, T_), smem, ctx->stream>>>(f.g, w, f.twz, src, dst, mult, done); \
+        ls.done();                                                                                \
+        return;                                                                                   \
+      }                                                                                           \
+    }
+    QSM_FIXED_PLANS(QSM_TRY_ZM)
+#undef QSM_TRY_ZM
+  }
   auto kern = k_z_fused_m<T>;
   const int P = zm_tile_width<T>(pl.n, pl.T);
   if (P == 0) throw QsmError(QSM_ERR_UNSUPPORTED_SIZE, "z axis does not fit one multiplier tile");

@@ -482,6 +482,60 @@ __global__ void __maxnreg__(YzRegCap<T>::value)
   if (grid_sum_last<1>(acc, partials, counter) && tid == 0) op.last(acc[0]);
 }
 
+// ------------------------------------------------------------------------------
+// Compile-time Y/Z passes: the same tile walk with the transform length, threads per
+// column and radices fixed (FP, a FixedPlan) and P columns per tile, so that loop
+// bounds, j mod Ns, twiddle strides and shared-memory addressing fold into constants.
+// Plain copies (k_pass_yz_fx) and the multiplier Z pass (k_z_fused_m_fx).
+// ------------------------------------------------------------------------------
+template <int P> struct SAStridedC {
+  __device__ __forceinline__ int operator()(int e) const { return e * P; }
+};
+
+template <typename T, int DIR, class FP, int P>
+__global__ void __launch_bounds__(P* FP::T, (P * FP::T <= 256 ? 3 : 1))
+    k_pass_yz_fx(Geom g, TileWalk w, const cplx_t<T>* __restrict__ twg, const cplx_t<T>* src, cplx_t<T>* dst,
+                 const int* __restrict__ done) {
+  using C = cplx_t<T>;
+  constexpr int n = FP::n;
+  if (done != nullptr && *done) return;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* tw = reinterpret_cast<C*>(smraw);
+  C* buf0 = tw + ((n + 7) & ~7);
+  C* buf1 = buf0 + n * P;
+  const int tid = threadIdx.x + threadIdx.y * P;
+  for (int i = tid; i < n; i += P * FP::T) tw[i] = twg[i];
+  const int px = threadIdx.x;
+  const int t = threadIdx.y;
+  SAStridedC<P> sa;
+  int tile = blockIdx.x;
+  if (tile < w.ntiles) issue_tile(src, buf0, g, w, tile, n, P);
+  cp_async_commit();
+  for (int it = 0; tile < w.ntiles; tile += gridDim.x, ++it) {
+    C* cur = (it & 1) ? buf1 : buf0;
+    C* nxt = (it & 1) ? buf0 : buf1;
+    const int next = tile + gridDim.x;
+    if (next < w.ntiles) issue_tile(src, nxt, g, w, next, n, P);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    const int tx = tile % w.ntx, outer = tile / w.ntx;
+    const int col = tx * P + px;
+    const bool active = col < g.nxh;
+    const long long base = col + (long long)outer * w.ostride;
+    C* sp = cur + px;
+    auto fetch = [&](int e) -> C { return sp[sa(e)]; };
+    auto emit = [&](int e, C v) { dst[base + e * w.estride] = v; };
+    FP::template run<DIR>(t, active, sp, sa, tw, fetch, emit);
+  }
+  cp_async_wait<0>();
+}
+
+template <typename T, class FP, int P>
+__global__ void __launch_bounds__(P* FP::T, (P * FP::T <= 256 ? 3 : 1))
+    k_z_fused_m_fx(Geom g, TileWalk w, const cplx_t<T>* __restrict__ twg, const cplx_t<T>* src, cplx_t<T>* dst,
+                   const T* __restrict__ mult, const int* __restrict__ done);
+
 // Real multiplier tile (same tile walk, element size sizeof(T)), 16-byte chunks.
 template <typename T>
 __device__ __forceinline__ void issue_mtile(const T* __restrict__ src, T* buf, const Geom& g, const TileWalk& w,
@@ -555,6 +609,59 @@ __global__ void __maxnreg__(YzRegCap<T>::value) k_z_fused_m(Geom g, const __grid
     }
     __syncthreads();
     fft_pencil<+1, C, SAStrided, false, true>(&pl, t, active, sp, sa, tw, nullptr, dst, base, w.estride);
+  }
+  cp_async_wait<0>();
+}
+
+// Compile-time form of k_z_fused_m (see k_pass_yz_fx).
+template <typename T, class FP, int P>
+__global__ void __launch_bounds__(P* FP::T, (P * FP::T <= 256 ? 3 : 1))
+    k_z_fused_m_fx(Geom g, TileWalk w, const cplx_t<T>* __restrict__ twg, const cplx_t<T>* src, cplx_t<T>* dst,
+                   const T* __restrict__ mult, const int* __restrict__ done) {
+  using C = cplx_t<T>;
+  constexpr int n = FP::n;
+  if (done != nullptr && *done) return;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* tw = reinterpret_cast<C*>(smraw);
+  C* buf0 = tw + ((n + 7) & ~7);
+  C* buf1 = buf0 + n * P;
+  T* mb0 = reinterpret_cast<T*>(buf1 + n * P);
+  T* mb1 = mb0 + ((n * P + 3) & ~3);
+  const int tid = threadIdx.x + threadIdx.y * P;
+  for (int i = tid; i < n; i += P * FP::T) tw[i] = twg[i];
+  const int px = threadIdx.x;
+  const int t = threadIdx.y;
+  SAStridedC<P> sa;
+  int tile = blockIdx.x;
+  if (tile < w.ntiles) {
+    issue_tile(src, buf0, g, w, tile, n, P);
+    issue_mtile(mult, mb0, g, w, tile, n, P);
+  }
+  cp_async_commit();
+  for (int it = 0; tile < w.ntiles; tile += gridDim.x, ++it) {
+    C* cur = (it & 1) ? buf1 : buf0;
+    C* nxt = (it & 1) ? buf0 : buf1;
+    T* mcur = (it & 1) ? mb1 : mb0;
+    T* mnxt = (it & 1) ? mb0 : mb1;
+    const int next = tile + gridDim.x;
+    if (next < w.ntiles) {
+      issue_tile(src, nxt, g, w, next, n, P);
+      issue_mtile(mult, mnxt, g, w, next, n, P);
+    }
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    const int tx = tile % w.ntx, iy = tile / w.ntx;
+    const int col = tx * P + px;
+    const bool active = col < g.nxh;
+    const long long base = col + (long long)iy * w.ostride;
+    C* sp = cur + px;
+    auto fetch = [&](int e) -> C { return sp[sa(e)]; };
+    // forward transform back into the tile, scaled by the multiplier on the way out
+    auto emit_m = [&](int e, C v) { sp[sa(e)] = cscale(v, mcur[e * P + px]); };
+    FP::template run<-1>(t, active, sp, sa, tw, fetch, emit_m);
+    auto emit = [&](int e, C v) { dst[base + e * w.estride] = v; };
+    FP::template run<+1>(t, active, sp, sa, tw, fetch, emit);
   }
   cp_async_wait<0>();
 }

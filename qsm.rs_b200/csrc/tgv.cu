@@ -850,3 +850,102 @@ qsm_status qsm_tgv_oblique_stencil(const double res[3], const double b0_dir[3], 
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------ pipeline --
+namespace qsm {
+namespace {
+
+// apply_reference (src/pipeline/referencing.rs:12-43): Mean subtracts the mean over
+// mask > 0, None keeps the values; zero outside the mask in both
+__global__ void k_ref_sum(long long N, const double* __restrict__ chi, const uint8_t* __restrict__ m,
+                          double* partials, unsigned* counter, double* out) {
+  double acc[2] = {0.0, 0.0};
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
+    if (m[i] > 0) {
+      acc[0] += chi[i];
+      acc[1] += 1.0;
+    }
+  if (grid_sum_last<2>(acc, partials, counter) && threadIdx.x == 0) {
+    out[0] = acc[0];
+    out[1] = acc[1];
+  }
+}
+
+__global__ void k_ref_apply(long long N, const double* __restrict__ chi, const uint8_t* __restrict__ m,
+                            const double* __restrict__ sums, int mean, double* __restrict__ out) {
+  const double mu = (mean && sums[1] > 0.0) ? sums[0] / sums[1] : 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
+    out[i] = m[i] > 0 ? chi[i] - mu : 0.0;
+}
+
+}  // namespace
+
+void apply_reference_device(qsm_ctx* ctx, long long N, const double* chi, const uint8_t* mask, int method,
+                            double* out) {
+  if (method != QSM_REFERENCE_MEAN && method != QSM_REFERENCE_NONE)
+    throw QsmError(QSM_ERR_INVALID_ARGUMENT, "unknown QSM reference method " + std::to_string(method));
+  double* partials = ws<double>(ctx, "ref.partials", (size_t)kMaxPersistentBlocks * 2);
+  unsigned* counter = ws<unsigned>(ctx, "ref.counter", 1);
+  double* sums = ws<double>(ctx, "ref.sums", 2);
+  QSM_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned), ctx->stream));
+  QSM_CUDA(cudaMemsetAsync(sums, 0, 2 * sizeof(double), ctx->stream));
+  LaunchScope ls(ctx, "apply_reference");
+  if (method == QSM_REFERENCE_MEAN)
+    k_ref_sum<<<grid1d(N), 256, 0, ctx->stream>>>(N, chi, mask, partials, counter, sums);
+  k_ref_apply<<<grid1d(N), 256, 0, ctx->stream>>>(N, chi, mask, sums, method == QSM_REFERENCE_MEAN, out);
+  ls.done();
+}
+
+}  // namespace qsm
+
+extern "C" {
+
+qsm_status qsm_apply_reference(qsm_ctx* ctx, const double* chi, const uint8_t* mask, size_t n, int method,
+                               double* out) {
+  return guarded(ctx, [&] {
+    if (n == 0) return;
+    check_ptr(chi, "chi");
+    check_ptr(mask, "mask");
+    check_ptr(out, "out");
+    double* din = ws<double>(ctx, "io.in", n);
+    uint8_t* dm = ws<uint8_t>(ctx, "io.mask", n);
+    double* dout = ws<double>(ctx, "io.out", n);
+    h2d(ctx, din, chi, n * sizeof(double));
+    h2d(ctx, dm, mask, n);
+    apply_reference_device(ctx, (long long)n, din, dm, method, dout);
+    d2h(ctx, out, dout, n * sizeof(double));
+    sync(ctx);
+  });
+}
+
+qsm_status qsm_run_tgv(qsm_ctx* ctx, const double* const* phases, size_t n_echoes, size_t len, const uint8_t* mask,
+                       const qsm_scan_metadata* md, const qsm_tgv_params* params, int reference,
+                       qsm_progress_fn progress, void* user, double* out_chi) {
+  return guarded(ctx, [&] {
+    check_ptr(md, "metadata");
+    check_ptr(params, "params");
+    check_ptr(phases, "phases");
+    if (n_echoes == 0) throw QsmError(QSM_ERR_INVALID_ARGUMENT, "no echoes");
+    if (n_echoes > 1)
+      throw QsmError(QSM_ERR_INVALID_CONFIG,
+                     "invalid config: multi-echo run_tgv needs field mapping, which this library does not provide");
+    qsm_grid g{md->nx, md->ny, md->nz, md->vsx, md->vsy, md->vsz};
+    GridDims d = check_grid(&g);
+    if (len != (size_t)d.n)
+      throw QsmError(QSM_ERR_DIMENSION_MISMATCH,
+                     "dimension mismatch: expected " + std::to_string(d.n) + ", got " + std::to_string(len));
+    if (reference != QSM_REFERENCE_MEAN && reference != QSM_REFERENCE_NONE)
+      throw QsmError(QSM_ERR_INVALID_ARGUMENT, "unknown QSM reference method");
+    check_ptr(phases[0], "phases[0]");
+    check_ptr(mask, "mask");
+    check_ptr(out_chi, "out_chi");
+    // single echo: the wrapped phase goes to tgv_qsm directly (src/pipeline/inversion.rs:124-157)
+    with_host_io(ctx, d.n, phases[0], mask, out_chi, [&](const double* f, const uint8_t* m, double* o) {
+      double* chi = ws<double>(ctx, "tgv.chi_full", (size_t)d.n);
+      tgv_device(ctx, f, m, &g, params, md->b0_direction, progress, user, chi);
+      apply_reference_device(ctx, d.n, chi, m, reference, o);
+    });
+  });
+}
+
+}  // extern "C"

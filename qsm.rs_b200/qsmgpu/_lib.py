@@ -105,6 +105,10 @@ _SIGS = [
     ("qsm_grid_supported", C.c_int, [C.POINTER(QsmGrid)]),
     ("qsm_tv_params_default", None, [C.POINTER(QsmTvParams)]),
     ("qsm_ilsqr_params_default", None, [C.POINTER(QsmIlsqrParams)]),
+    ("qsm_apply_reference", C.c_int, [C.c_void_p, c_double_p, c_u8_p, C.c_size_t, C.c_int, c_double_p]),
+    ("qsm_run_tgv", C.c_int, [C.c_void_p, C.POINTER(c_double_p), C.c_size_t, C.c_size_t, c_u8_p,
+                              C.POINTER(QsmScanMetadata), C.POINTER(QsmTgvParams), C.c_int, PROGRESS_FN,
+                              C.c_void_p, c_double_p]),
     ("qsm_resharp_params_default", None, [C.POINTER(QsmResharpParams)]),
     ("qsm_resharp", C.c_int, [C.c_void_p, c_double_p, c_u8_p, C.POINTER(QsmGrid), C.POINTER(QsmResharpParams),
                               PROGRESS_FN, C.c_void_p, c_double_p, c_u8_p]),

@@ -109,3 +109,38 @@ def run_bg_removal(field_ppm, mask, metadata: ScanMetadata, config: BgRemovalCon
                                    _ptr_d(out), _ptr_u8(om))
     _check(c, st)
     return BgRemovalResult(out, om)
+
+
+REFERENCE_MEAN, REFERENCE_NONE = 0, 1  # QsmReference, src/pipeline/config.rs:69-72
+
+
+def apply_reference(chi, mask, method: int = REFERENCE_MEAN, *, ctx: Optional[Context] = None):
+    """pipeline::referencing::apply_reference (src/pipeline/referencing.rs:12-43)."""
+    c = _ctx(ctx)
+    x = np.ascontiguousarray(np.asarray(chi, dtype=np.float64)).ravel()
+    m = np.ascontiguousarray(np.asarray(mask, dtype=np.uint8)).ravel()
+    if m.size != x.size:
+        raise ValueError("mask and chi lengths differ")
+    out = np.empty_like(x)
+    _check(c, c._lib.qsm_apply_reference(c.handle, _ptr_d(x), _ptr_u8(m), x.size, int(method), _ptr_d(out)))
+    return out
+
+
+def run_tgv(phases, mask, metadata: ScanMetadata, tgv_params, reference: int = REFERENCE_MEAN,
+            progress: Optional[Callable[[int, int], None]] = None, *, ctx: Optional[Context] = None):
+    """pipeline::run_tgv (src/pipeline/inversion.rs:124-157), single echo."""
+    c = _ctx(ctx)
+    ph = [np.ascontiguousarray(np.asarray(p, dtype=np.float64)).ravel() for p in phases]
+    m = np.ascontiguousarray(np.asarray(mask, dtype=np.uint8)).ravel()
+    n = metadata.dims[0] * metadata.dims[1] * metadata.dims[2]
+    if m.size != n:
+        raise ValueError(f"mask has {m.size} values, expected {n}")
+    arr = (_lib.c_double_p * max(len(ph), 1))(*[_ptr_d(p) for p in ph])
+    out = np.empty(n, dtype=np.float64)
+    md = metadata._c()
+    p = tgv_params._c()
+    cb, _keep = _progress(progress)
+    st = c._lib.qsm_run_tgv(c.handle, arr, len(ph), ph[0].size if ph else 0, _ptr_u8(m), C.byref(md), C.byref(p),
+                            int(reference), cb, None, _ptr_d(out))
+    _check(c, st)
+    return out

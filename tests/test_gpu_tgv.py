@@ -114,3 +114,29 @@ def test_tgv_empty_mask_is_an_error(ctx64):
     m[3:5, 3:5, 3:5] = 1  # vanishes after the erosions
     with pytest.raises(qsmgpu.QsmError):
         inversion.tgv_qsm(np.zeros(grid.shape), m, grid, inversion.TgvParams(iterations=5), (0, 0, 1), ctx=ctx64)
+
+
+def test_apply_reference_known_answers(ctx64):
+    """src/pipeline/referencing.rs:49-82 through the C ABI."""
+    from qsmgpu import pipeline
+    np.testing.assert_allclose(pipeline.apply_reference([1.0, 2.0, 3.0, 4.0], [1, 1, 1, 0], ctx=ctx64),
+                               [-1.0, 0.0, 1.0, 0.0], atol=1e-10)
+    assert list(pipeline.apply_reference([1.0, 2.0, 3.0], [1, 0, 1], pipeline.REFERENCE_NONE, ctx=ctx64)) == [1.0, 0.0, 3.0]
+    assert list(pipeline.apply_reference([1.0, 2.0], [0, 0], ctx=ctx64)) == [0.0, 0.0]
+
+
+def test_run_tgv_single_echo_and_errors(ctx64):
+    """pipeline::run_tgv (src/pipeline/inversion.rs:124-157): tgv_qsm then apply_reference."""
+    from qsmgpu import pipeline
+    grid = Grid.new(30, 26, 22, 1.0, 1.1, 1.3)
+    phase, mask = phantom_phase(grid, OBLIQUE, seed=3)
+    p = inversion.TgvParams(iterations=120, erosions=2)
+    md = pipeline.ScanMetadata(grid.dims, grid.voxel_size, b0_direction=OBLIQUE)
+    got = pipeline.run_tgv([phase], mask, md, p, pipeline.REFERENCE_MEAN, ctx=ctx64)
+    chi = inversion.tgv_qsm(phase, mask, grid, p, OBLIQUE, ctx=ctx64)
+    want = O.apply_reference(chi, mask)
+    assert rel(got, want) < 1e-12
+    with pytest.raises(qsmgpu.InvalidConfig):
+        pipeline.run_tgv([phase, phase], mask, md, p, ctx=ctx64)
+    with pytest.raises(qsmgpu.DimensionMismatch):
+        pipeline.run_tgv([phase.ravel()[:-1]], mask, md, p, ctx=ctx64)

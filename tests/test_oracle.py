@@ -447,3 +447,10 @@ def test_resharp_reference_tests():
     field = (np.arange(n ** 3, dtype=np.float64) * 0.01).reshape(n, n, n)
     local, eroded = O.resharp(field, np.ones((n, n, n), np.uint8), grid, p)
     assert np.all(np.isfinite(local)) and eroded.sum() > 0
+
+
+def test_apply_reference_known_answers():
+    """src/pipeline/referencing.rs:49-82."""
+    np.testing.assert_allclose(O.apply_reference([1.0, 2.0, 3.0, 4.0], [1, 1, 1, 0]), [-1.0, 0.0, 1.0, 0.0], atol=1e-10)
+    assert list(O.apply_reference([1.0, 2.0, 3.0], [1, 0, 1], "none")) == [1.0, 0.0, 3.0]
+    assert list(O.apply_reference([1.0, 2.0], [0, 0])) == [0.0, 0.0]
