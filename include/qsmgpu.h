@@ -131,6 +131,31 @@ QSM_API qsm_status qsm_tv_admm_device(qsm_ctx* ctx, const double* d_local_field,
 /* Iterations actually run by the last tv_admm call on this context (early exit). */
 QSM_API size_t qsm_tv_last_iterations(const qsm_ctx* ctx);
 
+/* One volume of a batch: its own grid, field direction, input, mask and output (host
+ * pointers for the plain batch call, device pointers for the *_device one). */
+typedef struct {
+  const double* local_field;
+  const uint8_t* mask;
+  double* out_chi;
+  qsm_grid grid;
+  double bdir[3];
+} qsm_volume;
+
+/* inversion::tv_admm over a batch of volumes of any sizes and field directions, one
+ * call (no counterpart in the reference, which solves one volume per call; each volume's
+ * result equals a qsm_tv_admm call with the same parameters).  One CUDA graph advances
+ * every volume by two iterations, the volumes running as parallel branches.  progress
+ * is (volumes finished, n); out_iterations (may be NULL) receives each volume's
+ * iteration count. */
+QSM_API qsm_status qsm_tv_admm_batch(qsm_ctx* ctx, const qsm_volume* volumes, size_t n, const qsm_tv_params* params,
+                                     qsm_progress_fn progress, void* user, size_t* out_iterations);
+QSM_API qsm_status qsm_tv_admm_batch_device(qsm_ctx* ctx, const qsm_volume* volumes, size_t n,
+                                            const qsm_tv_params* params, qsm_progress_fn progress, void* user,
+                                            size_t* out_iterations);
+/* inversion::tkd over a batch of volumes (no counterpart in the reference). */
+QSM_API qsm_status qsm_tkd_batch_device(qsm_ctx* ctx, const qsm_volume* volumes, size_t n,
+                                        const qsm_tkd_params* params);
+
 /* inversion::tkd — src/inversion/tkd.rs:48-99. */
 QSM_API qsm_status qsm_tkd(qsm_ctx* ctx, const double* local_field, const uint8_t* mask, const qsm_grid* grid,
                    const double bdir[3], const qsm_tkd_params* params, double* out_chi);

@@ -116,6 +116,15 @@ qsm_status qsm_tkd_device(qsm_ctx* ctx, const double* f, const uint8_t* m, const
     sync(ctx);
   });
 }
+qsm_status qsm_tkd_batch_device(qsm_ctx* ctx, const qsm_volume* vols, size_t n, const qsm_tkd_params* p) {
+  return guarded(ctx, [&] {
+    if (n == 0) return;
+    check_ptr(vols, "volumes");
+    for (size_t b = 0; b < n; ++b)
+      tkd_device(ctx, vols[b].local_field, vols[b].mask, &vols[b].grid, vols[b].bdir, p, vols[b].out_chi, 0);
+    sync(ctx);
+  });
+}
 qsm_status qsm_tkd(qsm_ctx* ctx, const double* f, const uint8_t* m, const qsm_grid* grid, const double bdir[3],
                    const qsm_tkd_params* p, double* out) {
   return guarded(ctx, [&] {

@@ -401,78 +401,132 @@ __global__ void k_tv_out(long long N, const T* __restrict__ x0, const T* __restr
     out[i] = mask[i] != 0 ? (double)(x0[i] - y[i]) : 0.0;  // apply_mask_zero, src/utils/mask.rs:47-53
 }
 
+// Device buffers, launch shapes and constants of one TV-ADMM volume.
+template <typename T> struct TvVol {
+  GridDims d;
+  Fft3<T> f;
+  OpAdmmMul<T> mul;
+  T* x0;
+  T* yb[2];
+  T* ub[2];
+  T* div;
+  T* mult;
+  cplx_t<T>* spec;
+  double2* partials;
+  TvState* st;
+  dim3 sgrid;
+  int zchunk;
+  bool vec, use_mult;
+  T hx, hy, hz, thr, scale;
+  const uint8_t* mask;
+  double* out;
+};
+
+// Allocate one volume's buffers (workspace names prefixed by `pre`) and enqueue, on
+// ctx->stream, x0 = Re IFFT(F(f) * sym(D * inv_a)), y_0 = x0 (x_0 = 0), u = 0, the
+// per-iteration multiplier and the initial state (st is this volume's device state).
 template <typename T>
-void tv_admm_impl(qsm_ctx* ctx, const GridDims& d, const double* d_f, const uint8_t* d_mask, const double bdir[3],
-                  const qsm_tv_params& p, qsm_progress_fn progress, void* user, double* d_out) {
+void tv_setup(qsm_ctx* ctx, TvVol<T>& v, const std::string& pre, const GridDims& d, const double* d_f,
+              const uint8_t* d_mask, const double bdir[3], const qsm_tv_params& p, TvState* st, double* d_out) {
   using C = cplx_t<T>;
-  Fft3<T> f = make_fft3<T>(ctx, d);
-  KSpace K64 = make_kspace(ctx, d, bdir);
-  KSpaceT<T> KT = make_kspace_t<T>(ctx, d, bdir);
+  v.d = d;
+  v.f = make_fft3<T>(ctx, d);
+  const KSpace K64 = make_kspace(ctx, d, bdir);
+  v.mul = OpAdmmMul<T>{make_kspace_t<T>(ctx, d, bdir), (T)p.rho};
   const long long N = d.n;
-  const long long H = f.g.hsize();
-  const char* pre = sizeof(T) == 4 ? "tv32." : "tv64.";
-  auto nm = [&](const char* s) { return std::string(pre) + s; };
-  T* x0 = ws<T>(ctx, nm("x0"), (size_t)N);
-  T* yb[2] = {ws<T>(ctx, nm("y0"), (size_t)N), ws<T>(ctx, nm("y1"), (size_t)N)};
-  T* ub[2] = {ws<T>(ctx, nm("u0"), (size_t)(3 * N)), ws<T>(ctx, nm("u1"), (size_t)(3 * N))};
-  T* div = ws<T>(ctx, nm("div"), (size_t)N);
-  C* spec = ws<C>(ctx, nm("spec"), (size_t)H);
+  const long long H = v.f.g.hsize();
+  auto nm = [&](const char* s) { return pre + s; };
+  v.x0 = ws<T>(ctx, nm("x0"), (size_t)N);
+  v.yb[0] = ws<T>(ctx, nm("y0"), (size_t)N);
+  v.yb[1] = ws<T>(ctx, nm("y1"), (size_t)N);
+  v.ub[0] = ws<T>(ctx, nm("u0"), (size_t)(3 * N));
+  v.ub[1] = ws<T>(ctx, nm("u1"), (size_t)(3 * N));
+  v.div = ws<T>(ctx, nm("div"), (size_t)N);
+  v.spec = ws<C>(ctx, nm("spec"), (size_t)H);
   // stencil grid: 32x8 threads per block (each thread one x, or one 16-byte vector of
-  // x when nx allows), z split into chunks so that ~3000 blocks run
-  const bool vec = sizeof(T) == 4 && d.nx % Vec16<T>::n == 0;
-  const int xper = vec ? Vec16<T>::n : 1;
+  // x in single precision when nx allows), z split into chunks so that ~3000 blocks run
+  v.vec = sizeof(T) == 4 && d.nx % Vec16<T>::n == 0;
+  const int xper = v.vec ? Vec16<T>::n : 1;
   const int gbx = (d.nx / xper + kStepBX - 1) / kStepBX, gby = (d.ny + kStepBY - 1) / kStepBY;
   int zchunk = (int)std::max<long long>(2, (long long)d.nz * gbx * gby / 3000);
   if (zchunk > d.nz) zchunk = d.nz;
-  const dim3 sgrid(gbx, gby, (d.nz + zchunk - 1) / zchunk);
-  double2* partials = ws<double2>(ctx, nm("partials"), (size_t)sgrid.x * sgrid.y * sgrid.z);
-  TvState* st = ws<TvState>(ctx, nm("state"), 1);
-  const int* done = &st->done;
-  const T scale = (T)(1.0 / (double)N);
-
-  // x0 = Re IFFT(F(f) * sym(D * inv_a)); x_0 = 0 means y_0 = x0
-  run_x_r2c<T>(ctx, f, spec, LoadCast<double, T>{d_f, d.nx}, nullptr);
-  run_yz<T, -1, 1>(ctx, f, spec, spec, OpId<T>{}, nullptr);
-  run_z_fused<T>(ctx, f, spec, spec, OpAdmmRhs<T>{K64, p.rho}, nullptr);
-  run_yz<T, +1, 1>(ctx, f, spec, spec, OpId<T>{}, nullptr);
-  run_x_c2r<T>(ctx, f, spec, StoreReal<T>{x0, d.nx, scale}, nullptr);
-  QSM_CUDA(cudaMemcpyAsync(yb[0], x0, sizeof(T) * N, cudaMemcpyDeviceToDevice, ctx->stream));
-  QSM_CUDA(cudaMemsetAsync(ub[0], 0, sizeof(T) * 3 * N, ctx->stream));
+  v.zchunk = zchunk;
+  v.sgrid = dim3(gbx, gby, (d.nz + zchunk - 1) / zchunk);
+  v.partials = ws<double2>(ctx, nm("partials"), (size_t)v.sgrid.x * v.sgrid.y * v.sgrid.z);
+  v.st = st;
+  v.scale = (T)(1.0 / (double)N);
+  v.hx = (T)(1.0 / d.vsx);
+  v.hy = (T)(1.0 / d.vsy);
+  v.hz = (T)(1.0 / d.vsz);
+  v.thr = (T)(p.lambda / p.rho);
+  v.mask = d_mask;
+  v.out = d_out;
+  run_x_r2c<T>(ctx, v.f, v.spec, LoadCast<double, T>{d_f, d.nx}, nullptr);
+  run_yz<T, -1, 1>(ctx, v.f, v.spec, v.spec, OpId<T>{}, nullptr);
+  run_z_fused<T>(ctx, v.f, v.spec, v.spec, OpAdmmRhs<T>{K64, p.rho}, nullptr);
+  run_yz<T, +1, 1>(ctx, v.f, v.spec, v.spec, OpId<T>{}, nullptr);
+  run_x_c2r<T>(ctx, v.f, v.spec, StoreReal<T>{v.x0, d.nx, v.scale}, nullptr);
+  QSM_CUDA(cudaMemcpyAsync(v.yb[0], v.x0, sizeof(T) * N, cudaMemcpyDeviceToDevice, ctx->stream));
+  QSM_CUDA(cudaMemsetAsync(v.ub[0], 0, sizeof(T) * 3 * N, ctx->stream));
   TvState init{};
   init.k = 1;
   init.tol = p.tol;
   QSM_CUDA(cudaMemcpyAsync(st, &init, sizeof(TvState), cudaMemcpyHostToDevice, ctx->stream));
-
-  const T hx = (T)(1.0 / d.vsx), hy = (T)(1.0 / d.vsy), hz = (T)(1.0 / d.vsz);
-  const T thr = (T)(p.lambda / p.rho);
-  const OpAdmmMul<T> mul{KT, (T)p.rho};
   // precomputed multiplier tiles need P*sizeof(T) >= 16 (always true for the
   // 128-byte tiles; narrow tiles of very long z axes use the in-kernel multiplier)
-  T* mult = ws<T>(ctx, nm("mult"), (size_t)H);
+  v.mult = ws<T>(ctx, nm("mult"), (size_t)H);
   {
     LaunchScope ls(ctx, "admm_mult");
-    k_admm_mult<T><<<grid1d(H), 256, 0, ctx->stream>>>(f.g, K64, p.rho, mult);
+    k_admm_mult<T><<<grid1d(H), 256, 0, ctx->stream>>>(v.f.g, K64, p.rho, v.mult);
     ls.done();
   }
-  const bool use_mult = zm_tile_width<T>(d.nz, f.pz.T) > 0;
-  // iteration i with parity q = i % 2: reads y_{i-1} = yb[1-q], y_{i-2} = yb[q],
-  // u = ub[1-q]; writes u' = ub[q], y_i = yb[q]
-  auto step = [&](int q, int check_only) {
-    LaunchScope ls(ctx, "tv_step");
-    auto kern = vec ? k_tv_step_v<T> : k_tv_step<T>;
-    kern<<<sgrid, dim3(kStepBX, kStepBY), 0, ctx->stream>>>(d.nx, d.ny, d.nz, zchunk, hx, hy, hz, thr, x0, yb[1 - q],
-                                                            yb[q], ub[1 - q], ub[q], div, partials, st, check_only);
-    ls.done();
-  };
-  auto one_iter = [&](int q) {
-    step(q, 0);
-    run_x_r2c<T>(ctx, f, spec, LoadCast<T, T>{div, d.nx}, done);
-    run_yz<T, -1, 1>(ctx, f, spec, spec, OpId<T>{}, done);
-    if (use_mult) run_z_fused_m<T>(ctx, f, spec, spec, mult, done);
-    else run_z_fused<T>(ctx, f, spec, spec, mul, done);
-    run_yz<T, +1, 1>(ctx, f, spec, spec, OpId<T>{}, done);
-    run_x_c2r<T>(ctx, f, spec, StoreReal<T>{yb[q], d.nx, scale}, done);
-  };
+  v.use_mult = zm_tile_width<T>(d.nz, v.f.pz.T) > 0;
+}
+
+// iteration i with parity q = i % 2: reads y_{i-1} = yb[1-q], y_{i-2} = yb[q],
+// u = ub[1-q]; writes u' = ub[q], y_i = yb[q]
+template <typename T> void tv_step_launch(qsm_ctx* ctx, const TvVol<T>& v, int q, int check_only) {
+  LaunchScope ls(ctx, "tv_step");
+  auto kern = v.vec ? k_tv_step_v<T> : k_tv_step<T>;
+  kern<<<v.sgrid, dim3(kStepBX, kStepBY), 0, ctx->stream>>>(v.d.nx, v.d.ny, v.d.nz, v.zchunk, v.hx, v.hy, v.hz,
+                                                              v.thr, v.x0, v.yb[1 - q], v.yb[q], v.ub[1 - q],
+                                                              v.ub[q], v.div, v.partials, v.st, check_only);
+  ls.done();
+}
+
+template <typename T> void tv_iter(qsm_ctx* ctx, const TvVol<T>& v, int q) {
+  const int* done = &v.st->done;
+  tv_step_launch(ctx, v, q, 0);
+  run_x_r2c<T>(ctx, v.f, v.spec, LoadCast<T, T>{v.div, v.d.nx}, done);
+  run_yz<T, -1, 1>(ctx, v.f, v.spec, v.spec, OpId<T>{}, done);
+  if (v.use_mult) run_z_fused_m<T>(ctx, v.f, v.spec, v.spec, v.mult, done);
+  else run_z_fused<T>(ctx, v.f, v.spec, v.spec, v.mul, done);
+  run_yz<T, +1, 1>(ctx, v.f, v.spec, v.spec, OpId<T>{}, done);
+  run_x_c2r<T>(ctx, v.f, v.spec, StoreReal<T>{v.yb[q], v.d.nx, v.scale}, done);
+}
+
+template <typename T> void tv_out_launch(qsm_ctx* ctx, const TvVol<T>& v, size_t completed) {
+  LaunchScope ls(ctx, "tv_out");
+  k_tv_out<T><<<grid1d(v.d.n), 256, 0, ctx->stream>>>(v.d.n, v.x0, v.yb[completed % 2], v.mask, v.out);
+  ls.done();
+}
+
+// Instantiate a captured graph; the launch count it holds is returned in *per.
+inline cudaGraphExec_t instantiate(qsm_ctx* ctx, cudaGraph_t graph) {
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ie != cudaSuccess) throw QsmError(QSM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+  return exec;
+}
+
+template <typename T>
+void tv_admm_impl(qsm_ctx* ctx, const GridDims& d, const double* d_f, const uint8_t* d_mask, const double bdir[3],
+                  const qsm_tv_params& p, qsm_progress_fn progress, void* user, double* d_out) {
+  const char* pre = sizeof(T) == 4 ? "tv32." : "tv64.";
+  TvState* st = ws<TvState>(ctx, std::string(pre) + "state", 1);
+  TvVol<T> v;
+  tv_setup<T>(ctx, v, pre, d, d_f, d_mask, bdir, p, st, d_out);
 
   const size_t max_iter = p.max_iter;
   const bool watch = (progress != nullptr) || (p.tol > 0.0);
@@ -491,17 +545,16 @@ void tv_admm_impl(qsm_ctx* ctx, const GridDims& d, const double* d_f, const uint
   if (ctx->profiling || max_iter < 2) {
     // eager launches (per-kernel timing, or too short to be worth a graph)
     for (size_t it = 1; it <= max_iter && !converged; ++it) {
-      one_iter((int)(it % 2));
+      tv_iter(ctx, v, (int)(it % 2));
       if (watch && (it % 16 == 0)) converged = poll();
     }
   } else {
     cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
     const uint64_t l0 = ctx->launches;
     QSM_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     try {
-      one_iter(1);
-      one_iter(0);
+      tv_iter(ctx, v, 1);
+      tv_iter(ctx, v, 0);
     } catch (...) {
       cudaStreamEndCapture(ctx->stream, &graph);
       if (graph) cudaGraphDestroy(graph);
@@ -510,9 +563,7 @@ void tv_admm_impl(qsm_ctx* ctx, const GridDims& d, const double* d_f, const uint
     QSM_CUDA(cudaStreamEndCapture(ctx->stream, &graph));
     const uint64_t per_pair = ctx->launches - l0;
     ctx->launches = l0;
-    cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (ie != cudaSuccess) throw QsmError(QSM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+    cudaGraphExec_t exec = instantiate(ctx, graph);
     const size_t pairs = max_iter / 2;
     const size_t chunk = 8;  // graph launches (16 iterations) between host polls when watching
     try {
@@ -526,7 +577,7 @@ void tv_admm_impl(qsm_ctx* ctx, const GridDims& d, const double* d_f, const uint
         launched += todo;
         if (watch) converged = poll();
       }
-      if (!converged && (max_iter % 2 == 1)) one_iter(1);
+      if (!converged && (max_iter % 2 == 1)) tv_iter(ctx, v, 1);
     } catch (...) {
       cudaGraphExecDestroy(exec);
       throw;
@@ -537,21 +588,175 @@ void tv_admm_impl(qsm_ctx* ctx, const GridDims& d, const double* d_f, const uint
   size_t completed = converged ? (size_t)hs.conv_iter : max_iter;
   if (!converged && max_iter >= 1 && p.tol > 0.0) {
     // the reference also tests the last iterate (tv.rs:85-91)
-    step((int)((max_iter + 1) % 2), 1);
+    tv_step_launch(ctx, v, (int)((max_iter + 1) % 2), 1);
     converged = poll();
     completed = max_iter;
   }
-  {
-    LaunchScope ls(ctx, "tv_out");
-    k_tv_out<T><<<grid1d(N), 256, 0, ctx->stream>>>(N, x0, yb[completed % 2], d_mask, d_out);
-    ls.done();
-  }
+  tv_out_launch(ctx, v, completed);
   sync(ctx);
   if (progress) {
     for (; reported < completed; ++reported) progress(user, reported + 1, max_iter);
     if (converged) progress(user, completed, completed);
   }
   ctx->tv_last_iters = completed;
+}
+
+// Batched TV-ADMM: every volume keeps its own buffers, grid, field direction and
+// device state; one CUDA graph holds two iterations of every volume as parallel
+// branches on up to 8 streams (volumes placed longest-first on the least-loaded
+// stream), so small volumes run side by side and one graph launch advances the whole
+// batch.  Converged volumes' kernels return at once.  progress(k, n) reports the
+// number of finished volumes.
+template <typename T>
+void tv_admm_batch_impl(qsm_ctx* ctx, const qsm_volume* vols, size_t n, const qsm_tv_params& p,
+                        qsm_progress_fn progress, void* user, size_t* out_iters) {
+  const char* pre = sizeof(T) == 4 ? "tvb32." : "tvb64.";
+  TvState* states = ws<TvState>(ctx, std::string(pre) + "states", n);
+  std::vector<TvVol<T>> V(n);
+  for (size_t b = 0; b < n; ++b) {
+    const GridDims d = check_grid(&vols[b].grid);
+    tv_setup<T>(ctx, V[b], std::string(pre) + std::to_string(b) + ".", d, vols[b].local_field, vols[b].mask,
+                vols[b].bdir, p, states + b, vols[b].out_chi);
+  }
+  // longest-processing-time placement on K branch streams (cost ~ N log N)
+  const int K = (int)std::min<size_t>(n, 8);
+  std::vector<size_t> order(n);
+  for (size_t b = 0; b < n; ++b) order[b] = b;
+  auto cost = [&](size_t b) { return (double)V[b].d.n * std::log2((double)V[b].d.n + 2.0); };
+  std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return cost(a) > cost(b); });
+  std::vector<int> lane(n, 0);
+  std::vector<double> load(K, 0.0);
+  for (size_t b : order) {
+    const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    lane[b] = k;
+    load[k] += cost(b);
+  }
+  std::vector<cudaStream_t> streams(K, nullptr);
+  std::vector<cudaEvent_t> joins(K, nullptr);
+  cudaEvent_t fork = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t s0 = ctx->stream;
+  auto cleanup = [&]() {
+    ctx->stream = s0;
+    if (exec) cudaGraphExecDestroy(exec);
+    for (auto& e : joins)
+      if (e) cudaEventDestroy(e);
+    if (fork) cudaEventDestroy(fork);
+    for (auto& s : streams)
+      if (s) cudaStreamDestroy(s);
+  };
+  try {
+    QSM_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    for (int k = 0; k < K; ++k) {
+      QSM_CUDA(cudaStreamCreateWithFlags(&streams[k], cudaStreamNonBlocking));
+      QSM_CUDA(cudaEventCreateWithFlags(&joins[k], cudaEventDisableTiming));
+    }
+    // one step of every volume on its branch stream; `pair` = two iterations
+    auto enqueue = [&](bool pair, int q_single) {
+      QSM_CUDA(cudaEventRecord(fork, s0));
+      for (int k = 0; k < K; ++k) QSM_CUDA(cudaStreamWaitEvent(streams[k], fork, 0));
+      for (size_t b : order) {
+        ctx->stream = streams[lane[b]];
+        if (pair) {
+          tv_iter(ctx, V[b], 1);
+          tv_iter(ctx, V[b], 0);
+        } else {
+          tv_iter(ctx, V[b], q_single);
+        }
+      }
+      ctx->stream = s0;
+      for (int k = 0; k < K; ++k) {
+        QSM_CUDA(cudaEventRecord(joins[k], streams[k]));
+        QSM_CUDA(cudaStreamWaitEvent(s0, joins[k], 0));
+      }
+    };
+    const size_t max_iter = p.max_iter;
+    std::vector<TvState> hs(n);
+    size_t finished = 0;
+    auto poll = [&]() {
+      QSM_CUDA(cudaMemcpyAsync(hs.data(), states, sizeof(TvState) * n, cudaMemcpyDeviceToHost, s0));
+      QSM_CUDA(cudaStreamSynchronize(s0));
+      size_t f = 0;
+      for (size_t b = 0; b < n; ++b) f += hs[b].done != 0;
+      if (progress)
+        for (; finished < f; ++finished) progress(user, finished + 1, n);
+      return f == n;
+    };
+    bool all_done = false;
+    const size_t pairs = max_iter / 2;
+    if (pairs > 0 && ctx->profiling) {
+      // eager launches for per-kernel timing
+      for (size_t it = 0; it < pairs && !all_done; ++it) {
+        enqueue(true, 0);
+        if (p.tol > 0.0 && (it + 1) % 8 == 0) all_done = poll();
+      }
+    } else if (pairs > 0) {
+      cudaGraph_t graph = nullptr;
+      const uint64_t l0 = ctx->launches;
+      QSM_CUDA(cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal));
+      try {
+        enqueue(true, 0);
+      } catch (...) {
+        ctx->stream = s0;
+        cudaStreamEndCapture(s0, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        throw;
+      }
+      QSM_CUDA(cudaStreamEndCapture(s0, &graph));
+      const uint64_t per = ctx->launches - l0;
+      ctx->launches = l0;
+      exec = instantiate(ctx, graph);
+      const bool watch = p.tol > 0.0;
+      size_t launched = 0;
+      while (launched < pairs && !all_done) {
+        const size_t todo = watch ? std::min<size_t>(8, pairs - launched) : (pairs - launched);
+        for (size_t c = 0; c < todo; ++c) {
+          QSM_CUDA(cudaGraphLaunch(exec, s0));
+          ctx->launches += per;
+        }
+        launched += todo;
+        if (watch) all_done = poll();
+      }
+    }
+    if (!all_done && (max_iter % 2 == 1)) enqueue(false, 1);
+    all_done = poll();
+    for (size_t b = 0; b < n; ++b) {
+      size_t completed = hs[b].done ? (size_t)hs[b].conv_iter : max_iter;
+      if (!hs[b].done && max_iter >= 1 && p.tol > 0.0) {
+        tv_step_launch(ctx, V[b], (int)((max_iter + 1) % 2), 1);  // last-iterate test (tv.rs:85-91)
+        completed = max_iter;
+      }
+      tv_out_launch(ctx, V[b], completed);
+      if (out_iters) out_iters[b] = completed;
+    }
+    poll();
+    if (progress)
+      for (; finished < n; ++finished) progress(user, finished + 1, n);
+  } catch (...) {
+    cleanup();
+    throw;
+  }
+  cleanup();
+}
+
+void tv_batch_device(qsm_ctx* ctx, const qsm_volume* vols, size_t n, const qsm_tv_params* p,
+                     qsm_progress_fn progress, void* user, size_t* out_iters) {
+  check_ptr(p, "params");
+  check_finite(p->lambda, "lambda");
+  check_finite(p->rho, "rho");
+  if (std::isnan(p->tol)) throw QsmError(QSM_ERR_INVALID_ARGUMENT, "tol is NaN");
+  if (n == 0) return;
+  check_ptr(vols, "volumes");
+  for (size_t b = 0; b < n; ++b) {
+    check_grid(&vols[b].grid);
+    check_ptr(vols[b].local_field, "local_field");
+    check_ptr(vols[b].mask, "mask");
+    check_ptr(vols[b].out_chi, "out_chi");
+    check_bdir(vols[b].bdir);
+  }
+  if (ctx->precision == QSM_PRECISION_MIXED) tv_admm_batch_impl<float>(ctx, vols, n, *p, progress, user, out_iters);
+  else tv_admm_batch_impl<double>(ctx, vols, n, *p, progress, user, out_iters);
+  sync(ctx);
 }
 
 void tv_device(qsm_ctx* ctx, const double* f, const uint8_t* m, const qsm_grid* grid, const double bdir[3],
@@ -599,5 +804,41 @@ qsm_status qsm_tv_admm(qsm_ctx* ctx, const double* local_field, const uint8_t* m
 }
 
 size_t qsm_tv_last_iterations(const qsm_ctx* ctx) { return ctx ? ctx->tv_last_iters : 0; }
+
+qsm_status qsm_tv_admm_batch_device(qsm_ctx* ctx, const qsm_volume* vols, size_t n, const qsm_tv_params* params,
+                                    qsm_progress_fn progress, void* user, size_t* out_iterations) {
+  return guarded(ctx, [&] { tv_batch_device(ctx, vols, n, params, progress, user, out_iterations); });
+}
+
+qsm_status qsm_tv_admm_batch(qsm_ctx* ctx, const qsm_volume* vols, size_t n, const qsm_tv_params* params,
+                             qsm_progress_fn progress, void* user, size_t* out_iterations) {
+  return guarded(ctx, [&] {
+    if (n == 0) return;
+    check_ptr(vols, "volumes");
+    // stage every volume on the device, solve the batch, copy every result back
+    std::vector<qsm_volume> dv(vols, vols + n);
+    for (size_t b = 0; b < n; ++b) {
+      const GridDims d = check_grid(&vols[b].grid);
+      check_ptr(vols[b].local_field, "local_field");
+      check_ptr(vols[b].mask, "mask");
+      check_ptr(vols[b].out_chi, "out_chi");
+      const std::string k = "iob." + std::to_string(b) + ".";
+      double* f = ws<double>(ctx, k + "in", (size_t)d.n);
+      uint8_t* m = ws<uint8_t>(ctx, k + "mask", (size_t)d.n);
+      double* o = ws<double>(ctx, k + "out", (size_t)d.n);
+      h2d(ctx, f, vols[b].local_field, sizeof(double) * d.n);
+      h2d(ctx, m, vols[b].mask, (size_t)d.n);
+      dv[b].local_field = f;
+      dv[b].mask = m;
+      dv[b].out_chi = o;
+    }
+    tv_batch_device(ctx, dv.data(), n, params, progress, user, out_iterations);
+    for (size_t b = 0; b < n; ++b) {
+      const GridDims d = check_grid(&vols[b].grid);
+      d2h(ctx, vols[b].out_chi, dv[b].out_chi, sizeof(double) * d.n);
+    }
+    sync(ctx);
+  });
+}
 
 }  // extern "C"

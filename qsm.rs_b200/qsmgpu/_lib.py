@@ -70,6 +70,11 @@ class QsmTgvParams(C.Structure):
                 ("step_size", C.c_float), ("fieldstrength", C.c_float), ("te", C.c_float), ("tol", C.c_float)]
 
 
+class QsmVolume(C.Structure):
+    _fields_ = [("local_field", C.c_void_p), ("mask", C.c_void_p), ("out_chi", C.c_void_p), ("grid", QsmGrid),
+                ("bdir", C.c_double * 3)]
+
+
 class QsmScanMetadata(C.Structure):
     _fields_ = [("nx", C.c_size_t), ("ny", C.c_size_t), ("nz", C.c_size_t),
                 ("vsx", C.c_double), ("vsy", C.c_double), ("vsz", C.c_double),
@@ -105,6 +110,11 @@ _SIGS = [
     ("qsm_grid_supported", C.c_int, [C.POINTER(QsmGrid)]),
     ("qsm_tv_params_default", None, [C.POINTER(QsmTvParams)]),
     ("qsm_ilsqr_params_default", None, [C.POINTER(QsmIlsqrParams)]),
+    ("qsm_tv_admm_batch", C.c_int, [C.c_void_p, C.POINTER(QsmVolume), C.c_size_t, C.POINTER(QsmTvParams),
+                                    PROGRESS_FN, C.c_void_p, C.POINTER(C.c_size_t)]),
+    ("qsm_tv_admm_batch_device", C.c_int, [C.c_void_p, C.POINTER(QsmVolume), C.c_size_t, C.POINTER(QsmTvParams),
+                                           PROGRESS_FN, C.c_void_p, C.POINTER(C.c_size_t)]),
+    ("qsm_tkd_batch_device", C.c_int, [C.c_void_p, C.POINTER(QsmVolume), C.c_size_t, C.POINTER(QsmTkdParams)]),
     ("qsm_apply_reference", C.c_int, [C.c_void_p, c_double_p, c_u8_p, C.c_size_t, C.c_int, c_double_p]),
     ("qsm_run_tgv", C.c_int, [C.c_void_p, C.POINTER(c_double_p), C.c_size_t, C.c_size_t, c_u8_p,
                               C.POINTER(QsmScanMetadata), C.POINTER(QsmTgvParams), C.c_int, PROGRESS_FN,

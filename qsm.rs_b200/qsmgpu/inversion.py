@@ -255,3 +255,57 @@ def tgv_oblique_stencil(res=(1.0, 1.0, 1.0), b0_dir=(0.0, 0.0, 1.0)):
     if lib.qsm_tgv_oblique_stencil(r, b, out) != 0:
         raise RuntimeError("qsm_tgv_oblique_stencil failed")
     return np.frombuffer(out, dtype=np.float32).reshape(3, 3, 3).copy()
+
+
+def tv_admm_batch(cases, params: TvParams = TvParams(), progress: Optional[Callable[[int, int], None]] = None, *,
+                  ctx: Optional[Context] = None):
+    """TV-ADMM over a batch of volumes in one call: cases is a sequence of
+    (local_field, mask, grid, bdir).  Returns (list of chi arrays, list of iteration
+    counts).  progress(k, n) counts finished volumes."""
+    c = _ctx(ctx)
+    keep, outs = [], []
+    arr = (_lib.QsmVolume * max(len(cases), 1))()
+    for b, (field, mask, grid, bdir) in enumerate(cases):
+        f = _as_f64(field, grid, "local_field")
+        m = _as_u8(mask, "mask")
+        _check_len(f, grid, "local_field")
+        _check_len(m, grid, "mask")
+        o = np.empty_like(f)
+        keep += [f, m]
+        outs.append(o)
+        arr[b].local_field = f.ctypes.data
+        arr[b].mask = m.ctypes.data
+        arr[b].out_chi = o.ctypes.data
+        arr[b].grid = grid._c()
+        arr[b].bdir = (C.c_double * 3)(*bdir)
+    iters = (C.c_size_t * max(len(cases), 1))()
+    p = params._c()
+    cb, _cbkeep = _progress(progress)
+    _check(c, c._lib.qsm_tv_admm_batch(c.handle, arr, len(cases), C.byref(p), cb, None, iters))
+    return outs, [int(iters[b]) for b in range(len(cases))]
+
+
+def tv_admm_batch_device(ctx: Context, cases, params: TvParams, progress=None):
+    """Device form: cases is a sequence of (d_field, d_mask, d_out, grid, bdir) with
+    device pointers as ints.  Returns the iteration counts."""
+    arr = (_lib.QsmVolume * max(len(cases), 1))()
+    for b, (df, dm, do, grid, bdir) in enumerate(cases):
+        arr[b].local_field, arr[b].mask, arr[b].out_chi = df, dm, do
+        arr[b].grid = grid._c()
+        arr[b].bdir = (C.c_double * 3)(*bdir)
+    iters = (C.c_size_t * max(len(cases), 1))()
+    p = params._c()
+    cb, _cbkeep = _progress(progress)
+    _check(ctx, ctx._lib.qsm_tv_admm_batch_device(ctx.handle, arr, len(cases), C.byref(p), cb, None, iters))
+    return [int(iters[b]) for b in range(len(cases))]
+
+
+def tkd_batch_device(ctx: Context, cases, params: TkdParams):
+    """TKD over a batch: cases as for tv_admm_batch_device."""
+    arr = (_lib.QsmVolume * max(len(cases), 1))()
+    for b, (df, dm, do, grid, bdir) in enumerate(cases):
+        arr[b].local_field, arr[b].mask, arr[b].out_chi = df, dm, do
+        arr[b].grid = grid._c()
+        arr[b].bdir = (C.c_double * 3)(*bdir)
+    p = params._c()
+    _check(ctx, ctx._lib.qsm_tkd_batch_device(ctx.handle, arr, len(cases), C.byref(p)))
