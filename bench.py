@@ -35,7 +35,7 @@ METRIC = "TV-ADMM volumes/s at 256x256x176 (250 iterations)"
 # DRAM bytes (read + write) per launch of the dominant kernels, from one ncu --set full
 # capture of this workload (profiles/tv_admm_256x256x176_kernels.md); ncu flushes the
 # caches before each replay, so these are cold-cache figures.
-NCU_TRAFFIC = {"tv_step": 441453056, "fft_z_fused": 77602560}
+NCU_TRAFFIC = {"tv_step": 432803840, "fft_z_fused": 75244032}
 NCU_TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/tv_admm_256x256x176_kernels.md"
 UNIT = "volumes/s"
 
@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-cpu-baseline", action="store_true")
     ap.add_argument("--skip-fp64", action="store_true")
+    ap.add_argument("--skip-extras", action="store_true",
+                    help="skip the full-chain and 32-volume batch measurements (reported beside the headline)")
     ap.add_argument("--one-shot", type=int, default=0, metavar="ITERS",
                     help="profiling aid: run one TV-ADMM solve of ITERS iterations (mixed) and exit")
     ap.add_argument("--one-shot-precision", default="mixed", choices=["mixed", "f64"])
@@ -206,6 +208,128 @@ def cpu_baseline_tv(f, mask, budget_iters=4):
             "sample": f"oracle TV-ADMM at {DIMS[0]}x{DIMS[1]}x{DIMS[2]}: preparation + {budget_iters} iterations "
                       f"timed, scaled to {ITERS} ({t_iter * 1e3:.0f} ms/iteration, scipy.fft workers={cores})",
             "ms_per_iteration": t_iter * 1e3}
+
+
+def _fast_size(n):
+    """Smallest 2^a 3^b 5^c >= n (src/utils/padding.rs:9)."""
+    m = n
+    while True:
+        k = m
+        for p in (2, 3, 5):
+            while k % p == 0:
+                k //= p
+        if k == 1:
+            return m
+        m += 1
+
+
+def _timed(stream, fn, reps=1):
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def bench_chain(local, dev):
+    """Full chain at 256x256x176 (wrapped phase -> laplacian_unwrap -> ppm -> vsharp with
+    default radii -> tv_admm 250 iterations), mixed precision, stage times with CUDA events
+    and each stage's rel-L2 error against the FP64 GPU chain on the same input."""
+    import torch
+    import qsmgpu
+    from qsmgpu import Grid, inversion, unwrap, bgremove, phantom
+    case = phantom.chain_case()
+    grid = Grid.new(*case.dims)
+    N = case.mask.size
+    ph = torch.from_numpy(np.ascontiguousarray(case.wrapped_phase).ravel()).to(dev)
+    m = torch.from_numpy(np.ascontiguousarray(case.mask).ravel()).to(dev)
+    radii = bgremove.vsharp_radii()
+    out = {}
+    for prec in ("mixed", "f64"):
+        ctx = qsmgpu.Context(local, prec)
+        s = torch.cuda.ExternalStream(ctx.stream_handle(), device=dev)
+        uw = torch.empty(N, dtype=torch.float64, device=dev)
+        loc = torch.empty_like(uw)
+        fm = torch.empty(N, dtype=torch.uint8, device=dev)
+        chi = torch.empty_like(uw)
+        p = inversion.TvParams(2e-4, 2e-2, 0.0, ITERS)
+
+        def st_unwrap():
+            unwrap.laplacian_unwrap_device(ctx, ph.data_ptr(), m.data_ptr(), grid, uw.data_ptr())
+
+        def st_vsharp():
+            fppm = uw / case.rad_per_ppm
+            bgremove.vsharp_with_radii_device(ctx, fppm.data_ptr(), m.data_ptr(), grid, radii, 0.05, loc.data_ptr(),
+                                              fm.data_ptr())
+
+        def st_tv():
+            inversion.tv_admm_device(ctx, loc.data_ptr(), fm.data_ptr(), grid, (0.0, 0.0, 1.0), p, chi.data_ptr())
+
+        st_unwrap(), st_vsharp(), st_tv()  # warm-up
+        times = {"unwrap": _timed(s, st_unwrap), "vsharp": _timed(s, st_vsharp), "tv_admm": _timed(s, st_tv)}
+        out[prec] = {"ms": {k: round(v, 3) for k, v in times.items()},
+                     "arrays": (uw.cpu().numpy(), loc.cpu().numpy(), fm.cpu().numpy(), chi.cpu().numpy())}
+        ctx.close()
+    a, b = out["mixed"]["arrays"], out["f64"]["arrays"]
+    rl = lambda x, y: float(np.linalg.norm(x - y) / (np.linalg.norm(y) or 1.0))
+    return {"workload": "wrapped phase 256x256x176, 3 T, TE 20 ms -> laplacian_unwrap -> vsharp (12 radii) -> "
+                        f"tv_admm x{ITERS}; synthetic brain-mask phantom with 4 background dipoles",
+            "ms_mixed": out["mixed"]["ms"], "ms_f64": out["f64"]["ms"],
+            "rel_l2_mixed_vs_fp64": {"unwrap": rl(a[0], b[0]), "vsharp": rl(a[1], b[1]), "tv_admm": rl(a[3], b[3])},
+            "vsharp_mask_equal": bool(np.array_equal(a[2], b[2]))}
+
+
+def bench_batch(local, dev, n_vol=32, seed=7):
+    """32 volumes, each dimension from {96..224} x {96..224} x {64..160} rounded to
+    2^a 3^b 5^c, B0 tilted up to 25 degrees, ellipsoid phantom + noise: batched TV-ADMM
+    (250 iterations, mixed) and TKD (threshold 0.19) in one call each, against the same
+    volumes solved one call at a time."""
+    import torch
+    import qsmgpu
+    from qsmgpu import Grid, inversion, phantom
+    rng = np.random.default_rng(seed)
+    ctx = qsmgpu.Context(local, "mixed")
+    s = torch.cuda.ExternalStream(ctx.stream_handle(), device=dev)
+    cases, keep, vox = [], [], 0
+    for _ in range(n_vol):
+        nx, ny = (_fast_size(int(rng.integers(96, 225))) for _ in range(2))
+        nz = _fast_size(int(rng.integers(64, 161)))
+        th, ph = np.radians(rng.uniform(0, 25)), rng.uniform(0, 2 * np.pi)
+        bdir = (float(np.sin(th) * np.cos(ph)), float(np.sin(th) * np.sin(ph)), float(np.cos(th)))
+        grid = Grid.new(nx, ny, nz)
+        shape = (nz, ny, nx)
+        mask = phantom.ellipsoid_mask(shape, (0.4 * nx, 0.45 * ny, 0.4 * nz))
+        chi = np.zeros(shape)
+        ctr = ((nx - 1) / 2, (ny - 1) / 2, (nz - 1) / 2)
+        phantom.add_ellipsoids(chi, rng, 8, [(c - 0.25 * n, c + 0.25 * n) for c, n in zip(ctr, (nx, ny, nz))],
+                               semi=(3.0, 10.0))
+        chi *= mask
+        dchi = torch.from_numpy(chi.ravel()).to(dev)
+        f = torch.empty_like(dchi)
+        inversion.dipole_forward_device(ctx, dchi.data_ptr(), grid, bdir, f.data_ptr())
+        f += torch.from_numpy(rng.normal(0.0, 0.01, size=chi.size) * mask.ravel()).to(dev)
+        dm = torch.from_numpy(mask.ravel()).to(dev)
+        do = torch.empty_like(f)
+        keep += [f, dm, do]
+        cases.append((f.data_ptr(), dm.data_ptr(), do.data_ptr(), grid, bdir))
+        vox += chi.size
+    p = inversion.TvParams(2e-4, 2e-2, 0.0, ITERS)
+    inversion.tv_admm_batch_device(ctx, cases, p)  # warm-up
+    t_batch = _timed(s, lambda: inversion.tv_admm_batch_device(ctx, cases, p))
+    t_seq = _timed(s, lambda: [inversion.tv_admm_device(ctx, df, dm, g, b, p, do) for df, dm, do, g, b in cases])
+    tk = inversion.TkdParams(0.19)
+    inversion.tkd_batch_device(ctx, cases, tk)
+    t_tkd = _timed(s, lambda: inversion.tkd_batch_device(ctx, cases, tk), reps=3)
+    ctx.close()
+    return {"workload": f"{n_vol} volumes of uneven size (2^a 3^b 5^c in 96-224 x 96-224 x 64-160), B0 tilted "
+                        f"<= 25 deg, TV-ADMM x{ITERS} + TKD 0.19, mixed; {vox / 1e6:.1f} M voxels in total",
+            "tv_admm_batched": {"volumes_per_s": round(n_vol / (t_batch / 1e3), 3), "ms": round(t_batch, 2)},
+            "tv_admm_one_call_per_volume": {"volumes_per_s": round(n_vol / (t_seq / 1e3), 3), "ms": round(t_seq, 2)},
+            "tkd_batched": {"volumes_per_s": round(n_vol / (t_tkd / 1e3), 3), "ms": round(t_tkd, 3)}}
 
 
 def run_reference(args):
@@ -388,6 +512,10 @@ def main():
                  "mixed_vs_fp64_speedup": round(ms64 / ms_step, 3),
                  "rel_l2_mixed_vs_fp64": err, "max_abs_mixed_vs_fp64": float(np.abs(chi_mixed - chi64).max())}
         ctx64.close()
+
+    if rank == 0 and world == 1 and not args.skip_extras:
+        extra["chain_256x256x176"] = bench_chain(local, dev)
+        extra["batch_32_volumes"] = bench_batch(local, dev)
 
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu_baseline:

@@ -218,6 +218,8 @@ QSM_API qsm_status qsm_tikhonov_device(qsm_ctx* ctx, const double* d_local_field
  * apply_dipole_inplace), used to synthesise local fields. */
 QSM_API qsm_status qsm_dipole_forward(qsm_ctx* ctx, const double* chi, const qsm_grid* grid, const double bdir[3],
                               double* out_field);
+QSM_API qsm_status qsm_dipole_forward_device(qsm_ctx* ctx, const double* d_chi, const qsm_grid* grid,
+                                             const double bdir[3], double* d_out_field);
 
 /* ---------------------------------------------------------------- unwrap ---- */
 /* unwrap::laplacian_unwrap — src/unwrap/laplacian.rs:135-161. */

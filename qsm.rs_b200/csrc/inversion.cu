@@ -176,6 +176,19 @@ qsm_status qsm_tikhonov(qsm_ctx* ctx, const double* f, const uint8_t* m, const q
   });
 }
 
+qsm_status qsm_dipole_forward_device(qsm_ctx* ctx, const double* d_chi, const qsm_grid* grid, const double bdir[3],
+                                     double* d_out_field) {
+  return guarded(ctx, [&] {
+    GridDims d = check_grid(grid);
+    check_ptr(d_chi, "chi");
+    check_ptr(d_out_field, "out_field");
+    check_bdir(bdir);
+    KSpace K = make_kspace(ctx, d, bdir);
+    closed_form(ctx, d, d_chi, nullptr, OpDipole<float>{K}, OpDipole<double>{K}, d_out_field);
+    sync(ctx);
+  });
+}
+
 qsm_status qsm_dipole_forward(qsm_ctx* ctx, const double* chi, const qsm_grid* grid, const double bdir[3],
                               double* out_field) {
   return guarded(ctx, [&] {

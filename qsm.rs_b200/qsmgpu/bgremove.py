@@ -123,3 +123,23 @@ def cg_kspace_normal_device(ctx: Context, grid: Grid, d_kernel_spectrum: int, d_
                                                      C.c_void_p(d_weight or None), float(lam), C.c_void_p(d_b),
                                                      C.c_void_p(d_x0 or None), float(tol), int(max_iter), cb, None,
                                                      C.c_void_p(d_x)))
+
+
+def vsharp_radii(params: VsharpParams = VsharpParams()):
+    """Descending radii max, max - min, ... while >= min (src/bgremove/vsharp.rs:70-82)."""
+    radii, r = [], params.max_radius
+    while r >= params.min_radius:
+        radii.append(r)
+        r -= params.min_radius
+    return radii or [params.max_radius]
+
+
+def vsharp_with_radii_device(ctx: Context, d_field: int, d_mask: int, grid: Grid, radii: Sequence[float],
+                             threshold: float, d_out_local: int, d_out_mask: int, progress=None):
+    """Device-pointer form of vsharp_with_radii (src/bgremove/vsharp.rs:88-199)."""
+    r = np.ascontiguousarray(np.asarray(radii, dtype=np.float64))
+    g = grid._c()
+    cb, _keep = _progress(progress)
+    _check(ctx, ctx._lib.qsm_vsharp_with_radii_device(ctx.handle, C.c_void_p(d_field), C.c_void_p(d_mask), C.byref(g),
+                                                      _ptr_d(r), r.size, float(threshold), cb, None,
+                                                      C.c_void_p(d_out_local), C.c_void_p(d_out_mask)))

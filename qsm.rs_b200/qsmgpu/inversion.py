@@ -151,6 +151,13 @@ def dipole_forward(chi, grid: Grid, bdir=(0.0, 0.0, 1.0), *, ctx: Optional[Conte
     return out
 
 
+def dipole_forward_device(ctx: Context, d_chi: int, grid: Grid, bdir, d_out: int):
+    """Device-pointer form of dipole_forward."""
+    b, _keep = _bdir(bdir)
+    g = grid._c()
+    _check(ctx, ctx._lib.qsm_dipole_forward_device(ctx.handle, C.c_void_p(d_chi), C.byref(g), b, C.c_void_p(d_out)))
+
+
 def ilsqr(local_field, mask, grid: Grid, bdir=(0.0, 0.0, 1.0), params: IlsqrParams = IlsqrParams(),
           progress: Optional[Callable[[int, int], None]] = None, *, ctx: Optional[Context] = None):
     """inversion::ilsqr (src/inversion/ilsqr.rs:1307-1351) -> (chi, xsa, xfs, xlsqr).
