@@ -156,6 +156,20 @@ QSM_API qsm_status qsm_tv_admm_batch_device(qsm_ctx* ctx, const qsm_volume* volu
 QSM_API qsm_status qsm_tkd_batch_device(qsm_ctx* ctx, const qsm_volume* volumes, size_t n,
                                         const qsm_tkd_params* params);
 
+/* Differentiable unrolled TV-ADMM (no counterpart in the reference): `iterations` fixed
+ * iterations of inversion::tv_admm (tol = 0, so the forward result equals qsm_tv_admm_device
+ * with max_iter = iterations) and, when d_grad_chi (dL/dchi, nx*ny*nz values) is not NULL,
+ * the vector-Jacobian product: dL/d(local_field) into d_out_grad_field and dL/dlambda into
+ * *out_grad_lambda (rho is held fixed).  The adjoint sweep recomputes the forward states
+ * from checkpoints taken every `checkpoint_every` iterations.  The shrink derivative
+ * is 1 where |v| > lambda/rho, else 0.  Device pointers; every axis >= 1, fewer than
+ * 2^32 voxels. */
+QSM_API qsm_status qsm_tv_admm_unrolled_vjp_device(qsm_ctx* ctx, const double* d_local_field, const uint8_t* d_mask,
+                                                   const qsm_grid* grid, const double bdir[3], double lambda,
+                                                   double rho, size_t iterations, size_t checkpoint_every,
+                                                   const double* d_grad_chi, double* d_out_chi,
+                                                   double* d_out_grad_field, double* out_grad_lambda);
+
 /* inversion::tkd — src/inversion/tkd.rs:48-99. */
 QSM_API qsm_status qsm_tkd(qsm_ctx* ctx, const double* local_field, const uint8_t* mask, const qsm_grid* grid,
                    const double bdir[3], const qsm_tkd_params* params, double* out_chi);

@@ -12,6 +12,9 @@ void* ws_get(qsm_ctx* ctx, const std::string& name, size_t bytes) {
   if (bytes == 0) bytes = 16;
   DevBuf& b = ctx->ws[name];
   if (b.bytes < bytes) {
+    // growing frees the old buffer: a pointer handed out earlier in this call would dangle
+    if (b.p && b.epoch == ctx->epoch)
+      throw QsmError(QSM_ERR_CUDA, "internal error: workspace '" + name + "' grown after use in the same call");
     if (b.p) {
       QSM_CUDA(cudaStreamSynchronize(ctx->stream));
       QSM_CUDA(cudaFree(b.p));
@@ -28,6 +31,7 @@ void* ws_get(qsm_ctx* ctx, const std::string& name, size_t bytes) {
     b.p = p;
     b.bytes = bytes;
   }
+  b.epoch = ctx->epoch;
   return b.p;
 }
 

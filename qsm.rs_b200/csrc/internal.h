@@ -31,6 +31,7 @@ struct QsmError : std::runtime_error {
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
+  uint64_t epoch = 0;  // API call that last handed the pointer out
 };
 
 struct GraphCache {
@@ -58,6 +59,7 @@ struct qsm_ctx {
   cudaStream_t stream = nullptr;
   std::string err;
   std::map<std::string, qsm::DevBuf> ws;
+  uint64_t epoch = 0;  // incremented by every API call (guarded)
   std::map<long long, void*> twiddles;  // key n*2 + (double ? 1 : 0)
   std::map<std::string, void*> tables;  // small per-grid tables
   std::map<std::string, qsm::GraphCache> graphs;
@@ -121,6 +123,7 @@ void prof_collect(qsm_ctx* ctx);
 // Run fn and convert exceptions into a status + last error string.
 template <class F> qsm_status guarded(qsm_ctx* ctx, F&& fn) {
   if (ctx == nullptr) return QSM_ERR_INVALID_ARGUMENT;
+  ctx->epoch++;
   try {
     QSM_CUDA(cudaSetDevice(ctx->device));
     fn();

@@ -120,8 +120,12 @@ qsm_status qsm_tkd_batch_device(qsm_ctx* ctx, const qsm_volume* vols, size_t n, 
   return guarded(ctx, [&] {
     if (n == 0) return;
     check_ptr(vols, "volumes");
-    for (size_t b = 0; b < n; ++b)
+    for (size_t b = 0; b < n; ++b) {
+      // volumes share the transform workspaces: the previous volume's pointers are dead
+      // here, so the buffers may be regrown
+      ctx->epoch++;
       tkd_device(ctx, vols[b].local_field, vols[b].mask, &vols[b].grid, vols[b].bdir, p, vols[b].out_chi, 0);
+    }
     sync(ctx);
   });
 }

@@ -1,0 +1,512 @@
+// TV-ADMM building blocks shared by the solver, the batched solver and the unrolled
+// adjoint: the stencil kernels, the per-iteration multiplier, and the per-volume
+// setup / iteration / output launchers.
+#pragma once
+
+#include "functors.cuh"
+#include "solvers.h"
+
+#include <algorithm>
+
+namespace qsm {
+
+template <typename S> __device__ __forceinline__ S sabs(S x) { return x < S(0) ? -x : x; }
+
+// inv_a = 1/(D^2 + rho*Lneg), 0 where |a| <= 1e-20 (src/inversion/admm.rs:164-168)
+template <typename S>
+__device__ __forceinline__ S admm_inv_a(const KSpaceT<S>& K, S kx, S ky, S kz, int ix, int iy, int iz, S rho) {
+  const S d = K.dipole(kx, ky, kz);
+  const S a = d * d + rho * K.lapneg(ix, iy, iz);
+  return sabs(a) > S(1e-20) ? S(1) / a : S(0);
+}
+
+// x0 = Re IFFT(F(f) * D * inv_a) (admm.rs:169-176), multiplier in double
+template <typename T> struct OpAdmmRhs {
+  using C = cplx_t<T>;
+  KSpace K;
+  double rho;
+  __device__ __forceinline__ C mid(C v, int ix, int iy, int iz, long long) const {
+    const KSpace& k = K;
+    const double r = rho;
+    const double m = K.sym(ix, iy, iz, [&](double kx, double ky, double kz, int a, int b, int c) {
+      return k.dipole(kx, ky, kz) * admm_inv_a<double>(k, kx, ky, kz, a, b, c, r);
+    });
+    return cscale(v, (T)m);
+  }
+};
+
+// per-iteration multiplier rho * sym(inv_a) (admm.rs:105-108), working precision
+template <typename T> struct OpAdmmMul {
+  using C = cplx_t<T>;
+  KSpaceT<T> K;
+  T rho;
+  __device__ __forceinline__ C mid(C v, int ix, int iy, int iz, long long) const {
+    const KSpaceT<T>& k = K;
+    const T r = rho;
+    const T ia = K.sym(ix, iy, iz, [&](T kx, T ky, T kz, int a, int b, int c) {
+      return admm_inv_a<T>(k, kx, ky, kz, a, b, c, r);
+    });
+    return cscale(v, r * ia);
+  }
+};
+
+// Per-iteration multiplier rho*sym(inv_a) as a real half-spectrum array (spectrum
+// layout, padding columns 0), evaluated once per solve in double.
+template <typename T>
+__global__ void k_admm_mult(Geom g, KSpace K, double rho, T* __restrict__ out) {
+  const long long H = g.hsize();
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < H; i += (long long)gridDim.x * blockDim.x) {
+    const int ix = (int)(i % g.pitch);
+    const long long r = i / g.pitch;
+    const int iy = (int)(r % g.ny);
+    const int iz = (int)(r / g.ny);
+    double m = 0.0;
+    if (ix < g.nxh) {
+      const KSpace& k = K;
+      m = rho * K.sym(ix, iy, iz, [&](double kx, double ky, double kz, int a, int b, int c) {
+        return admm_inv_a<double>(k, kx, ky, kz, a, b, c, rho);
+      });
+    }
+    out[i] = (T)m;
+  }
+}
+
+template <typename T> struct StoreReal {
+  T* __restrict__ out;
+  int nx;
+  T scale;
+  __device__ __forceinline__ void operator()(int row, int e, T v) { out[(long long)row * nx + e] = v * scale; }
+  __device__ __forceinline__ void finish() {}
+};
+
+struct TvState {
+  int done;       // 1 once relative_change < tol
+  int k;          // iteration whose k_tv_step runs next (1-based)
+  unsigned counter;
+  int conv_iter;  // iteration that converged
+  double tol;
+  double rc;      // last relative change
+};
+
+// Convergence test of x_{k-1} (k >= 2) + z/u update + divergence, periodic BC
+// (src/utils/gradient.rs:21-108, src/utils/mod.rs:44-77, src/inversion/admm.rs:117-142).
+// x_j = x0 - y_j.  u is read from ui and written to uo; the backward neighbours' g
+// components are recomputed from x and ui there.
+//
+// blockDim = (32, 8): a warp spans 32 consecutive x, so x-neighbours come from
+// shuffles; each thread marches through `zchunk` planes keeping x at k-1, k, k+1 and
+// u_z at k-1 in registers.  grid = (ceil(nx/32), ceil(ny/8), ceil(nz/zchunk)).
+constexpr int kStepBX = 32, kStepBY = 8;
+
+template <typename T>
+__global__ void __launch_bounds__(kStepBX* kStepBY)
+    k_tv_step(int nx, int ny, int nz, int zchunk, T hx, T hy, T hz, T thr, const T* __restrict__ x0,
+              const T* __restrict__ ycur, const T* __restrict__ yprev, const T* __restrict__ ui, T* __restrict__ uo,
+              T* __restrict__ div, double2* __restrict__ partials, TvState* st, int check_only) {
+  if (st->done) return;
+  const int kiter = st->k;
+  const bool check = kiter >= 2;
+  const long long N = (long long)nx * ny * nz;
+  const long long sz = (long long)nx * ny;
+  const int lane = threadIdx.x;
+  const int i0 = blockIdx.x * kStepBX + lane;
+  const int j0 = blockIdx.y * kStepBY + threadIdx.y;
+  const bool in = i0 < nx && j0 < ny;
+  const int i = i0 < nx ? i0 : nx - 1;  // clamped for the shuffle partners
+  const int j = j0 < ny ? j0 : ny - 1;
+  const int ip = i + 1 < nx ? i + 1 : 0, im = i > 0 ? i - 1 : nx - 1;
+  const int jp = j + 1 < ny ? j + 1 : 0, jm = j > 0 ? j - 1 : ny - 1;
+  const int k0 = blockIdx.z * zchunk;
+  const int k1 = k0 + zchunk < nz ? k0 + zchunk : nz;
+  // x-neighbours through shuffles when the partner lane holds them
+  const bool shf_p = (lane < 31) && (i + 1 < nx) && (i0 < nx);
+  const bool shf_m = (lane > 0) && (i > 0) && (i0 < nx);
+  auto X = [&](long long q) -> T { return x0[q] - ycur[q]; };
+  const long long rowj = (long long)j * nx;
+  const int kmm = k0 > 0 ? k0 - 1 : nz - 1;
+  T x_km = X(kmm * sz + rowj + i);
+  T uz_km = check_only ? T(0) : ui[2 * N + kmm * sz + rowj + i];
+  T x_k = X(k0 * sz + rowj + i);
+  double sd = 0.0, sx = 0.0;
+  for (int k = k0; k < k1; ++k) {
+    const int kp = k + 1 < nz ? k + 1 : 0;
+    const long long base = k * sz;
+    const long long c = base + rowj + i;
+    const T x_kp = X(kp * sz + rowj + i);
+    if (check && in) {
+      const T xp = x0[c] - yprev[c];
+      const double dd = (double)x_k - (double)xp;
+      sd += dd * dd;
+      sx += (double)x_k * (double)x_k;
+    }
+    if (!check_only) {
+      const T ux = ui[c], uy = ui[N + c], uz = ui[2 * N + c];
+      T xip = __shfl_down_sync(0xffffffffu, x_k, 1);
+      T xim = __shfl_up_sync(0xffffffffu, x_k, 1);
+      T uxm = __shfl_up_sync(0xffffffffu, ux, 1);
+      if (!shf_p) xip = X(base + rowj + ip);
+      if (!shf_m) {
+        xim = X(base + rowj + im);
+        uxm = ui[base + rowj + im];
+      }
+      const T xjp = X(base + (long long)jp * nx + i);
+      const long long cjm = base + (long long)jm * nx + i;
+      const T xjm = X(cjm);
+      const T uym = ui[N + cjm];
+      const T vx = (xip - x_k) * hx + ux;
+      const T vy = (xjp - x_k) * hy + uy;
+      const T vz = (x_kp - x_k) * hz + uz;
+      const T zx = shrink(vx, thr), zy = shrink(vy, thr), zz = shrink(vz, thr);
+      const T gx = T(2) * zx - vx, gy = T(2) * zy - vy, gz = T(2) * zz - vz;
+      const T vxm = (x_k - xim) * hx + uxm;
+      const T vym = (x_k - xjm) * hy + uym;
+      const T vzm = (x_k - x_km) * hz + uz_km;
+      const T gxm = T(2) * shrink(vxm, thr) - vxm;
+      const T gym = T(2) * shrink(vym, thr) - vym;
+      const T gzm = T(2) * shrink(vzm, thr) - vzm;
+      if (in) {
+        uo[c] = vx - zx;
+        uo[N + c] = vy - zy;
+        uo[2 * N + c] = vz - zz;
+        div[c] = (gx - gxm) * hx + (gy - gym) * hy + (gz - gzm) * hz;
+      }
+      uz_km = uz;
+    }
+    x_km = x_k;
+    x_k = x_kp;
+  }
+  // deterministic two-level reduction: per-block partials, summed in a fixed order
+  // by the block that arrives last
+  __shared__ int am_last;
+  double a = sd, b = sx;
+  block_sum2(a, b);
+  const int tid = threadIdx.x + kStepBX * threadIdx.y;
+  const int nblocks = gridDim.x * gridDim.y * gridDim.z;
+  const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+  if (tid == 0) {
+    partials[bid] = make_double2(a, b);
+    __threadfence();
+    const unsigned prev = atomicAdd(&st->counter, 1u);
+    am_last = (prev == (unsigned)nblocks - 1);
+  }
+  __syncthreads();
+  if (am_last) {
+    __threadfence();
+    double pa = 0.0, pb = 0.0;
+    for (int i = tid; i < nblocks; i += kStepBX * kStepBY) {
+      const double2 p = __ldcg(&partials[i]);
+      pa += p.x;
+      pb += p.y;
+    }
+    block_sum2(pa, pb);
+    if (tid == 0) {
+      if (check) {
+        const double rc = sqrt(pa) / (sqrt(pb) + 1e-20);  // src/utils/mod.rs:69-77
+        st->rc = rc;
+        if (rc < st->tol) {
+          st->done = 1;
+          st->conv_iter = kiter - 1;
+        }
+      }
+      st->k = kiter + 1;
+      st->counter = 0u;
+    }
+  }
+}
+
+// 16-byte vectors: 4 floats or 2 doubles per thread along x.
+template <typename T> struct Vec16;
+template <> struct Vec16<float> {
+  static constexpr int n = 4;
+  struct V { float v[4]; };
+  static __device__ __forceinline__ V ld(const float* p) {
+    const float4 a = __ldg(reinterpret_cast<const float4*>(p));
+    return V{{a.x, a.y, a.z, a.w}};
+  }
+  static __device__ __forceinline__ void st(float* p, const V& a) {
+    *reinterpret_cast<float4*>(p) = make_float4(a.v[0], a.v[1], a.v[2], a.v[3]);
+  }
+};
+template <> struct Vec16<double> {
+  static constexpr int n = 2;
+  struct V { double v[2]; };
+  static __device__ __forceinline__ V ld(const double* p) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+    return V{{a.x, a.y}};
+  }
+  static __device__ __forceinline__ void st(double* p, const V& a) {
+    *reinterpret_cast<double2*>(p) = make_double2(a.v[0], a.v[1]);
+  }
+};
+
+// k_tv_step with 16-byte vector loads and stores: each thread owns Vec16<T>::n
+// consecutive x (nx a multiple of that), x-neighbours across vectors come from the
+// adjacent lanes.  Same arithmetic per voxel as k_tv_step.
+template <typename T>
+__global__ void __launch_bounds__(kStepBX* kStepBY)
+    k_tv_step_v(int nx, int ny, int nz, int zchunk, T hx, T hy, T hz, T thr, const T* __restrict__ x0,
+                const T* __restrict__ ycur, const T* __restrict__ yprev, const T* __restrict__ ui,
+                T* __restrict__ uo, T* __restrict__ div, double2* __restrict__ partials, TvState* st,
+                int check_only) {
+  using W = Vec16<T>;
+  using V = typename W::V;
+  constexpr int NV = W::n;
+  if (st->done) return;
+  const int kiter = st->k;
+  const bool check = kiter >= 2;
+  const long long N = (long long)nx * ny * nz;
+  const long long sz = (long long)nx * ny;
+  const int lane = threadIdx.x;
+  const int nxv = nx / NV;
+  const int v0 = blockIdx.x * kStepBX + lane;
+  const int j0 = blockIdx.y * kStepBY + threadIdx.y;
+  const bool in = v0 < nxv && j0 < ny;
+  const int i = (v0 < nxv ? v0 : nxv - 1) * NV;  // first x of this thread (clamped for the shuffles)
+  const int j = j0 < ny ? j0 : ny - 1;
+  const int ip = i + NV < nx ? i + NV : 0, im = i > 0 ? i - 1 : nx - 1;
+  const int jp = j + 1 < ny ? j + 1 : 0, jm = j > 0 ? j - 1 : ny - 1;
+  const int k0 = blockIdx.z * zchunk;
+  const int k1 = k0 + zchunk < nz ? k0 + zchunk : nz;
+  const bool shf_p = (lane < 31) && (v0 + 1 < nxv);
+  const bool shf_m = (lane > 0) && (v0 > 0) && (v0 < nxv);
+  auto X = [&](long long q) -> V {
+    const V a = W::ld(x0 + q), b = W::ld(ycur + q);
+    V r;
+#pragma unroll
+    for (int e = 0; e < NV; ++e) r.v[e] = a.v[e] - b.v[e];
+    return r;
+  };
+  auto Xs = [&](long long q) -> T { return x0[q] - ycur[q]; };
+  const long long rowj = (long long)j * nx;
+  const int kmm = k0 > 0 ? k0 - 1 : nz - 1;
+  V x_km = X(kmm * sz + rowj + i);
+  V uz_km{};
+  if (!check_only) uz_km = W::ld(ui + 2 * N + kmm * sz + rowj + i);
+  V x_k = X(k0 * sz + rowj + i);
+  double sd = 0.0, sx = 0.0;
+  for (int k = k0; k < k1; ++k) {
+    const int kp = k + 1 < nz ? k + 1 : 0;
+    const long long base = k * sz;
+    const long long c = base + rowj + i;
+    const V x_kp = X(kp * sz + rowj + i);
+    if (check && in) {
+      const V a = W::ld(x0 + c), b = W::ld(yprev + c);
+#pragma unroll
+      for (int e = 0; e < NV; ++e) {
+        const double dd = (double)x_k.v[e] - (double)(a.v[e] - b.v[e]);
+        sd += dd * dd;
+        sx += (double)x_k.v[e] * (double)x_k.v[e];
+      }
+    }
+    if (!check_only) {
+      const V ux = W::ld(ui + c), uy = W::ld(ui + N + c), uz = W::ld(ui + 2 * N + c);
+      T xnext = __shfl_down_sync(0xffffffffu, x_k.v[0], 1);
+      T xprev = __shfl_up_sync(0xffffffffu, x_k.v[NV - 1], 1);
+      T uxprev = __shfl_up_sync(0xffffffffu, ux.v[NV - 1], 1);
+      if (!shf_p) xnext = Xs(base + rowj + ip);
+      if (!shf_m) {
+        xprev = Xs(base + rowj + im);
+        uxprev = ui[base + rowj + im];
+      }
+      const V xjp = X(base + (long long)jp * nx + i);
+      const long long cjm = base + (long long)jm * nx + i;
+      const V xjm = X(cjm);
+      const V uym = W::ld(ui + N + cjm);
+      V ox, oy, oz, dv;
+#pragma unroll
+      for (int e = 0; e < NV; ++e) {
+        const T xe = x_k.v[e];
+        const T xip = e + 1 < NV ? x_k.v[e + 1] : xnext;
+        const T xim = e > 0 ? x_k.v[e - 1] : xprev;
+        const T uxm = e > 0 ? ux.v[e - 1] : uxprev;
+        const T vx = (xip - xe) * hx + ux.v[e];
+        const T vy = (xjp.v[e] - xe) * hy + uy.v[e];
+        const T vz = (x_kp.v[e] - xe) * hz + uz.v[e];
+        const T zx = shrink(vx, thr), zy = shrink(vy, thr), zz = shrink(vz, thr);
+        const T gx = T(2) * zx - vx, gy = T(2) * zy - vy, gz = T(2) * zz - vz;
+        const T vxm = (xe - xim) * hx + uxm;
+        const T vym = (xe - xjm.v[e]) * hy + uym.v[e];
+        const T vzm = (xe - x_km.v[e]) * hz + uz_km.v[e];
+        const T gxm = T(2) * shrink(vxm, thr) - vxm;
+        const T gym = T(2) * shrink(vym, thr) - vym;
+        const T gzm = T(2) * shrink(vzm, thr) - vzm;
+        ox.v[e] = vx - zx;
+        oy.v[e] = vy - zy;
+        oz.v[e] = vz - zz;
+        dv.v[e] = (gx - gxm) * hx + (gy - gym) * hy + (gz - gzm) * hz;
+      }
+      if (in) {
+        W::st(uo + c, ox);
+        W::st(uo + N + c, oy);
+        W::st(uo + 2 * N + c, oz);
+        W::st(div + c, dv);
+      }
+      uz_km = uz;
+    }
+    x_km = x_k;
+    x_k = x_kp;
+  }
+  __shared__ int am_last;
+  double a = sd, b = sx;
+  block_sum2(a, b);
+  const int tid = threadIdx.x + kStepBX * threadIdx.y;
+  const int nblocks = gridDim.x * gridDim.y * gridDim.z;
+  const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+  if (tid == 0) {
+    partials[bid] = make_double2(a, b);
+    __threadfence();
+    const unsigned prev = atomicAdd(&st->counter, 1u);
+    am_last = (prev == (unsigned)nblocks - 1);
+  }
+  __syncthreads();
+  if (am_last) {
+    __threadfence();
+    double pa = 0.0, pb = 0.0;
+    for (int q = tid; q < nblocks; q += kStepBX * kStepBY) {
+      const double2 p = __ldcg(&partials[q]);
+      pa += p.x;
+      pb += p.y;
+    }
+    block_sum2(pa, pb);
+    if (tid == 0) {
+      if (check) {
+        const double rc = sqrt(pa) / (sqrt(pb) + 1e-20);  // src/utils/mod.rs:69-77
+        st->rc = rc;
+        if (rc < st->tol) {
+          st->done = 1;
+          st->conv_iter = kiter - 1;
+        }
+      }
+      st->k = kiter + 1;
+      st->counter = 0u;
+    }
+  }
+}
+
+template <typename T>
+__global__ void k_tv_out(long long N, const T* __restrict__ x0, const T* __restrict__ y,
+                         const uint8_t* __restrict__ mask, double* __restrict__ out) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
+    out[i] = mask[i] != 0 ? (double)(x0[i] - y[i]) : 0.0;  // apply_mask_zero, src/utils/mask.rs:47-53
+}
+
+// Device buffers, launch shapes and constants of one TV-ADMM volume.
+template <typename T> struct TvVol {
+  GridDims d;
+  Fft3<T> f;
+  OpAdmmMul<T> mul;
+  T* x0;
+  T* yb[2];
+  T* ub[2];
+  T* div;
+  T* mult;
+  cplx_t<T>* spec;
+  double2* partials;
+  TvState* st;
+  dim3 sgrid;
+  int zchunk;
+  bool vec, use_mult;
+  T hx, hy, hz, thr, scale;
+  const uint8_t* mask;
+  double* out;
+};
+
+// Allocate one volume's buffers (workspace names prefixed by `pre`) and enqueue, on
+// ctx->stream, x0 = Re IFFT(F(f) * sym(D * inv_a)), y_0 = x0 (x_0 = 0), u = 0, the
+// per-iteration multiplier and the initial state (st is this volume's device state).
+template <typename T>
+void tv_setup(qsm_ctx* ctx, TvVol<T>& v, const std::string& pre, const GridDims& d, const double* d_f,
+              const uint8_t* d_mask, const double bdir[3], const qsm_tv_params& p, TvState* st, double* d_out) {
+  using C = cplx_t<T>;
+  v.d = d;
+  v.f = make_fft3<T>(ctx, d);
+  const KSpace K64 = make_kspace(ctx, d, bdir);
+  v.mul = OpAdmmMul<T>{make_kspace_t<T>(ctx, d, bdir), (T)p.rho};
+  const long long N = d.n;
+  const long long H = v.f.g.hsize();
+  auto nm = [&](const char* s) { return pre + s; };
+  v.x0 = ws<T>(ctx, nm("x0"), (size_t)N);
+  v.yb[0] = ws<T>(ctx, nm("y0"), (size_t)N);
+  v.yb[1] = ws<T>(ctx, nm("y1"), (size_t)N);
+  v.ub[0] = ws<T>(ctx, nm("u0"), (size_t)(3 * N));
+  v.ub[1] = ws<T>(ctx, nm("u1"), (size_t)(3 * N));
+  v.div = ws<T>(ctx, nm("div"), (size_t)N);
+  v.spec = ws<C>(ctx, nm("spec"), (size_t)H);
+  // stencil grid: 32x8 threads per block (each thread one x, or one 16-byte vector of
+  // x in single precision when nx allows), z split into chunks so that ~3000 blocks run
+  v.vec = sizeof(T) == 4 && d.nx % Vec16<T>::n == 0;
+  const int xper = v.vec ? Vec16<T>::n : 1;
+  const int gbx = (d.nx / xper + kStepBX - 1) / kStepBX, gby = (d.ny + kStepBY - 1) / kStepBY;
+  int zchunk = (int)std::max<long long>(2, (long long)d.nz * gbx * gby / 3000);
+  if (zchunk > d.nz) zchunk = d.nz;
+  v.zchunk = zchunk;
+  v.sgrid = dim3(gbx, gby, (d.nz + zchunk - 1) / zchunk);
+  v.partials = ws<double2>(ctx, nm("partials"), (size_t)v.sgrid.x * v.sgrid.y * v.sgrid.z);
+  v.st = st;
+  v.scale = (T)(1.0 / (double)N);
+  v.hx = (T)(1.0 / d.vsx);
+  v.hy = (T)(1.0 / d.vsy);
+  v.hz = (T)(1.0 / d.vsz);
+  v.thr = (T)(p.lambda / p.rho);
+  v.mask = d_mask;
+  v.out = d_out;
+  run_x_r2c<T>(ctx, v.f, v.spec, LoadCast<double, T>{d_f, d.nx}, nullptr);
+  run_yz<T, -1, 1>(ctx, v.f, v.spec, v.spec, OpId<T>{}, nullptr);
+  run_z_fused<T>(ctx, v.f, v.spec, v.spec, OpAdmmRhs<T>{K64, p.rho}, nullptr);
+  run_yz<T, +1, 1>(ctx, v.f, v.spec, v.spec, OpId<T>{}, nullptr);
+  run_x_c2r<T>(ctx, v.f, v.spec, StoreReal<T>{v.x0, d.nx, v.scale}, nullptr);
+  QSM_CUDA(cudaMemcpyAsync(v.yb[0], v.x0, sizeof(T) * N, cudaMemcpyDeviceToDevice, ctx->stream));
+  QSM_CUDA(cudaMemsetAsync(v.ub[0], 0, sizeof(T) * 3 * N, ctx->stream));
+  TvState init{};
+  init.k = 1;
+  init.tol = p.tol;
+  QSM_CUDA(cudaMemcpyAsync(st, &init, sizeof(TvState), cudaMemcpyHostToDevice, ctx->stream));
+  // precomputed multiplier tiles need P*sizeof(T) >= 16 (always true for the
+  // 128-byte tiles; narrow tiles of very long z axes use the in-kernel multiplier)
+  v.mult = ws<T>(ctx, nm("mult"), (size_t)H);
+  {
+    LaunchScope ls(ctx, "admm_mult");
+    k_admm_mult<T><<<grid1d(H), 256, 0, ctx->stream>>>(v.f.g, K64, p.rho, v.mult);
+    ls.done();
+  }
+  v.use_mult = zm_tile_width<T>(d.nz, v.f.pz.T) > 0;
+}
+
+// iteration i with parity q = i % 2: reads y_{i-1} = yb[1-q], y_{i-2} = yb[q],
+// u = ub[1-q]; writes u' = ub[q], y_i = yb[q]
+template <typename T> void tv_step_launch(qsm_ctx* ctx, const TvVol<T>& v, int q, int check_only) {
+  LaunchScope ls(ctx, "tv_step");
+  auto kern = v.vec ? k_tv_step_v<T> : k_tv_step<T>;
+  kern<<<v.sgrid, dim3(kStepBX, kStepBY), 0, ctx->stream>>>(v.d.nx, v.d.ny, v.d.nz, v.zchunk, v.hx, v.hy, v.hz,
+                                                              v.thr, v.x0, v.yb[1 - q], v.yb[q], v.ub[1 - q],
+                                                              v.ub[q], v.div, v.partials, v.st, check_only);
+  ls.done();
+}
+
+template <typename T> void tv_iter(qsm_ctx* ctx, const TvVol<T>& v, int q) {
+  const int* done = &v.st->done;
+  tv_step_launch(ctx, v, q, 0);
+  run_x_r2c<T>(ctx, v.f, v.spec, LoadCast<T, T>{v.div, v.d.nx}, done);
+  run_yz<T, -1, 1>(ctx, v.f, v.spec, v.spec, OpId<T>{}, done);
+  if (v.use_mult) run_z_fused_m<T>(ctx, v.f, v.spec, v.spec, v.mult, done);
+  else run_z_fused<T>(ctx, v.f, v.spec, v.spec, v.mul, done);
+  run_yz<T, +1, 1>(ctx, v.f, v.spec, v.spec, OpId<T>{}, done);
+  run_x_c2r<T>(ctx, v.f, v.spec, StoreReal<T>{v.yb[q], v.d.nx, v.scale}, done);
+}
+
+template <typename T> void tv_out_launch(qsm_ctx* ctx, const TvVol<T>& v, size_t completed) {
+  LaunchScope ls(ctx, "tv_out");
+  k_tv_out<T><<<grid1d(v.d.n), 256, 0, ctx->stream>>>(v.d.n, v.x0, v.yb[completed % 2], v.mask, v.out);
+  ls.done();
+}
+
+// Instantiate a captured graph; the launch count it holds is returned in *per.
+inline cudaGraphExec_t instantiate(qsm_ctx* ctx, cudaGraph_t graph) {
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ie != cudaSuccess) throw QsmError(QSM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+  return exec;
+}
+
+}  // namespace qsm

@@ -110,6 +110,9 @@ _SIGS = [
     ("qsm_grid_supported", C.c_int, [C.POINTER(QsmGrid)]),
     ("qsm_tv_params_default", None, [C.POINTER(QsmTvParams)]),
     ("qsm_ilsqr_params_default", None, [C.POINTER(QsmIlsqrParams)]),
+    ("qsm_tv_admm_unrolled_vjp_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(QsmGrid), c_double_p,
+                                                  C.c_double, C.c_double, C.c_size_t, C.c_size_t, C.c_void_p,
+                                                  C.c_void_p, C.c_void_p, c_double_p]),
     ("qsm_dipole_forward_device", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(QsmGrid), c_double_p, C.c_void_p]),
     ("qsm_tv_admm_batch", C.c_int, [C.c_void_p, C.POINTER(QsmVolume), C.c_size_t, C.POINTER(QsmTvParams),
                                     PROGRESS_FN, C.c_void_p, C.POINTER(C.c_size_t)]),

@@ -316,3 +316,19 @@ def tkd_batch_device(ctx: Context, cases, params: TkdParams):
         arr[b].bdir = (C.c_double * 3)(*bdir)
     p = params._c()
     _check(ctx, ctx._lib.qsm_tkd_batch_device(ctx.handle, arr, len(cases), C.byref(p)))
+
+
+def tv_admm_unrolled_vjp_device(ctx: Context, d_local_field: int, d_mask: int, grid: Grid, bdir, lam: float,
+                                rho: float, iterations: int, checkpoint_every: int, d_grad_chi: int, d_out_chi: int,
+                                d_out_grad_field: int = 0):
+    """Unrolled TV-ADMM forward (chi into d_out_chi) and, when d_grad_chi is non-zero, its
+    vector-Jacobian product: dL/dfield into d_out_grad_field; returns dL/dlambda."""
+    b, _keep = _bdir(bdir)
+    g = grid._c()
+    gl = C.c_double(0.0)
+    _check(ctx, ctx._lib.qsm_tv_admm_unrolled_vjp_device(ctx.handle, C.c_void_p(d_local_field), C.c_void_p(d_mask),
+                                                         C.byref(g), b, float(lam), float(rho), int(iterations),
+                                                         int(checkpoint_every), C.c_void_p(d_grad_chi or None),
+                                                         C.c_void_p(d_out_chi), C.c_void_p(d_out_grad_field or None),
+                                                         C.byref(gl)))
+    return gl.value
