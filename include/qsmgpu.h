@@ -107,6 +107,8 @@ typedef struct {
 } qsm_tgv_params;
 /* ResharpParams — src/bgremove/resharp.rs:22-45 (radius 6 mm, tik_reg 1e-4, tol 1e-6, 30). */
 typedef struct { double radius, tik_reg, tol; size_t max_iter; } qsm_resharp_params;
+/* RtsParams — src/inversion/rts.rs:22-51 (delta 0.15, mu 1e5, rho 10, tol 1e-2, 20, 4). */
+typedef struct { double delta, mu, rho, tol; size_t max_iter, lsmr_iter; } qsm_rts_params;
 /* IlsqrParams — src/inversion/ilsqr.rs:20-34 (tol 0.01, max_iter 50: the LSMR step's
  * tolerance and iteration cap). */
 typedef struct { double tol; size_t max_iter; } qsm_ilsqr_params;
@@ -117,6 +119,7 @@ QSM_API void qsm_tikhonov_params_default(qsm_tikhonov_params* p);
 QSM_API void qsm_sharp_params_default(qsm_sharp_params* p);
 QSM_API void qsm_vsharp_params_default(qsm_vsharp_params* p);
 QSM_API void qsm_ilsqr_params_default(qsm_ilsqr_params* p);
+QSM_API void qsm_rts_params_default(qsm_rts_params* p);
 QSM_API void qsm_resharp_params_default(qsm_resharp_params* p);
 QSM_API void qsm_tgv_params_default(qsm_tgv_params* p);
 
@@ -169,6 +172,15 @@ QSM_API qsm_status qsm_tv_admm_unrolled_vjp_device(qsm_ctx* ctx, const double* d
                                                    double rho, size_t iterations, size_t checkpoint_every,
                                                    const double* d_grad_chi, double* d_out_chi,
                                                    double* d_out_grad_field, double* out_grad_lambda);
+
+/* inversion::rts — src/inversion/rts.rs:72-211 (the pipeline's default inversion).
+ * Progress (iter, max_iter) per ADMM iteration and (iters, iters) on convergence. */
+QSM_API qsm_status qsm_rts(qsm_ctx* ctx, const double* local_field, const uint8_t* mask, const qsm_grid* grid,
+                           const double bdir[3], const qsm_rts_params* params, qsm_progress_fn progress, void* user,
+                           double* out_chi);
+QSM_API qsm_status qsm_rts_device(qsm_ctx* ctx, const double* d_local_field, const uint8_t* d_mask,
+                                  const qsm_grid* grid, const double bdir[3], const qsm_rts_params* params,
+                                  qsm_progress_fn progress, void* user, double* d_out_chi);
 
 /* inversion::tkd — src/inversion/tkd.rs:48-99. */
 QSM_API qsm_status qsm_tkd(qsm_ctx* ctx, const double* local_field, const uint8_t* mask, const qsm_grid* grid,
@@ -320,6 +332,7 @@ typedef struct {
   qsm_tikhonov_params tikhonov;
   qsm_tv_params tv;
   qsm_ilsqr_params ilsqr;
+  qsm_rts_params rts;
 } qsm_inversion_config;
 
 /* BgRemovalAlgorithm — src/pipeline/config.rs:33-42, same variant order.  Variants

@@ -330,10 +330,25 @@ class TvParams:  # src/inversion/tv.rs:23-43
     max_iter: int = 250
 
 
-def prepare_admm_spectral(local_field, grid: Grid, bdir, rho):
+def laplacian_eigenvalues(grid: Grid, exact_dc: bool = False) -> np.ndarray:
+    """Re FFT(laplacian_kernel(negative=True)) as src/inversion/admm.rs:159-163 and
+    src/inversion/rts.rs:93-99 compute it.  The DC bin is the floating-point sum of the
+    seven taps: exactly 0 for some voxel sizes and a few ulp (e.g. 4.4e-16 at
+    (1, 1, 0.9)) for others, depending on the FFT's summation order.  A nonzero value
+    there defeats the |a| > 1e-20 guard of the ADMM inverse, so inv_a(0) becomes ~1e17
+    and the iterate picks up a constant offset made of amplified roundoff.
+    exact_dc=True stores the exact eigenvalue 0 there, which makes the guard fire as
+    intended; the GPU tables hold that value."""
+    lap = fft3d(laplacian_kernel(grid, True).astype(np.complex128)).real
+    if exact_dc:
+        lap[0, 0, 0] = 0.0
+    return lap
+
+
+def prepare_admm_spectral(local_field, grid: Grid, bdir, rho, exact_dc: bool = False):
     """(inv_a, f_hat) (src/inversion/admm.rs:150-178)."""
     d = dipole_kernel(grid, bdir)
-    lap = fft3d(laplacian_kernel(grid, True).astype(np.complex128)).real
+    lap = laplacian_eigenvalues(grid, exact_dc)
     a = d * d + rho * lap
     with np.errstate(divide="ignore"):
         inv_a = np.where(np.abs(a) > 1e-20, 1.0 / a, 0.0)
@@ -342,15 +357,15 @@ def prepare_admm_spectral(local_field, grid: Grid, bdir, rho):
 
 
 def tv_admm(local_field, mask, grid: Grid, bdir, params: TvParams = TvParams(),
-            progress: Optional[Callable[[int, int], None]] = None, return_iters=False):
+            progress: Optional[Callable[[int, int], None]] = None, return_iters=False, exact_dc=False):
     """TV-ADMM dipole inversion (src/inversion/tv.rs:63-97, src/inversion/admm.rs:76-145).
 
     State starts at x = u = g = 0.  Each iteration: div = bdiv(g); x = Re IFFT(f_hat -
     rho*FFT(div)*inv_a); stop if relative_change(x, x_prev) < tol (checked before the
     z/u update, admm.rs:117); then v = grad x + u, z = shrink(v, lambda/rho), u = v - z,
-    g = 2z - v.
+    g = 2z - v.  exact_dc: see laplacian_eigenvalues.
     """
-    inv_a, f_hat = prepare_admm_spectral(local_field, grid, bdir, params.rho)
+    inv_a, f_hat = prepare_admm_spectral(local_field, grid, bdir, params.rho, exact_dc)
     shape = grid.shape
     x = np.zeros(shape)
     ux = np.zeros(shape); uy = np.zeros(shape); uz = np.zeros(shape)
@@ -1381,3 +1396,62 @@ def apply_reference(chi, mask, method="mean"):
     m = np.asarray(mask) > 0
     mu = float(x[m].sum()) / int(m.sum()) if (method == "mean" and m.any()) else 0.0
     return np.where(m, x - mu, 0.0)
+
+
+# ---------------------------------------------------------------------------
+# RTS (src/inversion/rts.rs)
+# ---------------------------------------------------------------------------
+@dataclass
+class RtsParams:  # src/inversion/rts.rs:22-51
+    delta: float = 0.15
+    mu: float = 1e5
+    rho: float = 10.0
+    tol: float = 1e-2
+    max_iter: int = 20
+    lsmr_iter: int = 4
+
+
+def rts(local_field, mask, grid: Grid, bdir, params: RtsParams = RtsParams(), progress=None, return_iters=False,
+        exact_dc=False):
+    """src/inversion/rts.rs:72-211: k-space refinement in the well-conditioned region, then
+    ADMM (admm.rs:76-145) with inv_a = rho/(M + rho L), unit divergence factor, shrink
+    threshold 1/rho, first convergence test against the step-1 estimate.  exact_dc: see
+    laplacian_eigenvalues."""
+    d = dipole_kernel(grid, bdir)
+    lap = laplacian_eigenvalues(grid, exact_dc)
+    well = np.abs(d) > params.delta
+    m_mask = np.where(well, params.mu, 0.0)
+    a = m_mask + params.rho * lap
+    with np.errstate(divide="ignore"):
+        inv_a = np.where(np.abs(a) > 1e-20, params.rho / a, 0.0)
+    F = fft3d(_vol(local_field, grid).astype(np.complex128))
+    chi = np.where(well, F * d / (d * d + 1e-6), 0.0)
+    for _ in range(params.lsmr_iter):
+        res = F - chi * d
+        chi = np.where(well, chi + res * d / (d * d + 1e-6), chi)
+    m = _vol(mask, grid, np.uint8)
+    x = np.where(m != 0, ifft3d(chi).real, 0.0)
+    X = fft3d(x.astype(np.complex128))
+    f_hat = np.where((np.abs(m_mask) > 1e-20) & (np.abs(inv_a) > 1e-20), X * (m_mask / params.rho) * inv_a, 0.0)
+    z = np.zeros(grid.shape)
+    ux, uy, uz, gx, gy, gz = z.copy(), z.copy(), z.copy(), z.copy(), z.copy(), z.copy()
+    t = 1.0 / params.rho
+    iters = 0
+    for it in range(params.max_iter):
+        if progress is not None:
+            progress(it + 1, params.max_iter)
+        x_prev = x
+        div = bdiv(gx, gy, gz, grid)
+        x = ifft3d(f_hat - 1.0 * fft3d(div.astype(np.complex128)) * inv_a).real
+        iters = it + 1
+        if relative_change(x, x_prev) < params.tol:
+            if progress is not None:
+                progress(it + 1, it + 1)
+            break
+        ggx, ggy, ggz = fgrad(x, grid)
+        vx, vy, vz = ggx + ux, ggy + uy, ggz + uz
+        zx, zy, zz = shrink(vx, t), shrink(vy, t), shrink(vz, t)
+        ux, uy, uz = vx - zx, vy - zy, vz - zz
+        gx, gy, gz = 2.0 * zx - vx, 2.0 * zy - vy, 2.0 * zz - vz
+    out = apply_mask_zero(x, m)
+    return (out, iters) if return_iters else out

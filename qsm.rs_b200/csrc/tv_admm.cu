@@ -29,77 +29,7 @@ void tv_admm_impl(qsm_ctx* ctx, const GridDims& d, const double* d_f, const uint
   TvVol<T> v;
   tv_setup<T>(ctx, v, pre, d, d_f, d_mask, bdir, p, st, d_out);
 
-  const size_t max_iter = p.max_iter;
-  const bool watch = (progress != nullptr) || (p.tol > 0.0);
-  TvState hs{};
-  size_t reported = 0;
-  auto poll = [&]() {
-    QSM_CUDA(cudaMemcpyAsync(&hs, st, sizeof(TvState), cudaMemcpyDeviceToHost, ctx->stream));
-    sync(ctx);
-    const size_t completed = hs.done ? (size_t)hs.conv_iter : (size_t)(hs.k - 1);
-    if (progress)
-      for (; reported < completed; ++reported) progress(user, reported + 1, max_iter);
-    return hs.done != 0;
-  };
-
-  bool converged = false;
-  if (ctx->profiling || max_iter < 2) {
-    // eager launches (per-kernel timing, or too short to be worth a graph)
-    for (size_t it = 1; it <= max_iter && !converged; ++it) {
-      tv_iter(ctx, v, (int)(it % 2));
-      if (watch && (it % 16 == 0)) converged = poll();
-    }
-  } else {
-    cudaGraph_t graph = nullptr;
-    const uint64_t l0 = ctx->launches;
-    QSM_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    try {
-      tv_iter(ctx, v, 1);
-      tv_iter(ctx, v, 0);
-    } catch (...) {
-      cudaStreamEndCapture(ctx->stream, &graph);
-      if (graph) cudaGraphDestroy(graph);
-      throw;
-    }
-    QSM_CUDA(cudaStreamEndCapture(ctx->stream, &graph));
-    const uint64_t per_pair = ctx->launches - l0;
-    ctx->launches = l0;
-    cudaGraphExec_t exec = instantiate(ctx, graph);
-    const size_t pairs = max_iter / 2;
-    const size_t chunk = 8;  // graph launches (16 iterations) between host polls when watching
-    try {
-      size_t launched = 0;
-      while (launched < pairs && !converged) {
-        const size_t todo = watch ? std::min(chunk, pairs - launched) : (pairs - launched);
-        for (size_t c = 0; c < todo; ++c) {
-          QSM_CUDA(cudaGraphLaunch(exec, ctx->stream));
-          ctx->launches += per_pair;
-        }
-        launched += todo;
-        if (watch) converged = poll();
-      }
-      if (!converged && (max_iter % 2 == 1)) tv_iter(ctx, v, 1);
-    } catch (...) {
-      cudaGraphExecDestroy(exec);
-      throw;
-    }
-    cudaGraphExecDestroy(exec);
-  }
-  converged = poll();
-  size_t completed = converged ? (size_t)hs.conv_iter : max_iter;
-  if (!converged && max_iter >= 1 && p.tol > 0.0) {
-    // the reference also tests the last iterate (tv.rs:85-91)
-    tv_step_launch(ctx, v, (int)((max_iter + 1) % 2), 1);
-    converged = poll();
-    completed = max_iter;
-  }
-  tv_out_launch(ctx, v, completed);
-  sync(ctx);
-  if (progress) {
-    for (; reported < completed; ++reported) progress(user, reported + 1, max_iter);
-    if (converged) progress(user, completed, completed);
-  }
-  ctx->tv_last_iters = completed;
+  ctx->tv_last_iters = tv_run<T>(ctx, v, p.max_iter, p.tol, progress, user);
 }
 
 // Batched TV-ADMM: every volume keeps its own buffers, grid, field direction and

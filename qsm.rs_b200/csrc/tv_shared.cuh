@@ -165,10 +165,13 @@ __global__ void __launch_bounds__(kStepBX* kStepBY)
       const T gym = T(2) * shrink(vym, thr) - vym;
       const T gzm = T(2) * shrink(vzm, thr) - vzm;
       if (in) {
-        uo[c] = vx - zx;
-        uo[N + c] = vy - zy;
-        uo[2 * N + c] = vz - zz;
-        div[c] = (gx - gxm) * hx + (gy - gym) * hy + (gz - gzm) * hz;
+        // the first update sees x_0 = u = g = 0 (admm.rs:18-53): zeros, whatever x_0's
+        // buffer holds (RTS keeps its starting iterate there for the first test)
+        const bool z0 = kiter == 1;
+        uo[c] = z0 ? T(0) : vx - zx;
+        uo[N + c] = z0 ? T(0) : vy - zy;
+        uo[2 * N + c] = z0 ? T(0) : vz - zz;
+        div[c] = z0 ? T(0) : (gx - gxm) * hx + (gy - gym) * hy + (gz - gzm) * hz;
       }
       uz_km = uz;
     }
@@ -336,6 +339,12 @@ __global__ void __launch_bounds__(kStepBX* kStepBY)
         dv.v[e] = (gx - gxm) * hx + (gy - gym) * hy + (gz - gzm) * hz;
       }
       if (in) {
+        if (kiter == 1) {  // first update: x_0 = u = g = 0 (see k_tv_step)
+          ox = V{};
+          oy = V{};
+          oz = V{};
+          dv = V{};
+        }
         W::st(uo + c, ox);
         W::st(uo + N + c, oy);
         W::st(uo + 2 * N + c, oz);
@@ -411,17 +420,15 @@ template <typename T> struct TvVol {
   double* out;
 };
 
-// Allocate one volume's buffers (workspace names prefixed by `pre`) and enqueue, on
-// ctx->stream, x0 = Re IFFT(F(f) * sym(D * inv_a)), y_0 = x0 (x_0 = 0), u = 0, the
-// per-iteration multiplier and the initial state (st is this volume's device state).
+// Allocate one volume's buffers (workspace names prefixed by `pre`), launch shapes and
+// constants; `thr` is the shrink threshold.  Nothing is enqueued.
 template <typename T>
-void tv_setup(qsm_ctx* ctx, TvVol<T>& v, const std::string& pre, const GridDims& d, const double* d_f,
-              const uint8_t* d_mask, const double bdir[3], const qsm_tv_params& p, TvState* st, double* d_out) {
+void tv_alloc(qsm_ctx* ctx, TvVol<T>& v, const std::string& pre, const GridDims& d, const double bdir[3],
+              double rho_mul, double thr, TvState* st, const uint8_t* d_mask, double* d_out) {
   using C = cplx_t<T>;
   v.d = d;
   v.f = make_fft3<T>(ctx, d);
-  const KSpace K64 = make_kspace(ctx, d, bdir);
-  v.mul = OpAdmmMul<T>{make_kspace_t<T>(ctx, d, bdir), (T)p.rho};
+  v.mul = OpAdmmMul<T>{make_kspace_t<T>(ctx, d, bdir), (T)rho_mul};
   const long long N = d.n;
   const long long H = v.f.g.hsize();
   auto nm = [&](const char* s) { return pre + s; };
@@ -447,29 +454,43 @@ void tv_setup(qsm_ctx* ctx, TvVol<T>& v, const std::string& pre, const GridDims&
   v.hx = (T)(1.0 / d.vsx);
   v.hy = (T)(1.0 / d.vsy);
   v.hz = (T)(1.0 / d.vsz);
-  v.thr = (T)(p.lambda / p.rho);
+  v.thr = (T)thr;
   v.mask = d_mask;
   v.out = d_out;
+  v.mult = ws<T>(ctx, pre + "mult", (size_t)v.f.g.hsize());
+  v.use_mult = zm_tile_width<T>(d.nz, v.f.pz.T) > 0;
+}
+
+// Initial state on ctx->stream: y_0 = x0 (x_0 = 0), u = 0, iteration counter 1.
+template <typename T> void tv_init_state(qsm_ctx* ctx, const TvVol<T>& v, double tol) {
+  const long long N = v.d.n;
+  QSM_CUDA(cudaMemcpyAsync(v.yb[0], v.x0, sizeof(T) * N, cudaMemcpyDeviceToDevice, ctx->stream));
+  QSM_CUDA(cudaMemsetAsync(v.ub[0], 0, sizeof(T) * 3 * N, ctx->stream));
+  TvState init{};
+  init.k = 1;
+  init.tol = tol;
+  QSM_CUDA(cudaMemcpyAsync(v.st, &init, sizeof(TvState), cudaMemcpyHostToDevice, ctx->stream));
+}
+
+// TV-ADMM setup: buffers, x0 = Re IFFT(F(f) * sym(D * inv_a)), the per-iteration
+// multiplier rho * sym(inv_a) and the initial state (st is this volume's device state).
+template <typename T>
+void tv_setup(qsm_ctx* ctx, TvVol<T>& v, const std::string& pre, const GridDims& d, const double* d_f,
+              const uint8_t* d_mask, const double bdir[3], const qsm_tv_params& p, TvState* st, double* d_out) {
+  tv_alloc<T>(ctx, v, pre, d, bdir, p.rho, p.lambda / p.rho, st, d_mask, d_out);
+  const KSpace K64 = make_kspace(ctx, d, bdir);
+  const long long H = v.f.g.hsize();
   run_x_r2c<T>(ctx, v.f, v.spec, LoadCast<double, T>{d_f, d.nx}, nullptr);
   run_yz<T, -1, 1>(ctx, v.f, v.spec, v.spec, OpId<T>{}, nullptr);
   run_z_fused<T>(ctx, v.f, v.spec, v.spec, OpAdmmRhs<T>{K64, p.rho}, nullptr);
   run_yz<T, +1, 1>(ctx, v.f, v.spec, v.spec, OpId<T>{}, nullptr);
   run_x_c2r<T>(ctx, v.f, v.spec, StoreReal<T>{v.x0, d.nx, v.scale}, nullptr);
-  QSM_CUDA(cudaMemcpyAsync(v.yb[0], v.x0, sizeof(T) * N, cudaMemcpyDeviceToDevice, ctx->stream));
-  QSM_CUDA(cudaMemsetAsync(v.ub[0], 0, sizeof(T) * 3 * N, ctx->stream));
-  TvState init{};
-  init.k = 1;
-  init.tol = p.tol;
-  QSM_CUDA(cudaMemcpyAsync(st, &init, sizeof(TvState), cudaMemcpyHostToDevice, ctx->stream));
+  tv_init_state<T>(ctx, v, p.tol);
   // precomputed multiplier tiles need P*sizeof(T) >= 16 (always true for the
   // 128-byte tiles; narrow tiles of very long z axes use the in-kernel multiplier)
-  v.mult = ws<T>(ctx, nm("mult"), (size_t)H);
-  {
-    LaunchScope ls(ctx, "admm_mult");
-    k_admm_mult<T><<<grid1d(H), 256, 0, ctx->stream>>>(v.f.g, K64, p.rho, v.mult);
-    ls.done();
-  }
-  v.use_mult = zm_tile_width<T>(d.nz, v.f.pz.T) > 0;
+  LaunchScope ls(ctx, "admm_mult");
+  k_admm_mult<T><<<grid1d(H), 256, 0, ctx->stream>>>(v.f.g, K64, p.rho, v.mult);
+  ls.done();
 }
 
 // iteration i with parity q = i % 2: reads y_{i-1} = yb[1-q], y_{i-2} = yb[q],
@@ -507,6 +528,87 @@ inline cudaGraphExec_t instantiate(qsm_ctx* ctx, cudaGraph_t graph) {
   cudaGraphDestroy(graph);
   if (ie != cudaSuccess) throw QsmError(QSM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
   return exec;
+}
+
+
+// Iterate an initialised volume (tv_setup or an equivalent) until relative_change < tol
+// or max_iter iterations, write chi, and deliver progress as (iter, max_iter) per
+// iteration plus (iters, iters) on convergence (src/inversion/tv.rs:78-93).  Returns the
+// iterations run.
+template <typename T>
+size_t tv_run(qsm_ctx* ctx, const TvVol<T>& v, size_t max_iter, double tol, qsm_progress_fn progress, void* user) {
+  TvState* st = v.st;
+  const bool watch = (progress != nullptr) || (tol > 0.0);
+  TvState hs{};
+  size_t reported = 0;
+  auto poll = [&]() {
+    QSM_CUDA(cudaMemcpyAsync(&hs, st, sizeof(TvState), cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);
+    // the test-only step after the last iteration also advances k: clamp to max_iter
+    const size_t completed = std::min(max_iter, hs.done ? (size_t)hs.conv_iter : (size_t)(hs.k - 1));
+    if (progress)
+      for (; reported < completed; ++reported) progress(user, reported + 1, max_iter);
+    return hs.done != 0;
+  };
+
+  bool converged = false;
+  if (ctx->profiling || max_iter < 2) {
+    // eager launches (per-kernel timing, or too short to be worth a graph)
+    for (size_t it = 1; it <= max_iter && !converged; ++it) {
+      tv_iter(ctx, v, (int)(it % 2));
+      if (watch && (it % 16 == 0)) converged = poll();
+    }
+  } else {
+    cudaGraph_t graph = nullptr;
+    const uint64_t l0 = ctx->launches;
+    QSM_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      tv_iter(ctx, v, 1);
+      tv_iter(ctx, v, 0);
+    } catch (...) {
+      cudaStreamEndCapture(ctx->stream, &graph);
+      if (graph) cudaGraphDestroy(graph);
+      throw;
+    }
+    QSM_CUDA(cudaStreamEndCapture(ctx->stream, &graph));
+    const uint64_t per_pair = ctx->launches - l0;
+    ctx->launches = l0;
+    cudaGraphExec_t exec = instantiate(ctx, graph);
+    const size_t pairs = max_iter / 2;
+    const size_t chunk = 8;  // graph launches (16 iterations) between host polls when watching
+    try {
+      size_t launched = 0;
+      while (launched < pairs && !converged) {
+        const size_t todo = watch ? std::min(chunk, pairs - launched) : (pairs - launched);
+        for (size_t c = 0; c < todo; ++c) {
+          QSM_CUDA(cudaGraphLaunch(exec, ctx->stream));
+          ctx->launches += per_pair;
+        }
+        launched += todo;
+        if (watch) converged = poll();
+      }
+      if (!converged && (max_iter % 2 == 1)) tv_iter(ctx, v, 1);
+    } catch (...) {
+      cudaGraphExecDestroy(exec);
+      throw;
+    }
+    cudaGraphExecDestroy(exec);
+  }
+  converged = poll();
+  size_t completed = converged ? (size_t)hs.conv_iter : max_iter;
+  if (!converged && max_iter >= 1 && tol > 0.0) {
+    // the reference also tests the last iterate (tv.rs:85-91)
+    tv_step_launch(ctx, v, (int)((max_iter + 1) % 2), 1);
+    converged = poll();
+    completed = max_iter;
+  }
+  tv_out_launch(ctx, v, completed);
+  sync(ctx);
+  if (progress) {
+    for (; reported < completed; ++reported) progress(user, reported + 1, max_iter);
+    if (converged) progress(user, completed, completed);
+  }
+  return completed;
 }
 
 }  // namespace qsm

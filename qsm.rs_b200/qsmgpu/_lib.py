@@ -61,6 +61,11 @@ class QsmResharpParams(C.Structure):
     _fields_ = [("radius", C.c_double), ("tik_reg", C.c_double), ("tol", C.c_double), ("max_iter", C.c_size_t)]
 
 
+class QsmRtsParams(C.Structure):
+    _fields_ = [("delta", C.c_double), ("mu", C.c_double), ("rho", C.c_double), ("tol", C.c_double),
+                ("max_iter", C.c_size_t), ("lsmr_iter", C.c_size_t)]
+
+
 class QsmIlsqrParams(C.Structure):
     _fields_ = [("tol", C.c_double), ("max_iter", C.c_size_t)]
 
@@ -83,7 +88,8 @@ class QsmScanMetadata(C.Structure):
 
 class QsmInversionConfig(C.Structure):
     _fields_ = [("algorithm", C.c_int), ("tkd", QsmTkdParams), ("tsvd", QsmTkdParams),
-                ("tikhonov", QsmTikhonovParams), ("tv", QsmTvParams), ("ilsqr", QsmIlsqrParams)]
+                ("tikhonov", QsmTikhonovParams), ("tv", QsmTvParams), ("ilsqr", QsmIlsqrParams),
+                ("rts", QsmRtsParams)]
 
 
 class QsmBgRemovalConfig(C.Structure):
@@ -110,6 +116,11 @@ _SIGS = [
     ("qsm_grid_supported", C.c_int, [C.POINTER(QsmGrid)]),
     ("qsm_tv_params_default", None, [C.POINTER(QsmTvParams)]),
     ("qsm_ilsqr_params_default", None, [C.POINTER(QsmIlsqrParams)]),
+    ("qsm_rts_params_default", None, [C.POINTER(QsmRtsParams)]),
+    ("qsm_rts", C.c_int, [C.c_void_p, c_double_p, c_u8_p, C.POINTER(QsmGrid), c_double_p, C.POINTER(QsmRtsParams),
+                          PROGRESS_FN, C.c_void_p, c_double_p]),
+    ("qsm_rts_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(QsmGrid), c_double_p,
+                                 C.POINTER(QsmRtsParams), PROGRESS_FN, C.c_void_p, C.c_void_p]),
     ("qsm_tv_admm_unrolled_vjp_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(QsmGrid), c_double_p,
                                                   C.c_double, C.c_double, C.c_size_t, C.c_size_t, C.c_void_p,
                                                   C.c_void_p, C.c_void_p, c_double_p]),

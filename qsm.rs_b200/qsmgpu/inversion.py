@@ -48,6 +48,21 @@ class TikhonovParams:
 
 
 @dataclass
+class RtsParams:
+    """src/inversion/rts.rs:22-51."""
+
+    delta: float = 0.15
+    mu: float = 1e5
+    rho: float = 10.0
+    tol: float = 1e-2
+    max_iter: int = 20
+    lsmr_iter: int = 4
+
+    def _c(self):
+        return _lib.QsmRtsParams(self.delta, self.mu, self.rho, self.tol, int(self.max_iter), int(self.lsmr_iter))
+
+
+@dataclass
 class IlsqrParams:
     """src/inversion/ilsqr.rs:20-34."""
 
@@ -332,3 +347,20 @@ def tv_admm_unrolled_vjp_device(ctx: Context, d_local_field: int, d_mask: int, g
                                                          C.c_void_p(d_out_chi), C.c_void_p(d_out_grad_field or None),
                                                          C.byref(gl)))
     return gl.value
+
+
+def rts(local_field, mask, grid: Grid, bdir=(0.0, 0.0, 1.0), params: RtsParams = RtsParams(),
+        progress: Optional[Callable[[int, int], None]] = None, *, ctx: Optional[Context] = None):
+    """inversion::rts (src/inversion/rts.rs:72-211)."""
+    c = _ctx(ctx)
+    f = _as_f64(local_field, grid, "local_field")
+    m = _as_u8(mask, "mask")
+    _check_len(f, grid, "local_field")
+    _check_len(m, grid, "mask")
+    out = np.empty_like(f)
+    b, _keep = _bdir(bdir)
+    g = grid._c()
+    p = params._c()
+    cb, _cbkeep = _progress(progress)
+    _check(c, c._lib.qsm_rts(c.handle, _ptr_d(f), _ptr_u8(m), C.byref(g), b, C.byref(p), cb, None, _ptr_d(out)))
+    return out

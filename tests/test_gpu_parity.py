@@ -139,6 +139,33 @@ def test_tv_admm_early_exit_and_progress_f64(ctx64):
     assert rel(got, ref) < 1e-9
 
 
+@pytest.mark.parametrize("vs", [(0.9, 1.0, 1.2), (1.0, 0.9, 1.0), (1.0, 1.0, 0.9)])
+def test_tv_admm_anisotropic_f64(ctx64, vs):
+    """Anisotropic voxels on odd and even axes.  The GPU's Laplacian tables hold the exact
+    DC eigenvalue 0; the reference's FFT of the taps leaves roundoff there at some voxel
+    sizes, which only shifts the iterate by a constant (oracle exact_dc)."""
+    for dims in ((24, 28, 16), (25, 27, 15)):
+        grid = Grid.new(*dims, *vs)
+        c = phantom.tv_case(dims, seed=3, n_ellipsoids=6, mask_radius=min(dims) * 0.4, bdir=OBLIQUE, voxel_size=vs)
+        got = inversion.tv_admm(c.local_field, c.mask, grid, OBLIQUE, inversion.TvParams(2e-4, 2e-2, 0.0, 9),
+                                ctx=ctx64)
+        ref = O.tv_admm(c.local_field, c.mask, og(grid), OBLIQUE, O.TvParams(2e-4, 2e-2, 0.0, 9), exact_dc=True)
+        assert rel(got, ref) < 1e-9, (dims, rel(got, ref))
+
+
+def test_tv_admm_progress_at_max_iter_f64(ctx64):
+    """tol > 0 but no convergence: progress stops at (max_iter, max_iter's total)
+    (src/inversion/tv.rs:78-93), with the last iterate still tested."""
+    grid, c = _tv_case(20, 8)
+    calls, ref_calls = [], []
+    p = inversion.TvParams(1e-3, 0.1, 1e-9, 6)
+    inversion.tv_admm(c.local_field, c.mask, grid, (0, 0, 1), p, lambda a, b: calls.append((a, b)), ctx=ctx64)
+    O.tv_admm(c.local_field, c.mask, og(grid), (0, 0, 1), O.TvParams(1e-3, 0.1, 1e-9, 6),
+              lambda a, b: ref_calls.append((a, b)))
+    assert calls == ref_calls == [(i + 1, 6) for i in range(6)]
+    assert ctx64.tv_last_iterations() == 6
+
+
 def test_tv_admm_mixed_target(ctx32):
     grid, c = _tv_case(32, 9)
     p = inversion.TvParams(2e-4, 2e-2, 0.0, 60)

@@ -97,7 +97,7 @@ def loss_and_grads(qctx, grid, f, mask, chi_true, lam, rho, K, C, bdir=(0.0, 0.0
     chi = UnrolledTv.apply(ft, lt, mt, grid, bdir, rho, K, C, qctx)
     L = ((chi - torch.from_numpy(chi_true.ravel()).cuda()) ** 2).sum()
     L.backward()
-    return float(L), ft.grad.cpu().numpy(), float(lt.grad)
+    return float(L.detach()), ft.grad.cpu().numpy(), float(lt.grad)
 
 
 def loss_only(qctx, grid, f, mask, chi_true, lam, rho, K, C, bdir=(0.0, 0.0, 1.0)):

@@ -454,3 +454,43 @@ def test_apply_reference_known_answers():
     np.testing.assert_allclose(O.apply_reference([1.0, 2.0, 3.0, 4.0], [1, 1, 1, 0]), [-1.0, 0.0, 1.0, 0.0], atol=1e-10)
     assert list(O.apply_reference([1.0, 2.0, 3.0], [1, 0, 1], "none")) == [1.0, 0.0, 3.0]
     assert list(O.apply_reference([1.0, 2.0], [0, 0])) == [0.0, 0.0]
+
+
+def test_rts_reference_tests():
+    """src/inversion/rts.rs:213-263: zero field -> ~0; ramp -> finite; masked voxels zero."""
+    n = 8
+    grid = g(n)
+    p = O.RtsParams(0.15, 1e5, 10.0, 1e-2, 5, 2)
+    assert np.all(np.abs(O.rts(np.zeros((n, n, n)), np.ones((n, n, n), np.uint8), grid, (0, 0, 1), p)) < 1e-6)
+    field = (np.arange(n ** 3, dtype=np.float64) * 0.001).reshape(n, n, n)
+    mask = np.ones(n ** 3, np.uint8)
+    mask[0] = 0
+    mask[10] = 0
+    chi = O.rts(field, mask.reshape(n, n, n), grid, (0, 0, 1), p)
+    assert np.all(np.isfinite(chi)) and chi.ravel()[0] == 0.0 and chi.ravel()[10] == 0.0
+
+
+@pytest.mark.parametrize("solver", ["tv", "rts"])
+def test_laplacian_dc_roundoff_is_a_constant_offset(solver):
+    """src/inversion/admm.rs:159-167 and src/inversion/rts.rs:93-113 take the Laplacian's
+    eigenvalues from an FFT of its taps, so at voxel sizes whose taps do not sum to exactly
+    0 in floating point the DC eigenvalue is a few ulp and inv_a(0) is ~1e17.  The effect
+    is confined to k = 0: the faithful iterate and the one with the exact eigenvalue 0
+    differ by a constant over the grid, i.e. inside the mask."""
+    grid = O.Grid.new(24, 28, 16, 1.0, 1.0, 0.9)
+    lap = O.laplacian_eigenvalues(grid)
+    assert lap[0, 0, 0] != 0.0 and abs(lap[0, 0, 0]) < 1e-14
+    assert O.laplacian_eigenvalues(grid, exact_dc=True)[0, 0, 0] == 0.0
+    rng = np.random.default_rng(5)
+    mask = np.zeros(grid.shape, np.uint8)
+    mask[3:13, 4:24, 4:20] = 1
+    f = rng.normal(0, 0.01, grid.shape) * mask
+    if solver == "tv":
+        run = lambda e: O.tv_admm(f, mask, grid, (0, 0, 1), O.TvParams(2e-4, 2e-2, 0.0, 6), exact_dc=e)
+    else:
+        run = lambda e: O.rts(f, mask, grid, (0, 0, 1), O.RtsParams(0.15, 1e5, 10.0, 0.0, 6, 4), exact_dc=e)
+    faithful, exact = run(False), run(True)
+    diff = (faithful - exact)[mask != 0]
+    assert abs(diff.mean()) > 1e-6 * np.abs(exact).max()  # the roundoff does move the DC term
+    assert np.abs(diff - diff.mean()).max() < 1e-9 * np.abs(exact).max()
+    assert np.all((faithful - exact)[mask == 0] == 0.0)
