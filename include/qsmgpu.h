@@ -109,6 +109,9 @@ typedef struct {
 typedef struct { double radius, tik_reg, tol; size_t max_iter; } qsm_resharp_params;
 /* RtsParams — src/inversion/rts.rs:22-51 (delta 0.15, mu 1e5, rho 10, tol 1e-2, 20, 4). */
 typedef struct { double delta, mu, rho, tol; size_t max_iter, lsmr_iter; } qsm_rts_params;
+/* NltvParams — src/inversion/nltv.rs:24-48 (lambda 1e-3, mu 1, tol 1e-3, max_iter 250 per
+ * pass, newton_iter 10 passes). */
+typedef struct { double lambda, mu, tol; size_t max_iter, newton_iter; } qsm_nltv_params;
 /* IlsqrParams — src/inversion/ilsqr.rs:20-34 (tol 0.01, max_iter 50: the LSMR step's
  * tolerance and iteration cap). */
 typedef struct { double tol; size_t max_iter; } qsm_ilsqr_params;
@@ -120,6 +123,7 @@ QSM_API void qsm_sharp_params_default(qsm_sharp_params* p);
 QSM_API void qsm_vsharp_params_default(qsm_vsharp_params* p);
 QSM_API void qsm_ilsqr_params_default(qsm_ilsqr_params* p);
 QSM_API void qsm_rts_params_default(qsm_rts_params* p);
+QSM_API void qsm_nltv_params_default(qsm_nltv_params* p);
 QSM_API void qsm_resharp_params_default(qsm_resharp_params* p);
 QSM_API void qsm_tgv_params_default(qsm_tgv_params* p);
 
@@ -181,6 +185,15 @@ QSM_API qsm_status qsm_rts(qsm_ctx* ctx, const double* local_field, const uint8_
 QSM_API qsm_status qsm_rts_device(qsm_ctx* ctx, const double* d_local_field, const uint8_t* d_mask,
                                   const qsm_grid* grid, const double bdir[3], const qsm_rts_params* params,
                                   qsm_progress_fn progress, void* user, double* d_out_chi);
+
+/* inversion::nltv — src/inversion/nltv.rs:62-131.  Progress (k, max_iter * newton_iter)
+ * before every inner ADMM step, k running over all passes; no (k, k) call. */
+QSM_API qsm_status qsm_nltv(qsm_ctx* ctx, const double* local_field, const uint8_t* mask, const qsm_grid* grid,
+                            const double bdir[3], const qsm_nltv_params* params, qsm_progress_fn progress, void* user,
+                            double* out_chi);
+QSM_API qsm_status qsm_nltv_device(qsm_ctx* ctx, const double* d_local_field, const uint8_t* d_mask,
+                                   const qsm_grid* grid, const double bdir[3], const qsm_nltv_params* params,
+                                   qsm_progress_fn progress, void* user, double* d_out_chi);
 
 /* inversion::tkd — src/inversion/tkd.rs:48-99. */
 QSM_API qsm_status qsm_tkd(qsm_ctx* ctx, const double* local_field, const uint8_t* mask, const qsm_grid* grid,
@@ -333,6 +346,7 @@ typedef struct {
   qsm_tv_params tv;
   qsm_ilsqr_params ilsqr;
   qsm_rts_params rts;
+  qsm_nltv_params nltv;
 } qsm_inversion_config;
 
 /* BgRemovalAlgorithm — src/pipeline/config.rs:33-42, same variant order.  Variants

@@ -1455,3 +1455,61 @@ def rts(local_field, mask, grid: Grid, bdir, params: RtsParams = RtsParams(), pr
         gx, gy, gz = 2.0 * zx - vx, 2.0 * zy - vy, 2.0 * zz - vz
     out = apply_mask_zero(x, m)
     return (out, iters) if return_iters else out
+
+
+# ---------------------------------------------------------------------------
+# NLTV (src/inversion/nltv.rs)
+# ---------------------------------------------------------------------------
+@dataclass
+class NltvParams:  # src/inversion/nltv.rs:24-48
+    lambda_: float = 1e-3
+    mu: float = 1.0
+    tol: float = 1e-3
+    max_iter: int = 250
+    newton_iter: int = 10
+
+
+def nltv(local_field, mask, grid: Grid, bdir, params: NltvParams = NltvParams(), progress=None,
+         return_iters=False, exact_dc=False):
+    """src/inversion/nltv.rs:62-131 over the shared ADMM step (src/inversion/admm.rs:76-145).
+
+    rho = 100 lambda.  newton_iter outer passes, each an inner ADMM loop of at most
+    max_iter steps with the weighted shrink shrink(v, (lambda/rho) w_i) (src/utils/mod.rs:57-59)
+    and the usual relative-change exit.  x, x_prev, u and g carry over between passes,
+    except that after each pass g is overwritten with grad x (nltv.rs:114) and the weights
+    become 1/(|grad x| + mu 1e-6), divided by their maximum when that exceeds 1.
+    progress(k, max_iter * newton_iter) is called before every inner step with a running k.
+    """
+    rho = 100.0 * params.lambda_
+    inv_a, f_hat = prepare_admm_spectral(local_field, grid, bdir, rho, exact_dc)
+    shape = grid.shape
+    x = np.zeros(shape)
+    ux = np.zeros(shape); uy = np.zeros(shape); uz = np.zeros(shape)
+    gx = np.zeros(shape); gy = np.zeros(shape); gz = np.zeros(shape)
+    w = np.ones(shape)
+    total = params.max_iter * params.newton_iter
+    cur = 0
+    t = params.lambda_ / rho
+    for _ in range(params.newton_iter):
+        for _ in range(params.max_iter):
+            cur += 1
+            if progress is not None:
+                progress(cur, total)
+            x_prev = x
+            div = bdiv(gx, gy, gz, grid)
+            x = ifft3d(f_hat - rho * fft3d(div.astype(np.complex128)) * inv_a).real
+            if relative_change(x, x_prev) < params.tol:
+                break
+            ggx, ggy, ggz = fgrad(x, grid)
+            vx, vy, vz = ggx + ux, ggy + uy, ggz + uz
+            tw = t * w
+            zx, zy, zz = shrink(vx, tw), shrink(vy, tw), shrink(vz, tw)
+            ux, uy, uz = vx - zx, vy - zy, vz - zz
+            gx, gy, gz = 2.0 * zx - vx, 2.0 * zy - vy, 2.0 * zz - vz
+        gx, gy, gz = fgrad(x, grid)
+        w = 1.0 / (np.sqrt(gx * gx + gy * gy + gz * gz) + params.mu * 1e-6)
+        wmax = float(w.max(initial=0.0))
+        if wmax > 1.0:
+            w = w / wmax
+    out = apply_mask_zero(x, _vol(mask, grid, np.uint8))
+    return (out, cur) if return_iters else out

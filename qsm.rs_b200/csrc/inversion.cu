@@ -226,6 +226,7 @@ void qsm_inversion_config_default(qsm_inversion_config* c) {
   qsm_tv_params_default(&c->tv);
   qsm_ilsqr_params_default(&c->ilsqr);
   qsm_rts_params_default(&c->rts);
+  qsm_nltv_params_default(&c->nltv);
 }
 
 qsm_status qsm_run_dipole_inversion(qsm_ctx* ctx, const double* local_field_ppm, size_t len, const uint8_t* mask,
@@ -268,6 +269,11 @@ qsm_status qsm_run_dipole_inversion(qsm_ctx* ctx, const double* local_field_ppm,
       case QSM_INV_RTS:
         with_host_io(ctx, d.n, local_field_ppm, mask, out_chi, [&](const double* f, const uint8_t* m, double* o) {
           rts_device(ctx, f, m, &g, b, &cfg->rts, progress, user, o);
+        });
+        break;
+      case QSM_INV_NLTV:
+        with_host_io(ctx, d.n, local_field_ppm, mask, out_chi, [&](const double* f, const uint8_t* m, double* o) {
+          nltv_device(ctx, f, m, &g, b, &cfg->nltv, progress, user, o);
         });
         break;
       case QSM_INV_ILSQR:  // src/pipeline/inversion.rs:100-105: chi of the 4-tuple

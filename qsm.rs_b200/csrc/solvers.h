@@ -26,6 +26,8 @@ void apply_reference_device(qsm_ctx* ctx, long long N, const double* chi, const 
                             double* out);
 void rts_device(qsm_ctx* ctx, const double* f, const uint8_t* m, const qsm_grid* grid, const double bdir[3],
                 const qsm_rts_params* p, qsm_progress_fn progress, void* user, double* out);
+void nltv_device(qsm_ctx* ctx, const double* f, const uint8_t* m, const qsm_grid* grid, const double bdir[3],
+                 const qsm_nltv_params* p, qsm_progress_fn progress, void* user, double* out);
 void tgv_device(qsm_ctx* ctx, const double* phase, const uint8_t* mask, const qsm_grid* grid, const qsm_tgv_params* p,
                 const double b0[3], qsm_progress_fn progress, void* user, double* out);
 

@@ -98,11 +98,12 @@ struct TvState {
 // u_z at k-1 in registers.  grid = (ceil(nx/32), ceil(ny/8), ceil(nz/zchunk)).
 constexpr int kStepBX = 32, kStepBY = 8;
 
-template <typename T>
+template <typename T, bool WT>
 __global__ void __launch_bounds__(kStepBX* kStepBY)
-    k_tv_step(int nx, int ny, int nz, int zchunk, T hx, T hy, T hz, T thr, const T* __restrict__ x0,
-              const T* __restrict__ ycur, const T* __restrict__ yprev, const T* __restrict__ ui, T* __restrict__ uo,
-              T* __restrict__ div, double2* __restrict__ partials, TvState* st, int check_only) {
+    k_tv_step(int nx, int ny, int nz, int zchunk, T hx, T hy, T hz, T thr, const T* __restrict__ w,
+              const T* __restrict__ x0, const T* __restrict__ ycur, const T* __restrict__ yprev,
+              const T* __restrict__ ui, T* __restrict__ uo, T* __restrict__ div, double2* __restrict__ partials,
+              TvState* st, int check_only) {
   if (st->done) return;
   const int kiter = st->k;
   const bool check = kiter >= 2;
@@ -126,6 +127,7 @@ __global__ void __launch_bounds__(kStepBX* kStepBY)
   const int kmm = k0 > 0 ? k0 - 1 : nz - 1;
   T x_km = X(kmm * sz + rowj + i);
   T uz_km = check_only ? T(0) : ui[2 * N + kmm * sz + rowj + i];
+  T w_km = (WT && !check_only) ? w[kmm * sz + rowj + i] : T(1);
   T x_k = X(k0 * sz + rowj + i);
   double sd = 0.0, sx = 0.0;
   for (int k = k0; k < k1; ++k) {
@@ -153,17 +155,27 @@ __global__ void __launch_bounds__(kStepBX* kStepBY)
       const long long cjm = base + (long long)jm * nx + i;
       const T xjm = X(cjm);
       const T uym = ui[N + cjm];
+      // shrink thresholds: thr, or thr * w at each voxel whose g is formed (weighted
+      // shrink, src/utils/mod.rs:57-59)
+      T tc = thr, txm = thr, tym = thr, tzm = thr, w_k = T(1);
+      if (WT) {
+        w_k = w[c];
+        tc = thr * w_k;
+        txm = thr * w[base + rowj + im];
+        tym = thr * w[cjm];
+        tzm = thr * w_km;
+      }
       const T vx = (xip - x_k) * hx + ux;
       const T vy = (xjp - x_k) * hy + uy;
       const T vz = (x_kp - x_k) * hz + uz;
-      const T zx = shrink(vx, thr), zy = shrink(vy, thr), zz = shrink(vz, thr);
+      const T zx = shrink(vx, tc), zy = shrink(vy, tc), zz = shrink(vz, tc);
       const T gx = T(2) * zx - vx, gy = T(2) * zy - vy, gz = T(2) * zz - vz;
       const T vxm = (x_k - xim) * hx + uxm;
       const T vym = (x_k - xjm) * hy + uym;
       const T vzm = (x_k - x_km) * hz + uz_km;
-      const T gxm = T(2) * shrink(vxm, thr) - vxm;
-      const T gym = T(2) * shrink(vym, thr) - vym;
-      const T gzm = T(2) * shrink(vzm, thr) - vzm;
+      const T gxm = T(2) * shrink(vxm, txm) - vxm;
+      const T gym = T(2) * shrink(vym, tym) - vym;
+      const T gzm = T(2) * shrink(vzm, tzm) - vzm;
       if (in) {
         // the first update sees x_0 = u = g = 0 (admm.rs:18-53): zeros, whatever x_0's
         // buffer holds (RTS keeps its starting iterate there for the first test)
@@ -174,6 +186,7 @@ __global__ void __launch_bounds__(kStepBX* kStepBY)
         div[c] = z0 ? T(0) : (gx - gxm) * hx + (gy - gym) * hy + (gz - gzm) * hz;
       }
       uz_km = uz;
+      w_km = w_k;
     }
     x_km = x_k;
     x_k = x_kp;
@@ -245,12 +258,12 @@ template <> struct Vec16<double> {
 // k_tv_step with 16-byte vector loads and stores: each thread owns Vec16<T>::n
 // consecutive x (nx a multiple of that), x-neighbours across vectors come from the
 // adjacent lanes.  Same arithmetic per voxel as k_tv_step.
-template <typename T>
+template <typename T, bool WT>
 __global__ void __launch_bounds__(kStepBX* kStepBY)
-    k_tv_step_v(int nx, int ny, int nz, int zchunk, T hx, T hy, T hz, T thr, const T* __restrict__ x0,
-                const T* __restrict__ ycur, const T* __restrict__ yprev, const T* __restrict__ ui,
-                T* __restrict__ uo, T* __restrict__ div, double2* __restrict__ partials, TvState* st,
-                int check_only) {
+    k_tv_step_v(int nx, int ny, int nz, int zchunk, T hx, T hy, T hz, T thr, const T* __restrict__ w,
+                const T* __restrict__ x0, const T* __restrict__ ycur, const T* __restrict__ yprev,
+                const T* __restrict__ ui, T* __restrict__ uo, T* __restrict__ div, double2* __restrict__ partials,
+                TvState* st, int check_only) {
   using W = Vec16<T>;
   using V = typename W::V;
   constexpr int NV = W::n;
@@ -283,8 +296,9 @@ __global__ void __launch_bounds__(kStepBX* kStepBY)
   const long long rowj = (long long)j * nx;
   const int kmm = k0 > 0 ? k0 - 1 : nz - 1;
   V x_km = X(kmm * sz + rowj + i);
-  V uz_km{};
+  V uz_km{}, w_km{};
   if (!check_only) uz_km = W::ld(ui + 2 * N + kmm * sz + rowj + i);
+  if (WT && !check_only) w_km = W::ld(w + kmm * sz + rowj + i);
   V x_k = X(k0 * sz + rowj + i);
   double sd = 0.0, sx = 0.0;
   for (int k = k0; k < k1; ++k) {
@@ -315,6 +329,15 @@ __global__ void __launch_bounds__(kStepBX* kStepBY)
       const long long cjm = base + (long long)jm * nx + i;
       const V xjm = X(cjm);
       const V uym = W::ld(ui + N + cjm);
+      // weighted shrink thresholds (src/utils/mod.rs:57-59), as in k_tv_step
+      V w_k{}, wjm{};
+      T wprev = T(1);
+      if (WT) {
+        w_k = W::ld(w + c);
+        wjm = W::ld(w + cjm);
+        wprev = __shfl_up_sync(0xffffffffu, w_k.v[NV - 1], 1);
+        if (!shf_m) wprev = w[base + rowj + im];
+      }
       V ox, oy, oz, dv;
 #pragma unroll
       for (int e = 0; e < NV; ++e) {
@@ -322,17 +345,21 @@ __global__ void __launch_bounds__(kStepBX* kStepBY)
         const T xip = e + 1 < NV ? x_k.v[e + 1] : xnext;
         const T xim = e > 0 ? x_k.v[e - 1] : xprev;
         const T uxm = e > 0 ? ux.v[e - 1] : uxprev;
+        const T tc = WT ? thr * w_k.v[e] : thr;
+        const T txm = WT ? thr * (e > 0 ? w_k.v[e - 1] : wprev) : thr;
+        const T tym = WT ? thr * wjm.v[e] : thr;
+        const T tzm = WT ? thr * w_km.v[e] : thr;
         const T vx = (xip - xe) * hx + ux.v[e];
         const T vy = (xjp.v[e] - xe) * hy + uy.v[e];
         const T vz = (x_kp.v[e] - xe) * hz + uz.v[e];
-        const T zx = shrink(vx, thr), zy = shrink(vy, thr), zz = shrink(vz, thr);
+        const T zx = shrink(vx, tc), zy = shrink(vy, tc), zz = shrink(vz, tc);
         const T gx = T(2) * zx - vx, gy = T(2) * zy - vy, gz = T(2) * zz - vz;
         const T vxm = (xe - xim) * hx + uxm;
         const T vym = (xe - xjm.v[e]) * hy + uym.v[e];
         const T vzm = (xe - x_km.v[e]) * hz + uz_km.v[e];
-        const T gxm = T(2) * shrink(vxm, thr) - vxm;
-        const T gym = T(2) * shrink(vym, thr) - vym;
-        const T gzm = T(2) * shrink(vzm, thr) - vzm;
+        const T gxm = T(2) * shrink(vxm, txm) - vxm;
+        const T gym = T(2) * shrink(vym, tym) - vym;
+        const T gzm = T(2) * shrink(vzm, tzm) - vzm;
         ox.v[e] = vx - zx;
         oy.v[e] = vy - zy;
         oz.v[e] = vz - zz;
@@ -351,6 +378,7 @@ __global__ void __launch_bounds__(kStepBX* kStepBY)
         W::st(div + c, dv);
       }
       uz_km = uz;
+      if (WT) w_km = w_k;
     }
     x_km = x_k;
     x_k = x_kp;
@@ -416,6 +444,7 @@ template <typename T> struct TvVol {
   int zchunk;
   bool vec, use_mult;
   T hx, hy, hz, thr, scale;
+  const T* w = nullptr;  // per-voxel shrink weights (NLTV); nullptr: unweighted
   const uint8_t* mask;
   double* out;
 };
@@ -497,22 +526,28 @@ void tv_setup(qsm_ctx* ctx, TvVol<T>& v, const std::string& pre, const GridDims&
 // u = ub[1-q]; writes u' = ub[q], y_i = yb[q]
 template <typename T> void tv_step_launch(qsm_ctx* ctx, const TvVol<T>& v, int q, int check_only) {
   LaunchScope ls(ctx, "tv_step");
-  auto kern = v.vec ? k_tv_step_v<T> : k_tv_step<T>;
+  auto kern = v.w ? (v.vec ? k_tv_step_v<T, true> : k_tv_step<T, true>)
+                  : (v.vec ? k_tv_step_v<T, false> : k_tv_step<T, false>);
   kern<<<v.sgrid, dim3(kStepBX, kStepBY), 0, ctx->stream>>>(v.d.nx, v.d.ny, v.d.nz, v.zchunk, v.hx, v.hy, v.hz,
-                                                              v.thr, v.x0, v.yb[1 - q], v.yb[q], v.ub[1 - q],
+                                                              v.thr, v.w, v.x0, v.yb[1 - q], v.yb[q], v.ub[1 - q],
                                                               v.ub[q], v.div, v.partials, v.st, check_only);
   ls.done();
 }
 
-template <typename T> void tv_iter(qsm_ctx* ctx, const TvVol<T>& v, int q) {
+// y_i = Re IFFT(rho * sym(inv_a) * F(div)) into yb[q], skipped once the state is done
+template <typename T> void tv_fft(qsm_ctx* ctx, const TvVol<T>& v, int q) {
   const int* done = &v.st->done;
-  tv_step_launch(ctx, v, q, 0);
   run_x_r2c<T>(ctx, v.f, v.spec, LoadCast<T, T>{v.div, v.d.nx}, done);
   run_yz<T, -1, 1>(ctx, v.f, v.spec, v.spec, OpId<T>{}, done);
   if (v.use_mult) run_z_fused_m<T>(ctx, v.f, v.spec, v.spec, v.mult, done);
   else run_z_fused<T>(ctx, v.f, v.spec, v.spec, v.mul, done);
   run_yz<T, +1, 1>(ctx, v.f, v.spec, v.spec, OpId<T>{}, done);
   run_x_c2r<T>(ctx, v.f, v.spec, StoreReal<T>{v.yb[q], v.d.nx, v.scale}, done);
+}
+
+template <typename T> void tv_iter(qsm_ctx* ctx, const TvVol<T>& v, int q) {
+  tv_step_launch(ctx, v, q, 0);
+  tv_fft(ctx, v, q);
 }
 
 template <typename T> void tv_out_launch(qsm_ctx* ctx, const TvVol<T>& v, size_t completed) {
@@ -530,6 +565,62 @@ inline cudaGraphExec_t instantiate(qsm_ctx* ctx, cudaGraph_t graph) {
   return exec;
 }
 
+
+// Enqueue iterations first..last (1-based, inclusive) of an initialised volume whose
+// TvState has k == first.  Pairs of iterations run as one CUDA graph; when `watch`,
+// poll() (which reads the device state and returns true once done) runs every 16
+// iterations, so that a converged solve stops launching.  Returns poll()'s last answer
+// (false when it never ran).
+template <typename T, class Poll>
+bool tv_iterate(qsm_ctx* ctx, const TvVol<T>& v, size_t first, size_t last, bool watch, const Poll& poll) {
+  if (last < first) return false;
+  const size_t count = last - first + 1;
+  bool converged = false;
+  if (ctx->profiling || count < 2) {
+    // eager launches (per-kernel timing, or too short to be worth a graph)
+    for (size_t it = first; it <= last && !converged; ++it) {
+      tv_iter(ctx, v, (int)(it % 2));
+      if (watch && ((it - first + 1) % 16 == 0)) converged = poll();
+    }
+    return converged;
+  }
+  const int q0 = (int)(first % 2);
+  cudaGraph_t graph = nullptr;
+  const uint64_t l0 = ctx->launches;
+  QSM_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  try {
+    tv_iter(ctx, v, q0);
+    tv_iter(ctx, v, 1 - q0);
+  } catch (...) {
+    cudaStreamEndCapture(ctx->stream, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    throw;
+  }
+  QSM_CUDA(cudaStreamEndCapture(ctx->stream, &graph));
+  const uint64_t per_pair = ctx->launches - l0;
+  ctx->launches = l0;
+  cudaGraphExec_t exec = instantiate(ctx, graph);
+  const size_t pairs = count / 2;
+  const size_t chunk = 8;  // graph launches (16 iterations) between host polls when watching
+  try {
+    size_t launched = 0;
+    while (launched < pairs && !converged) {
+      const size_t todo = watch ? std::min(chunk, pairs - launched) : (pairs - launched);
+      for (size_t c = 0; c < todo; ++c) {
+        QSM_CUDA(cudaGraphLaunch(exec, ctx->stream));
+        ctx->launches += per_pair;
+      }
+      launched += todo;
+      if (watch) converged = poll();
+    }
+    if (!converged && (count % 2 == 1)) tv_iter(ctx, v, (int)(last % 2));
+  } catch (...) {
+    cudaGraphExecDestroy(exec);
+    throw;
+  }
+  cudaGraphExecDestroy(exec);
+  return converged;
+}
 
 // Iterate an initialised volume (tv_setup or an equivalent) until relative_change < tol
 // or max_iter iterations, write chi, and deliver progress as (iter, max_iter) per
@@ -550,51 +641,8 @@ size_t tv_run(qsm_ctx* ctx, const TvVol<T>& v, size_t max_iter, double tol, qsm_
       for (; reported < completed; ++reported) progress(user, reported + 1, max_iter);
     return hs.done != 0;
   };
-
-  bool converged = false;
-  if (ctx->profiling || max_iter < 2) {
-    // eager launches (per-kernel timing, or too short to be worth a graph)
-    for (size_t it = 1; it <= max_iter && !converged; ++it) {
-      tv_iter(ctx, v, (int)(it % 2));
-      if (watch && (it % 16 == 0)) converged = poll();
-    }
-  } else {
-    cudaGraph_t graph = nullptr;
-    const uint64_t l0 = ctx->launches;
-    QSM_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    try {
-      tv_iter(ctx, v, 1);
-      tv_iter(ctx, v, 0);
-    } catch (...) {
-      cudaStreamEndCapture(ctx->stream, &graph);
-      if (graph) cudaGraphDestroy(graph);
-      throw;
-    }
-    QSM_CUDA(cudaStreamEndCapture(ctx->stream, &graph));
-    const uint64_t per_pair = ctx->launches - l0;
-    ctx->launches = l0;
-    cudaGraphExec_t exec = instantiate(ctx, graph);
-    const size_t pairs = max_iter / 2;
-    const size_t chunk = 8;  // graph launches (16 iterations) between host polls when watching
-    try {
-      size_t launched = 0;
-      while (launched < pairs && !converged) {
-        const size_t todo = watch ? std::min(chunk, pairs - launched) : (pairs - launched);
-        for (size_t c = 0; c < todo; ++c) {
-          QSM_CUDA(cudaGraphLaunch(exec, ctx->stream));
-          ctx->launches += per_pair;
-        }
-        launched += todo;
-        if (watch) converged = poll();
-      }
-      if (!converged && (max_iter % 2 == 1)) tv_iter(ctx, v, 1);
-    } catch (...) {
-      cudaGraphExecDestroy(exec);
-      throw;
-    }
-    cudaGraphExecDestroy(exec);
-  }
-  converged = poll();
+  tv_iterate(ctx, v, 1, max_iter, watch, poll);
+  bool converged = poll();
   size_t completed = converged ? (size_t)hs.conv_iter : max_iter;
   if (!converged && max_iter >= 1 && tol > 0.0) {
     // the reference also tests the last iterate (tv.rs:85-91)

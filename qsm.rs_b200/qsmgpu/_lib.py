@@ -66,6 +66,11 @@ class QsmRtsParams(C.Structure):
                 ("max_iter", C.c_size_t), ("lsmr_iter", C.c_size_t)]
 
 
+class QsmNltvParams(C.Structure):
+    _fields_ = [("lambda_", C.c_double), ("mu", C.c_double), ("tol", C.c_double), ("max_iter", C.c_size_t),
+                ("newton_iter", C.c_size_t)]
+
+
 class QsmIlsqrParams(C.Structure):
     _fields_ = [("tol", C.c_double), ("max_iter", C.c_size_t)]
 
@@ -89,7 +94,7 @@ class QsmScanMetadata(C.Structure):
 class QsmInversionConfig(C.Structure):
     _fields_ = [("algorithm", C.c_int), ("tkd", QsmTkdParams), ("tsvd", QsmTkdParams),
                 ("tikhonov", QsmTikhonovParams), ("tv", QsmTvParams), ("ilsqr", QsmIlsqrParams),
-                ("rts", QsmRtsParams)]
+                ("rts", QsmRtsParams), ("nltv", QsmNltvParams)]
 
 
 class QsmBgRemovalConfig(C.Structure):
@@ -117,6 +122,11 @@ _SIGS = [
     ("qsm_tv_params_default", None, [C.POINTER(QsmTvParams)]),
     ("qsm_ilsqr_params_default", None, [C.POINTER(QsmIlsqrParams)]),
     ("qsm_rts_params_default", None, [C.POINTER(QsmRtsParams)]),
+    ("qsm_nltv_params_default", None, [C.POINTER(QsmNltvParams)]),
+    ("qsm_nltv", C.c_int, [C.c_void_p, c_double_p, c_u8_p, C.POINTER(QsmGrid), c_double_p, C.POINTER(QsmNltvParams),
+                           PROGRESS_FN, C.c_void_p, c_double_p]),
+    ("qsm_nltv_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(QsmGrid), c_double_p,
+                                  C.POINTER(QsmNltvParams), PROGRESS_FN, C.c_void_p, C.c_void_p]),
     ("qsm_rts", C.c_int, [C.c_void_p, c_double_p, c_u8_p, C.POINTER(QsmGrid), c_double_p, C.POINTER(QsmRtsParams),
                           PROGRESS_FN, C.c_void_p, c_double_p]),
     ("qsm_rts_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(QsmGrid), c_double_p,

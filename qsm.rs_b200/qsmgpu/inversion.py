@@ -63,6 +63,20 @@ class RtsParams:
 
 
 @dataclass
+class NltvParams:
+    """src/inversion/nltv.rs:24-48."""
+
+    lambda_: float = 1e-3
+    mu: float = 1.0
+    tol: float = 1e-3
+    max_iter: int = 250
+    newton_iter: int = 10
+
+    def _c(self):
+        return _lib.QsmNltvParams(self.lambda_, self.mu, self.tol, int(self.max_iter), int(self.newton_iter))
+
+
+@dataclass
 class IlsqrParams:
     """src/inversion/ilsqr.rs:20-34."""
 
@@ -363,4 +377,21 @@ def rts(local_field, mask, grid: Grid, bdir=(0.0, 0.0, 1.0), params: RtsParams =
     p = params._c()
     cb, _cbkeep = _progress(progress)
     _check(c, c._lib.qsm_rts(c.handle, _ptr_d(f), _ptr_u8(m), C.byref(g), b, C.byref(p), cb, None, _ptr_d(out)))
+    return out
+
+
+def nltv(local_field, mask, grid: Grid, bdir=(0.0, 0.0, 1.0), params: NltvParams = NltvParams(),
+         progress: Optional[Callable[[int, int], None]] = None, *, ctx: Optional[Context] = None):
+    """inversion::nltv (src/inversion/nltv.rs:62-131)."""
+    c = _ctx(ctx)
+    f = _as_f64(local_field, grid, "local_field")
+    m = _as_u8(mask, "mask")
+    _check_len(f, grid, "local_field")
+    _check_len(m, grid, "mask")
+    out = np.empty_like(f)
+    b, _keep = _bdir(bdir)
+    g = grid._c()
+    p = params._c()
+    cb, _cbkeep = _progress(progress)
+    _check(c, c._lib.qsm_nltv(c.handle, _ptr_d(f), _ptr_u8(m), C.byref(g), b, C.byref(p), cb, None, _ptr_d(out)))
     return out

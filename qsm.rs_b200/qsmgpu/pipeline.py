@@ -9,7 +9,7 @@ import numpy as np
 
 from . import _lib
 from . import Context, _ctx, _check, _ptr_d, _ptr_u8, _progress
-from .inversion import IlsqrParams, RtsParams, TkdParams, TikhonovParams, TvParams
+from .inversion import IlsqrParams, NltvParams, RtsParams, TkdParams, TikhonovParams, TvParams
 from .bgremove import ResharpParams, SharpParams, VsharpParams
 
 # InversionAlgorithm, src/pipeline/config.rs:47-58
@@ -45,10 +45,11 @@ class InversionConfig:
     tv: TvParams = field(default_factory=TvParams)
     ilsqr: IlsqrParams = field(default_factory=IlsqrParams)
     rts: RtsParams = field(default_factory=RtsParams)
+    nltv: NltvParams = field(default_factory=NltvParams)
 
     def _c(self):
         return _lib.QsmInversionConfig(self.algorithm, self.tkd._c(), self.tsvd._c(), self.tikhonov._c(),
-                                       self.tv._c(), self.ilsqr._c(), self.rts._c())
+                                       self.tv._c(), self.ilsqr._c(), self.rts._c(), self.nltv._c())
 
 
 @dataclass

@@ -71,6 +71,10 @@ def test_host_only_entry_points(lib):
     lib.qsm_inversion_config_default(C.byref(ic))
     assert ic.algorithm == 4  # Rts, src/pipeline/config.rs:251
     assert (ic.ilsqr.tol, ic.ilsqr.max_iter) == (0.01, 50)
+    assert (ic.rts.delta, ic.rts.mu, ic.rts.rho, ic.rts.tol, ic.rts.max_iter, ic.rts.lsmr_iter) == \
+        (0.15, 1e5, 10.0, 1e-2, 20, 4)  # src/inversion/rts.rs:40-51
+    assert (ic.nltv.lambda_, ic.nltv.mu, ic.nltv.tol, ic.nltv.max_iter, ic.nltv.newton_iter) == \
+        (1e-3, 1.0, 1e-3, 250, 10)  # src/inversion/nltv.rs:38-48
     bc = _lib.QsmBgRemovalConfig()
     lib.qsm_bg_removal_config_default(C.byref(bc))
     assert bc.algorithm == 0  # Vsharp

@@ -133,7 +133,7 @@ def test_vjp_matches_torch_float64_autograd(request, prec, tol, K, C):
     chi = torch_unrolled_tv(ft, lt, torch.from_numpy(mask.astype(np.float64)), grid, (0.0, 0.0, 1.0), rho, K)
     Lr = ((chi - torch.from_numpy(chi_true)) ** 2).sum()
     Lr.backward()
-    assert abs(L - float(Lr)) / float(Lr) < tol
+    assert abs(L - float(Lr.detach())) / float(Lr.detach()) < tol
     assert rel(gf, ft.grad.numpy()) < tol, rel(gf, ft.grad.numpy())
     if lt.grad is None:  # K = 1: the first iterate does not depend on lambda
         assert gl == 0.0

@@ -494,3 +494,40 @@ def test_laplacian_dc_roundoff_is_a_constant_offset(solver):
     assert abs(diff.mean()) > 1e-6 * np.abs(exact).max()  # the roundoff does move the DC term
     assert np.abs(diff - diff.mean()).max() < 1e-9 * np.abs(exact).max()
     assert np.all((faithful - exact)[mask == 0] == 0.0)
+
+
+def test_nltv_reference_tests():
+    """src/inversion/nltv.rs:137-177: zero field -> 0, ramp -> finite, weighted_shrink."""
+    n = 8
+    grid = g(n)
+    p = O.NltvParams(1e-3, 1.0, 1e-2, 10, 2)
+    ones = np.ones((n, n, n), np.uint8)
+    assert np.all(np.abs(O.nltv(np.zeros((n, n, n)), ones, grid, (0, 0, 1), p)) < 1e-8)
+    field = (np.arange(n ** 3, dtype=np.float64) * 0.001).reshape(n, n, n)
+    assert np.all(np.isfinite(O.nltv(field, ones, grid, (0, 0, 1), p)))
+    ws = lambda x, t, w: float(O.shrink(x, t * w))
+    assert abs(ws(1.0, 0.5, 1.0) - 0.5) < 1e-10 and abs(ws(-1.0, 0.5, 1.0) + 0.5) < 1e-10
+    assert abs(ws(0.3, 0.5, 1.0)) < 1e-10
+    assert abs(ws(1.0, 0.5, 0.5) - 0.75) < 1e-10 and abs(ws(0.3, 0.5, 0.5) - 0.05) < 1e-10
+
+
+def test_nltv_single_pass_is_weighted_tv():
+    """With one outer pass the weights stay 1, so NLTV is TV-ADMM with rho = 100 lambda
+    (src/inversion/nltv.rs:76-106 against src/inversion/tv.rs:63-97)."""
+    grid = O.Grid.new(12, 10, 8)
+    rng = np.random.default_rng(2)
+    f = rng.normal(0, 0.01, grid.shape)
+    m = np.ones(grid.shape, np.uint8)
+    a = O.nltv(f, m, grid, (0, 0, 1), O.NltvParams(2e-3, 1.0, 0.0, 7, 1))
+    b = O.tv_admm(f, m, grid, (0, 0, 1), O.TvParams(2e-3, 0.2, 0.0, 7))
+    assert np.abs(a - b).max() < 1e-14
+
+
+def test_nltv_progress_contract():
+    """progress(k, max_iter * newton_iter) before every inner step; no (k, k) call."""
+    grid = g(8)
+    f = np.sin(np.arange(512) * 0.7).reshape(grid.shape) * 0.01
+    calls = []
+    _, k = O.nltv(f, np.ones(grid.shape, np.uint8), grid, (0, 0, 1), O.NltvParams(1e-3, 1.0, 5e-2, 20, 3),
+                  lambda a, b: calls.append((a, b)), return_iters=True)
+    assert calls == [(i + 1, 60) for i in range(k)] and k < 60
