@@ -107,6 +107,8 @@ typedef struct {
 } qsm_tgv_params;
 /* ResharpParams — src/bgremove/resharp.rs:22-45 (radius 6 mm, tik_reg 1e-4, tol 1e-6, 30). */
 typedef struct { double radius, tik_reg, tol; size_t max_iter; } qsm_resharp_params;
+/* IsmvParams — src/bgremove/ismv.rs:19-35 (tol 1e-6, max_iter 50, radius 5 mm). */
+typedef struct { double tol; size_t max_iter; double radius; } qsm_ismv_params;
 /* RtsParams — src/inversion/rts.rs:22-51 (delta 0.15, mu 1e5, rho 10, tol 1e-2, 20, 4). */
 typedef struct { double delta, mu, rho, tol; size_t max_iter, lsmr_iter; } qsm_rts_params;
 /* NltvParams — src/inversion/nltv.rs:24-48 (lambda 1e-3, mu 1, tol 1e-3, max_iter 250 per
@@ -124,6 +126,7 @@ QSM_API void qsm_vsharp_params_default(qsm_vsharp_params* p);
 QSM_API void qsm_ilsqr_params_default(qsm_ilsqr_params* p);
 QSM_API void qsm_rts_params_default(qsm_rts_params* p);
 QSM_API void qsm_nltv_params_default(qsm_nltv_params* p);
+QSM_API void qsm_ismv_params_default(qsm_ismv_params* p);
 QSM_API void qsm_resharp_params_default(qsm_resharp_params* p);
 QSM_API void qsm_tgv_params_default(qsm_tgv_params* p);
 
@@ -271,6 +274,14 @@ QSM_API qsm_status qsm_laplacian_unwrap_device(qsm_ctx* ctx, const double* d_pha
 /* bgremove::smv — src/bgremove/smv.rs:31-59. */
 QSM_API qsm_status qsm_smv(qsm_ctx* ctx, const double* field, const uint8_t* mask, const qsm_grid* grid, double radius,
                    double* out_local, uint8_t* out_mask);
+/* bgremove::ismv — src/bgremove/ismv.rs:48-166: (local field, eroded mask).  Progress
+ * (iter, max_iter) per iteration and (iter, iter) when the change falls below tol. */
+QSM_API qsm_status qsm_ismv(qsm_ctx* ctx, const double* field, const uint8_t* mask, const qsm_grid* grid,
+                            const qsm_ismv_params* params, qsm_progress_fn progress, void* user, double* out_local,
+                            uint8_t* out_mask);
+QSM_API qsm_status qsm_ismv_device(qsm_ctx* ctx, const double* d_field, const uint8_t* d_mask, const qsm_grid* grid,
+                                   const qsm_ismv_params* params, qsm_progress_fn progress, void* user,
+                                   double* d_out_local, uint8_t* d_out_mask);
 /* bgremove::sharp — src/bgremove/sharp.rs:51-131. */
 QSM_API qsm_status qsm_sharp(qsm_ctx* ctx, const double* field, const uint8_t* mask, const qsm_grid* grid,
                      const qsm_sharp_params* params, double* out_local, uint8_t* out_mask);
@@ -368,6 +379,7 @@ typedef struct {
   qsm_vsharp_params vsharp;
   qsm_sharp_params sharp;
   qsm_resharp_params resharp;
+  qsm_ismv_params ismv;
 } qsm_bg_removal_config;
 
 QSM_API void qsm_inversion_config_default(qsm_inversion_config* c);

@@ -1513,3 +1513,47 @@ def nltv(local_field, mask, grid: Grid, bdir, params: NltvParams = NltvParams(),
             w = w / wmax
     out = apply_mask_zero(x, _vol(mask, grid, np.uint8))
     return (out, cur) if return_iters else out
+
+
+# ---------------------------------------------------------------------------
+# iSMV (src/bgremove/ismv.rs)
+# ---------------------------------------------------------------------------
+@dataclass
+class IsmvParams:  # src/bgremove/ismv.rs:19-34
+    tol: float = 1e-6
+    max_iter: int = 50
+    radius: float = 5.0
+
+
+def ismv(field_, mask, grid: Grid, params: IsmvParams = IsmvParams(), progress=None, return_iters=False):
+    """src/bgremove/ismv.rs:48-157: erode with the SMV kernel at 1 - 1e-10, then
+    f <- eroded * Re IFFT(F(f) * FFT(S)) + (mask - eroded) * field until the change
+    ||f0 - f|| <= tol * ||eroded * field|| (tested at the top of each iteration, f0 the
+    previous f, initially eroded * field).  Returns (mask * (field - f), eroded)."""
+    s = smv_kernel(grid, params.radius)
+    s_fft = fft3d(s.astype(np.complex128))  # complex, as the iteration uses it (ismv.rs:80-85)
+    m = _vol(mask, grid, np.uint8)
+    eroded = erode_mask_smv(m, fft_real_kernel(s), 1.0 - 1e-10).astype(np.float64)
+    m0 = (m != 0).astype(np.float64)
+    fld = _vol(field_, grid)
+    bc = fld * (m0 - eroded)
+    f = fld.copy()
+    f0 = fld * eroded
+    nr = math.sqrt(float(np.dot(f0.ravel(), f0.ravel())))
+    eps = params.tol * nr
+    done = 0
+    for it in range(params.max_iter):
+        if progress is not None:
+            progress(it + 1, params.max_iter)
+        if nr <= eps:
+            if progress is not None:
+                progress(it + 1, it + 1)
+            break
+        f = eroded * ifft3d(fft3d(f.astype(np.complex128)) * s_fft).real + bc
+        d = (f0 - f).ravel()
+        nr = math.sqrt(float(np.dot(d, d)))
+        f0 = f
+        done = it + 1
+    local = np.where(m != 0, fld - f, 0.0)
+    out = (local, (eroded > 0.5).astype(np.uint8))
+    return out + (done,) if return_iters else out

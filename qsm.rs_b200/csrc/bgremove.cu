@@ -304,6 +304,223 @@ void smv_impl(qsm_ctx* ctx, const GridDims& d, const double* field, const uint8_
   run_x_c2r<T>(ctx, f, spec, StoreSmvLocal<T>{field, out_mask, out_local, d.nx, (T)(1.0 / (double)d.n)}, nullptr);
 }
 
+// ------------------------------------------------------------------ iSMV --
+// src/bgremove/ismv.rs:48-157.  Device state: iterations done, the change norm and its
+// tolerance; the iteration whose top-of-loop test stops the loop (0: none).
+struct IsmvState {
+  int done;
+  int k;  // iterations completed
+  unsigned counter;
+  int stop_at;
+  double nr, eps;
+};
+
+// f_0 = field; nr_0 = ||eroded * field||, eps = tol * nr_0 (ismv.rs:106-120); a zero
+// norm stops the loop at its first test
+template <typename T>
+__global__ void k_ismv_init(long long N, const double* __restrict__ field, const uint8_t* __restrict__ eroded,
+                            double tol, size_t max_iter, T* __restrict__ f, IsmvState* st, double* partials) {
+  double acc[1] = {0.0};
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+    const double v = field[i];
+    f[i] = (T)v;
+    const double e = v * (double)eroded[i];
+    acc[0] += e * e;
+  }
+  if (grid_sum_last<1>(acc, partials, &st->counter) && threadIdx.x == 0) {
+    const double nr = sqrt(acc[0]);
+    st->nr = nr;
+    st->eps = tol * nr;
+    st->k = 0;
+    st->stop_at = 0;
+    st->done = 0;
+    if (max_iter > 0 && nr <= tol * nr) {
+      st->done = 1;
+      st->stop_at = 1;
+    }
+  }
+}
+
+// f_k = eroded * Re IFFT(F(f_{k-1}) S) + (m0 - eroded) field, FP64 sum of (f0 - f_k)^2
+// with f0 = eroded * field at k = 1 and f_{k-1} after (ismv.rs:127-155); the last block
+// stores the norm and runs the next iteration's top-of-loop test.
+template <typename T> struct StoreIsmv {
+  T* out;
+  const T* prev;  // f_{k-1}, or null at k = 1
+  const double* field;
+  const uint8_t* mask;
+  const uint8_t* eroded;
+  int nx;
+  T scale;
+  IsmvState* st;
+  double* partials;
+  int max_iter;
+  double acc[1];
+  __device__ __forceinline__ void operator()(int row, int e, T v) {
+    const long long i = (long long)row * nx + e;
+    const double er = (double)eroded[i];
+    const double fld = field[i];
+    const double m0 = mask[i] != 0 ? 1.0 : 0.0;
+    const T fn = (T)(er * (double)(v * scale) + fld * (m0 - er));
+    out[i] = fn;
+    const double f0 = prev ? (double)prev[i] : fld * er;
+    const double dd = f0 - (double)fn;
+    acc[0] += dd * dd;
+  }
+  __device__ void finish() {
+    if (!grid_sum_last<1>(acc, partials, &st->counter)) return;
+    if (threadIdx.x + blockDim.x * threadIdx.y != 0) return;
+    const double nr = sqrt(acc[0]);
+    st->nr = nr;
+    const int k = st->k + 1;
+    st->k = k;
+    if (k < max_iter && nr <= st->eps) {
+      st->done = 1;
+      st->stop_at = k + 1;
+    }
+  }
+};
+
+// local = mask ? field - f : 0 (ismv.rs:158-164)
+template <typename T>
+__global__ void k_ismv_out(long long N, const double* __restrict__ field, const uint8_t* __restrict__ mask,
+                           const T* __restrict__ f, double* __restrict__ out) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
+    out[i] = mask[i] != 0 ? field[i] - (double)f[i] : 0.0;
+}
+
+template <typename T>
+__global__ void k_re_spectrum(long long H, const double2* __restrict__ S, T* __restrict__ out) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < H; i += (long long)gridDim.x * blockDim.x)
+    out[i] = (T)S[i].x;
+}
+
+template <typename T> struct OpMulRe {
+  using C = cplx_t<T>;
+  const T* m;
+  __device__ __forceinline__ C mid(C v, int, int, int, long long idx) const { return cscale(v, m[idx]); }
+};
+
+template <typename T> struct LoadVol {
+  const T* p;
+  int nx;
+  __device__ __forceinline__ T operator()(int row, int e) const { return p[(long long)row * nx + e]; }
+};
+
+template <typename T>
+void ismv_impl(qsm_ctx* ctx, const GridDims& d, const double* field, const uint8_t* mask,
+               const qsm_ismv_params& p, qsm_progress_fn progress, void* user, double* out_local,
+               uint8_t* out_mask) {
+  using C = cplx_t<T>;
+  Fft3<double> f64 = make_fft3<double>(ctx, d);
+  Fft3<T> f = make_fft3<T>(ctx, d);
+  const size_t H = (size_t)f.g.hsize();
+  const long long N = d.n;
+  const std::string pre = sizeof(T) == 4 ? "ismv32." : "ismv64.";
+  double2* S = ws<double2>(ctx, "bg.S", H);
+  double2* Fm = ws<double2>(ctx, "bg.Fm", H);
+  T* Sr = ws<T>(ctx, pre + "Sr", H);
+  C* spec = ws<C>(ctx, pre + "spec", H);
+  T* fb[2] = {ws<T>(ctx, pre + "f0", (size_t)N), ws<T>(ctx, pre + "f1", (size_t)N)};
+  IsmvState* st = ws<IsmvState>(ctx, pre + "state", 1);
+  double* partials = ws<double>(ctx, pre + "partials", (size_t)kMaxPersistentBlocks);
+  QSM_CUDA(cudaMemsetAsync(st, 0, sizeof(IsmvState), ctx->stream));
+  smv_spectrum(ctx, f64, d, p.radius, S);
+  forward3<double>(ctx, f64, LoadCast<uint8_t, double>{mask, d.nx}, Fm);
+  erode_smv(ctx, f64, d, Fm, S, 1.0 - 1e-10, out_mask);  // ismv.rs:166-169
+  {
+    LaunchScope ls(ctx, "ismv_init");
+    k_re_spectrum<T><<<grid1d((long long)H), 256, 0, ctx->stream>>>((long long)H, S, Sr);
+    k_ismv_init<T><<<grid1d(N), 256, 0, ctx->stream>>>(N, field, out_mask, p.tol, p.max_iter, fb[0], st, partials);
+    ls.done();
+  }
+  const int* done = &st->done;
+  const bool use_m = zm_tile_width<T>(d.nz, f.pz.T) > 0;
+  const T scale = (T)(1.0 / (double)N);
+  const int maxi = (int)std::min<size_t>(p.max_iter, (size_t)1 << 30);
+  // iteration k reads fb[(k-1) % 2] and writes fb[k % 2]
+  auto iter = [&](int k) {
+    const T* in = fb[(k - 1) % 2];
+    StoreIsmv<T> store{fb[k % 2], k == 1 ? nullptr : in, field, mask, out_mask, d.nx, scale, st, partials, maxi,
+                       {0.0}};
+    run_x_r2c<T>(ctx, f, spec, LoadVol<T>{in, d.nx}, done);
+    run_yz<T, -1, 1>(ctx, f, spec, spec, OpId<T>{}, done);
+    if (use_m) run_z_fused_m<T>(ctx, f, spec, spec, Sr, done);
+    else run_z_fused<T>(ctx, f, spec, spec, OpMulRe<T>{Sr}, done);
+    run_yz<T, +1, 1>(ctx, f, spec, spec, OpId<T>{}, done);
+    run_x_c2r<T>(ctx, f, spec, store, done);
+  };
+  IsmvState hs{};
+  size_t reported = 0;
+  auto poll = [&]() {
+    d2h(ctx, &hs, st, sizeof(hs));
+    sync(ctx);
+    const size_t through = hs.stop_at ? (size_t)hs.stop_at : (size_t)hs.k;
+    if (progress)
+      for (; reported < through; ++reported) progress(user, reported + 1, p.max_iter);
+    return hs.done != 0;
+  };
+  const bool watch = progress != nullptr || p.tol > 0.0;
+  bool stopped = false;
+  if (maxi >= 1) {
+    iter(1);
+    if (maxi >= 2) {
+      if (ctx->profiling) {
+        for (int k = 2; k <= maxi && !stopped; ++k) {
+          iter(k);
+          if (watch && k % 8 == 0) stopped = poll();
+        }
+      } else {
+        cudaGraph_t graph = nullptr;
+        const uint64_t l0 = ctx->launches;
+        QSM_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        try {
+          iter(2);
+          iter(3);
+        } catch (...) {
+          cudaStreamEndCapture(ctx->stream, &graph);
+          if (graph) cudaGraphDestroy(graph);
+          throw;
+        }
+        QSM_CUDA(cudaStreamEndCapture(ctx->stream, &graph));
+        const uint64_t per = ctx->launches - l0;
+        ctx->launches = l0;
+        cudaGraphExec_t exec = nullptr;
+        const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ie != cudaSuccess)
+          throw QsmError(QSM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+        try {
+          const int pairs = (maxi - 1) / 2;
+          for (int q = 0; q < pairs && !stopped; ++q) {
+            QSM_CUDA(cudaGraphLaunch(exec, ctx->stream));
+            ctx->launches += per;
+            if (watch && (q + 1) % 4 == 0) stopped = poll();
+          }
+          if (!stopped && (maxi - 1) % 2 == 1) iter(maxi);
+        } catch (...) {
+          cudaGraphExecDestroy(exec);
+          throw;
+        }
+        cudaGraphExecDestroy(exec);
+      }
+    }
+  }
+  poll();
+  const int kdone = hs.k;
+  {
+    LaunchScope ls(ctx, "ismv_out");
+    k_ismv_out<T><<<grid1d(N), 256, 0, ctx->stream>>>(N, field, mask, fb[kdone % 2], out_local);
+    ls.done();
+  }
+  sync(ctx);
+  if (progress) {
+    const size_t through = hs.stop_at ? (size_t)hs.stop_at : p.max_iter;
+    for (; reported < through; ++reported) progress(user, reported + 1, p.max_iter);
+    if (hs.stop_at) progress(user, (size_t)hs.stop_at, (size_t)hs.stop_at);
+  }
+}
+
 template <typename T>
 void unwrap_impl(qsm_ctx* ctx, const GridDims& d, const double* phase, const uint8_t* mask, double* out) {
   using C = cplx_t<T>;
@@ -337,6 +554,15 @@ void smv_device(qsm_ctx* ctx, const double* f, const uint8_t* m, const GridDims&
   check_finite(radius, "radius");
   if (ctx->precision == QSM_PRECISION_MIXED) smv_impl<float>(ctx, d, f, m, radius, ol, om);
   else smv_impl<double>(ctx, d, f, m, radius, ol, om);
+}
+
+void ismv_device(qsm_ctx* ctx, const double* f, const uint8_t* m, const GridDims& d, const qsm_ismv_params* p,
+                 qsm_progress_fn progress, void* user, double* ol, uint8_t* om) {
+  check_ptr(p, "params");
+  check_finite(p->radius, "radius");
+  if (std::isnan(p->tol)) throw QsmError(QSM_ERR_INVALID_ARGUMENT, "tol is NaN");
+  if (ctx->precision == QSM_PRECISION_MIXED) ismv_impl<float>(ctx, d, f, m, *p, progress, user, ol, om);
+  else ismv_impl<double>(ctx, d, f, m, *p, progress, user, ol, om);
 }
 
 void sharp_device(qsm_ctx* ctx, const double* f, const uint8_t* m, const GridDims& d, double thr, double radius,
@@ -504,12 +730,47 @@ qsm_status qsm_vsharp(qsm_ctx* ctx, const double* field, const uint8_t* mask, co
   });
 }
 
+void qsm_ismv_params_default(qsm_ismv_params* p) {
+  if (!p) return;
+  // IsmvParams::default, src/bgremove/ismv.rs:31-35
+  p->tol = 1e-6;
+  p->max_iter = 50;
+  p->radius = 5.0;
+}
+
+qsm_status qsm_ismv_device(qsm_ctx* ctx, const double* d_field, const uint8_t* d_mask, const qsm_grid* grid,
+                           const qsm_ismv_params* params, qsm_progress_fn progress, void* user, double* d_out_local,
+                           uint8_t* d_out_mask) {
+  return guarded(ctx, [&] {
+    GridDims d = check_grid(grid);
+    check_io(d_field, d_mask, d_out_local);
+    check_ptr(d_out_mask, "out_mask");
+    ismv_device(ctx, d_field, d_mask, d, params, progress, user, d_out_local, d_out_mask);
+    sync(ctx);
+  });
+}
+
+qsm_status qsm_ismv(qsm_ctx* ctx, const double* field, const uint8_t* mask, const qsm_grid* grid,
+                    const qsm_ismv_params* params, qsm_progress_fn progress, void* user, double* out_local,
+                    uint8_t* out_mask) {
+  return guarded(ctx, [&] {
+    GridDims d = check_grid(grid);
+    check_io(field, mask, out_local);
+    check_ptr(out_mask, "out_mask");
+    with_host_io2(ctx, d, field, mask, out_local, out_mask,
+                  [&](const double* f, const uint8_t* m, double* o, uint8_t* om) {
+                    ismv_device(ctx, f, m, d, params, progress, user, o, om);
+                  });
+  });
+}
+
 void qsm_bg_removal_config_default(qsm_bg_removal_config* c) {
   if (!c) return;
   c->algorithm = QSM_BG_VSHARP;
   qsm_vsharp_params_default(&c->vsharp);
   qsm_sharp_params_default(&c->sharp);
   qsm_resharp_params_default(&c->resharp);
+  qsm_ismv_params_default(&c->ismv);
 }
 
 qsm_status qsm_run_bg_removal(qsm_ctx* ctx, const double* field_ppm, size_t len, const uint8_t* mask,
@@ -540,6 +801,12 @@ qsm_status qsm_run_bg_removal(qsm_ctx* ctx, const double* field_ppm, size_t len,
         with_host_io2(ctx, d, field_ppm, mask, out_local, out_mask,
                       [&](const double* f, const uint8_t* m, double* o, uint8_t* om) {
                         resharp_device(ctx, f, m, d, &cfg->resharp, progress, user, o, om);
+                      });
+        break;
+      case QSM_BG_ISMV:
+        with_host_io2(ctx, d, field_ppm, mask, out_local, out_mask,
+                      [&](const double* f, const uint8_t* m, double* o, uint8_t* om) {
+                        ismv_device(ctx, f, m, d, &cfg->ismv, progress, user, o, om);
                       });
         break;
       case QSM_BG_SHARP:

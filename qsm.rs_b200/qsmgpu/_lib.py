@@ -61,6 +61,10 @@ class QsmResharpParams(C.Structure):
     _fields_ = [("radius", C.c_double), ("tik_reg", C.c_double), ("tol", C.c_double), ("max_iter", C.c_size_t)]
 
 
+class QsmIsmvParams(C.Structure):
+    _fields_ = [("tol", C.c_double), ("max_iter", C.c_size_t), ("radius", C.c_double)]
+
+
 class QsmRtsParams(C.Structure):
     _fields_ = [("delta", C.c_double), ("mu", C.c_double), ("rho", C.c_double), ("tol", C.c_double),
                 ("max_iter", C.c_size_t), ("lsmr_iter", C.c_size_t)]
@@ -99,7 +103,7 @@ class QsmInversionConfig(C.Structure):
 
 class QsmBgRemovalConfig(C.Structure):
     _fields_ = [("algorithm", C.c_int), ("vsharp", QsmVsharpParams), ("sharp", QsmSharpParams),
-                ("resharp", QsmResharpParams)]
+                ("resharp", QsmResharpParams), ("ismv", QsmIsmvParams)]
 
 
 # (name, restype, argtypes)
@@ -144,6 +148,11 @@ _SIGS = [
     ("qsm_run_tgv", C.c_int, [C.c_void_p, C.POINTER(c_double_p), C.c_size_t, C.c_size_t, c_u8_p,
                               C.POINTER(QsmScanMetadata), C.POINTER(QsmTgvParams), C.c_int, PROGRESS_FN,
                               C.c_void_p, c_double_p]),
+    ("qsm_ismv_params_default", None, [C.POINTER(QsmIsmvParams)]),
+    ("qsm_ismv", C.c_int, [C.c_void_p, c_double_p, c_u8_p, C.POINTER(QsmGrid), C.POINTER(QsmIsmvParams),
+                           PROGRESS_FN, C.c_void_p, c_double_p, c_u8_p]),
+    ("qsm_ismv_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(QsmGrid), C.POINTER(QsmIsmvParams),
+                                  PROGRESS_FN, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("qsm_resharp_params_default", None, [C.POINTER(QsmResharpParams)]),
     ("qsm_resharp", C.c_int, [C.c_void_p, c_double_p, c_u8_p, C.POINTER(QsmGrid), C.POINTER(QsmResharpParams),
                               PROGRESS_FN, C.c_void_p, c_double_p, c_u8_p]),

@@ -36,6 +36,18 @@ class ResharpParams:
 
 
 @dataclass
+class IsmvParams:
+    """src/bgremove/ismv.rs:19-35."""
+
+    tol: float = 1e-6
+    max_iter: int = 50
+    radius: float = 5.0
+
+    def _c(self):
+        return _lib.QsmIsmvParams(self.tol, int(self.max_iter), self.radius)
+
+
+@dataclass
 class VsharpParams:
     """src/bgremove/vsharp.rs:22-40."""
 
@@ -110,6 +122,19 @@ def resharp(field, mask, grid: Grid, params: ResharpParams = ResharpParams(),
     cb, _keep = _progress(progress)
     _check(c, c._lib.qsm_resharp(c.handle, _ptr_d(f), _ptr_u8(m), C.byref(g), C.byref(p), cb, None, _ptr_d(out),
                                  _ptr_u8(om)))
+    return out, om
+
+
+def ismv(field, mask, grid: Grid, params: IsmvParams = IsmvParams(),
+         progress: Optional[Callable[[int, int], None]] = None, *, ctx: Optional[Context] = None):
+    """bgremove::ismv (src/bgremove/ismv.rs:48-166) -> (local_field, eroded_mask)."""
+    c = _ctx(ctx)
+    f, m, out, om = _io(field, mask, grid)
+    g = grid._c()
+    p = params._c()
+    cb, _keep = _progress(progress)
+    _check(c, c._lib.qsm_ismv(c.handle, _ptr_d(f), _ptr_u8(m), C.byref(g), C.byref(p), cb, None, _ptr_d(out),
+                              _ptr_u8(om)))
     return out, om
 
 

@@ -10,7 +10,7 @@ import numpy as np
 from . import _lib
 from . import Context, _ctx, _check, _ptr_d, _ptr_u8, _progress
 from .inversion import IlsqrParams, NltvParams, RtsParams, TkdParams, TikhonovParams, TvParams
-from .bgremove import ResharpParams, SharpParams, VsharpParams
+from .bgremove import IsmvParams, ResharpParams, SharpParams, VsharpParams
 
 # InversionAlgorithm, src/pipeline/config.rs:47-58
 TKD, TSVD, TIKHONOV, TV, RTS, NLTV, MEDI, ILSQR, TGV, QSMART = range(10)
@@ -60,9 +60,11 @@ class BgRemovalConfig:
     vsharp: VsharpParams = field(default_factory=VsharpParams)
     sharp: SharpParams = field(default_factory=SharpParams)
     resharp: ResharpParams = field(default_factory=ResharpParams)
+    ismv: IsmvParams = field(default_factory=IsmvParams)
 
     def _c(self):
-        return _lib.QsmBgRemovalConfig(self.algorithm, self.vsharp._c(), self.sharp._c(), self.resharp._c())
+        return _lib.QsmBgRemovalConfig(self.algorithm, self.vsharp._c(), self.sharp._c(), self.resharp._c(),
+                                       self.ismv._c())
 
 
 @dataclass

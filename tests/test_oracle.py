@@ -531,3 +531,46 @@ def test_nltv_progress_contract():
     _, k = O.nltv(f, np.ones(grid.shape, np.uint8), grid, (0, 0, 1), O.NltvParams(1e-3, 1.0, 5e-2, 20, 3),
                   lambda a, b: calls.append((a, b)), return_iters=True)
     assert calls == [(i + 1, 60) for i in range(k)] and k < 60
+
+
+def _ball_mask(n, radius):
+    c = n // 2
+    k, j, i = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    return (((i - c) ** 2 + (j - c) ** 2 + (k - c) ** 2) <= radius * radius).astype(np.uint8)
+
+
+def test_ismv_reference_tests():
+    """src/bgremove/ismv.rs:163-420: zero field; finite; interior kept; larger radius
+    erodes more; linear background on a 16^3 sphere."""
+    grid = g(8)
+    ones = np.ones(grid.shape, np.uint8)
+    local, er = O.ismv(np.zeros(grid.shape), ones, grid, O.IsmvParams(1e-3, 10, 2.0))
+    assert np.abs(local).max() < 1e-10 and er.sum() > 0
+    ramp = (np.arange(512) * 0.001).reshape(grid.shape)
+    assert np.all(np.isfinite(O.ismv(ramp, ones, grid, O.IsmvParams(1e-3, 20, 2.0))[0]))
+    g16 = g(16)
+    sph = _ball_mask(16, 16 // 3)
+    _, er = O.ismv(np.full(g16.shape, 0.1), sph, g16, O.IsmvParams(1e-3, 50, 1.5))
+    assert 0 < er.sum() <= sph.sum()
+    _, es = O.ismv(ramp, ones, grid, O.IsmvParams(1e-3, 20, 1.5))
+    _, el = O.ismv(ramp, ones, grid, O.IsmvParams(1e-3, 20, 3.0))
+    assert el.sum() <= es.sum()
+    z = np.arange(16)[:, None, None] * 0.1 * np.ones(g16.shape)
+    local, er = O.ismv(z, sph, g16, O.IsmvParams(1e-3, 50, 2.0))
+    assert local.shape == g16.shape and np.all(np.isfinite(local))
+    assert np.all(local[sph == 0] == 0.0)
+
+
+def test_ismv_progress_contract():
+    """(iter+1, max) per iteration; (iter+1, iter+1) when the change falls below tol."""
+    grid = g(8)
+    calls = []
+    O.ismv(np.zeros(grid.shape), np.ones(grid.shape, np.uint8), grid, O.IsmvParams(1e-3, 10, 2.0),
+           lambda a, b: calls.append((a, b)))
+    assert calls == [(1, 10), (1, 1)]
+    g16 = g(16)
+    f = np.sin(np.arange(16 ** 3) * 0.01).reshape(g16.shape)
+    calls = []
+    _, _, it = O.ismv(f, _ball_mask(16, 6), g16, O.IsmvParams(1e-2, 200, 2.0), lambda a, b: calls.append((a, b)),
+                      return_iters=True)
+    assert it < 200 and calls == [(i + 1, 200) for i in range(it + 1)] + [(it + 1, it + 1)]
