@@ -405,6 +405,46 @@ QSM_API qsm_status qsm_run_bg_removal(qsm_ctx* ctx, const double* field_ppm, siz
 QSM_API qsm_status qsm_prctile_device(qsm_ctx* ctx, const double* d_vals, const uint8_t* d_mask, size_t n,
                                       const double* p, size_t np, double* out);
 
+/* ------------------------------------------------- multi-echo field mapping -- */
+/* B0WeightType — src/utils/multi_echo.rs:78-91, same variant order. */
+typedef enum {
+  QSM_B0W_PHASE_SNR = 0,
+  QSM_B0W_PHASE_VAR = 1,
+  QSM_B0W_AVERAGE = 2,
+  QSM_B0W_TES = 3,
+  QSM_B0W_MAG = 4
+} qsm_b0_weight_type;
+
+/* LinearFitParams — src/utils/multi_echo.rs:33-48 (estimate_offset true, percentile 90). */
+typedef struct {
+  int estimate_offset;
+  double reliability_threshold_percentile;
+} qsm_linear_fit_params;
+QSM_API void qsm_linear_fit_params_default(qsm_linear_fit_params* p);
+
+/* utils::multi_echo::calculate_b0_weighted — src/utils/multi_echo.rs:450-506.  phases and
+ * mags hold n_echoes volumes of n values each, echo-major (echo e at e*n); tes holds the
+ * n_echoes echo times in seconds (host memory, at most 64).  Output: B0 in Hz. */
+QSM_API qsm_status qsm_calculate_b0_weighted(qsm_ctx* ctx, const double* phases, const double* mags,
+                                             const double* tes, size_t n_echoes, const uint8_t* mask, size_t n,
+                                             int weight_type, double* out_b0_hz);
+QSM_API qsm_status qsm_calculate_b0_weighted_device(qsm_ctx* ctx, const double* d_phases, const double* d_mags,
+                                                    const double* tes, size_t n_echoes, const uint8_t* d_mask,
+                                                    size_t n, int weight_type, double* d_out_b0_hz);
+/* utils::multi_echo::multi_echo_linear_fit — src/utils/multi_echo.rs:631-768 (layout as
+ * above): LinearFitResult's field (rad/s), phase_offset, fit_residual and
+ * reliability_mask. */
+QSM_API qsm_status qsm_multi_echo_linear_fit(qsm_ctx* ctx, const double* phases, const double* mags,
+                                             const double* tes, size_t n_echoes, const uint8_t* mask, size_t n,
+                                             const qsm_linear_fit_params* params, double* out_field,
+                                             double* out_phase_offset, double* out_fit_residual,
+                                             uint8_t* out_reliability);
+QSM_API qsm_status qsm_multi_echo_linear_fit_device(qsm_ctx* ctx, const double* d_phases, const double* d_mags,
+                                                    const double* tes, size_t n_echoes, const uint8_t* d_mask,
+                                                    size_t n, const qsm_linear_fit_params* params,
+                                                    double* d_out_field, double* d_out_phase_offset,
+                                                    double* d_out_fit_residual, uint8_t* d_out_reliability);
+
 /* QsmReference — src/pipeline/config.rs:69-72. */
 typedef enum { QSM_REFERENCE_MEAN = 0, QSM_REFERENCE_NONE = 1 } qsm_reference;
 

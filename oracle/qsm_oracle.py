@@ -1557,3 +1557,116 @@ def ismv(field_, mask, grid: Grid, params: IsmvParams = IsmvParams(), progress=N
     local = np.where(m != 0, fld - f, 0.0)
     out = (local, (eroded > 0.5).astype(np.uint8))
     return out + (done,) if return_iters else out
+
+
+# ---------------------------------------------------------------------------
+# Multi-echo field mapping (src/utils/multi_echo.rs)
+# ---------------------------------------------------------------------------
+B0W_PHASE_SNR, B0W_PHASE_VAR, B0W_AVERAGE, B0W_TES, B0W_MAG = range(5)  # B0WeightType, multi_echo.rs:78-91
+
+
+def calculate_b0_weighted(phases, mags, tes, mask, weight_type=B0W_PHASE_SNR):
+    """B0 in Hz = (1/2pi) sum_e (phase_e/TE_e) w_e / sum_e w_e over mask != 0, 0 where
+    sum w <= 1e-10 (src/utils/multi_echo.rs:450-506).  Echo loop in the reference's
+    order, so the float64 result is the reference's bit for bit."""
+    phases = [np.asarray(p, np.float64).ravel() for p in phases]
+    mags = [np.asarray(m, np.float64).ravel() for m in mags]
+    m = np.asarray(mask).ravel()
+    ws_ = np.zeros_like(phases[0])
+    w_sum = np.zeros_like(phases[0])
+    for e, te in enumerate(tes):
+        mag = mags[e]
+        if weight_type == B0W_PHASE_SNR:
+            w = mag * te
+        elif weight_type == B0W_PHASE_VAR:
+            w = mag * mag * te * te
+        elif weight_type == B0W_AVERAGE:
+            w = np.ones_like(mag)
+        elif weight_type == B0W_TES:
+            w = np.full_like(mag, te)
+        else:
+            w = mag
+        ws_ = ws_ + (phases[e] / te) * w
+        w_sum = w_sum + w
+    scale = 1.0 / (2.0 * math.pi)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        b0 = scale * ws_ / w_sum
+    return np.where((m != 0) & (w_sum > 1e-10), b0, 0.0)
+
+
+def compute_reliability_mask(fit_residual, mask, threshold_percentile):
+    """src/utils/multi_echo.rs:771-804: threshold = the floor(p/100 * count)-th smallest
+    (clamped) of the residuals with mask > 0, r > 0 and finite; reliable where
+    mask > 0 and r < threshold; the mask itself when no residual qualifies."""
+    r = np.asarray(fit_residual, np.float64).ravel()
+    m = np.asarray(mask).ravel()
+    sel = (m > 0) & (r > 0.0) & np.isfinite(r)
+    vals = np.sort(r[sel])
+    if vals.size == 0:
+        return m.astype(np.uint8).copy()
+    idx = int((threshold_percentile / 100.0) * vals.size)
+    thr = vals[min(idx, vals.size - 1)]
+    return ((m > 0) & (r < thr)).astype(np.uint8)
+
+
+def multi_echo_linear_fit(phases, mags, tes, mask, estimate_offset=True, reliability_threshold_percentile=90.0):
+    """Magnitude-weighted linear fit phase = offset + slope * TE per voxel
+    (src/utils/multi_echo.rs:631-768): (field rad/s, phase_offset, fit_residual,
+    reliability_mask).  Echo sums in the reference's order (float64 bit for bit)."""
+    phases = [np.asarray(p, np.float64).ravel() for p in phases]
+    mags = [np.asarray(w, np.float64).ravel() for w in mags]
+    m = np.asarray(mask).ravel()
+    n_e = len(phases)
+    zero = np.zeros_like(phases[0])
+    field, offset, resid = zero.copy(), zero.copy(), zero.copy()
+    on = m != 0
+    with np.errstate(divide="ignore", invalid="ignore"):
+        if estimate_offset:
+            sw, swt, swp = zero.copy(), zero.copy(), zero.copy()
+            for e in range(n_e):
+                w = mags[e]
+                sw = sw + w
+                swt = swt + w * tes[e]
+                swp = swp + w * phases[e]
+            ok = on & ~(sw < 1e-10)
+            te_mean = swt / sw
+            ph_mean = swp / sw
+            sxx, sxy = zero.copy(), zero.copy()
+            for e in range(n_e):
+                w = mags[e]
+                tc = tes[e] - te_mean
+                pc = phases[e] - ph_mean
+                sxx = sxx + w * tc * tc
+                sxy = sxy + w * tc * pc
+            ok = ok & (sxx > 1e-10)
+            slope = sxy / sxx
+            icpt = ph_mean - slope * te_mean
+            srr = zero.copy()
+            for e in range(n_e):
+                w = mags[e]
+                d = phases[e] - (icpt + slope * tes[e])
+                srr = srr + w * d * d
+            field = np.where(ok, slope, 0.0)
+            offset = np.where(ok, icpt, 0.0)
+            resid = np.where(ok, srr / sw * n_e, 0.0)
+        else:
+            stp, stt, sw = zero.copy(), zero.copy(), zero.copy()
+            for e in range(n_e):
+                w = mags[e]
+                stp = stp + w * tes[e] * phases[e]
+                stt = stt + w * tes[e] * tes[e]
+                sw = sw + w
+            ok = on & (stt > 1e-10)
+            slope = stp / stt
+            srr = zero.copy()
+            for e in range(n_e):
+                w = mags[e]
+                d = phases[e] - slope * tes[e]
+                srr = srr + w * d * d
+            field = np.where(ok, slope, 0.0)
+            resid = np.where(ok & (sw > 1e-10), srr / sw * n_e, 0.0)
+    if reliability_threshold_percentile > 0.0:
+        rel_mask = compute_reliability_mask(resid, m, reliability_threshold_percentile)
+    else:
+        rel_mask = m.astype(np.uint8).copy()
+    return field, offset, resid, rel_mask

@@ -75,6 +75,10 @@ class QsmNltvParams(C.Structure):
                 ("newton_iter", C.c_size_t)]
 
 
+class QsmLinearFitParams(C.Structure):
+    _fields_ = [("estimate_offset", C.c_int), ("reliability_threshold_percentile", C.c_double)]
+
+
 class QsmIlsqrParams(C.Structure):
     _fields_ = [("tol", C.c_double), ("max_iter", C.c_size_t)]
 
@@ -221,6 +225,17 @@ _SIGS = [
                                      C.POINTER(QsmBgRemovalConfig), PROGRESS_FN, C.c_void_p, c_double_p,
                                      c_u8_p]),
     ("qsm_fft3d_real", C.c_int, [C.c_void_p, c_double_p, C.POINTER(QsmGrid), c_double_p]),
+    ("qsm_linear_fit_params_default", None, [C.POINTER(QsmLinearFitParams)]),
+    ("qsm_calculate_b0_weighted", C.c_int, [C.c_void_p, c_double_p, c_double_p, c_double_p, C.c_size_t, c_u8_p,
+                                            C.c_size_t, C.c_int, c_double_p]),
+    ("qsm_calculate_b0_weighted_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, c_double_p, C.c_size_t,
+                                                   C.c_void_p, C.c_size_t, C.c_int, C.c_void_p]),
+    ("qsm_multi_echo_linear_fit", C.c_int, [C.c_void_p, c_double_p, c_double_p, c_double_p, C.c_size_t, c_u8_p,
+                                            C.c_size_t, C.POINTER(QsmLinearFitParams), c_double_p, c_double_p,
+                                            c_double_p, c_u8_p]),
+    ("qsm_multi_echo_linear_fit_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, c_double_p, C.c_size_t,
+                                                   C.c_void_p, C.c_size_t, C.POINTER(QsmLinearFitParams),
+                                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
 ]
 
 EXPORTED_SYMBOLS = [s[0] for s in _SIGS]

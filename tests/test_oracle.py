@@ -574,3 +574,53 @@ def test_ismv_progress_contract():
     _, _, it = O.ismv(f, _ball_mask(16, 6), g16, O.IsmvParams(1e-2, 200, 2.0), lambda a, b: calls.append((a, b)),
                       return_iters=True)
     assert it < 200 and calls == [(i + 1, 200) for i in range(it + 1)] + [(it + 1, it + 1)]
+
+
+def test_calculate_b0_weighted_reference_tests():
+    """src/utils/multi_echo.rs:1153-1263."""
+    tes = [0.005, 0.010, 0.015]
+    ph = [np.full(64, 200.0 * te) for te in tes]
+    b0 = O.calculate_b0_weighted(ph, [np.ones(64)] * 3, tes, np.ones(64, np.uint8), O.B0W_PHASE_SNR)
+    assert np.all(np.abs(b0 - 200.0 / (2 * math.pi)) < 1e-8)
+    ph = [np.full(16, 100.0 * te) for te in tes]
+    for wt in range(5):
+        b0 = O.calculate_b0_weighted(ph, [np.full(16, 2.0)] * 3, tes, np.ones(16, np.uint8), wt)
+        assert np.all(np.abs(b0 - 100.0 / (2 * math.pi)) < 1e-8)
+    b0 = O.calculate_b0_weighted([np.full(8, 500 * te) for te in tes[:2]], [np.ones(8)] * 2, tes[:2],
+                                 np.zeros(8, np.uint8))
+    assert np.all(b0 == 0.0)
+    ph = [np.full(4, 0.2 * te) for te in tes]
+    assert np.all(O.calculate_b0_weighted(ph, [np.zeros(4)] * 3, tes, np.ones(4, np.uint8)) == 0.0)
+    b0 = O.calculate_b0_weighted(ph, [np.zeros(4)] * 3, tes, np.ones(4, np.uint8), O.B0W_AVERAGE)
+    assert np.all(np.abs(b0 - 0.2 / (2 * math.pi)) < 1e-8)
+
+
+def test_multi_echo_linear_fit_reference_tests():
+    """src/utils/multi_echo.rs:1267-1491."""
+    tes = [0.005, 0.010, 0.015]
+    f, o, r, rm = O.multi_echo_linear_fit([np.full(32, 100.0 * te) for te in tes], [np.ones(32)] * 3, tes,
+                                          np.ones(32, np.uint8), False, 0.0)
+    assert np.all(np.abs(f - 100.0) < 1e-6) and np.all(o == 0.0) and np.all(r < 1e-10) and np.all(rm == 1)
+    tes4 = [0.005, 0.010, 0.015, 0.020]
+    f, o, r, _ = O.multi_echo_linear_fit([np.full(16, 0.5 + 200.0 * te) for te in tes4], [np.ones(16)] * 4, tes4,
+                                         np.ones(16, np.uint8), True, 0.0)
+    assert np.all(np.abs(f - 200.0) < 1e-4) and np.all(np.abs(o - 0.5) < 1e-4) and np.all(r < 1e-8)
+    f, o, r, _ = O.multi_echo_linear_fit([np.full(8, 100.0 * te) for te in tes], [np.ones(8)] * 3, tes,
+                                         np.zeros(8, np.uint8), True, 0.0)
+    assert np.all(f == 0) and np.all(o == 0) and np.all(r == 0)
+    slopes = 50.0 * (np.arange(8) + 1.0)
+    f, _, _, _ = O.multi_echo_linear_fit([slopes * te for te in tes], [np.ones(8)] * 3, tes, np.ones(8, np.uint8),
+                                         False, 0.0)
+    assert np.all(np.abs(f - slopes) < 1e-6)
+    ph = [np.full(100, 100.0 * te) for te in tes]
+    for e in range(3):
+        ph[e][90:] += 2.0 if e % 2 == 0 else -2.0
+    _, _, r, rm = O.multi_echo_linear_fit(ph, [np.ones(100)] * 3, tes, np.ones(100, np.uint8), False, 80.0)
+    assert r[:90].max() < r[90:].min() and set(np.unique(rm)) <= {0, 1}
+    for off in (False, True):
+        f, _, _, _ = O.multi_echo_linear_fit([np.full(4, 100.0 * te) for te in tes], [np.zeros(4)] * 3, tes,
+                                             np.ones(4, np.uint8), off, 0.0)
+        assert np.all(np.isfinite(f))
+    rm = O.compute_reliability_mask(np.arange(1, 11) * 0.1, np.ones(10, np.uint8), 50.0)
+    assert 0 < rm.sum() < 10
+    assert np.array_equal(O.compute_reliability_mask(np.zeros(5), np.ones(5, np.uint8), 50.0), np.ones(5))
