@@ -40,7 +40,8 @@ typedef enum {
   QSM_ERR_ALLOC = 4,
   QSM_ERR_CUDA = 5,
   QSM_ERR_INVALID_CONFIG = 6, /* PipelineError::InvalidConfig */
-  QSM_ERR_NO_DEVICE = 7
+  QSM_ERR_NO_DEVICE = 7,
+  QSM_ERR_IO = 8 /* file access, malformed or unsupported NIfTI data */
 } qsm_status;
 
 /* Arithmetic used by a context.  QSM_PRECISION_F64 runs every FFT, stencil and
@@ -444,6 +445,71 @@ QSM_API qsm_status qsm_multi_echo_linear_fit_device(qsm_ctx* ctx, const double* 
                                                     size_t n, const qsm_linear_fit_params* params,
                                                     double* d_out_field, double* d_out_phase_offset,
                                                     double* d_out_fit_residual, uint8_t* d_out_reliability);
+
+/* --------------------------------------------------------------- NIfTI I/O -- */
+/* io.rs:62-460.  Single-file NIfTI-1 (.nii, and .nii.gz detected by its gzip magic),
+ * either byte order.  The host functions need no context or GPU; they report errors
+ * through `err` (err_cap bytes, may be NULL). */
+typedef enum {
+  QSM_NIFTI_UINT8 = 2,
+  QSM_NIFTI_INT16 = 4,
+  QSM_NIFTI_INT32 = 8,
+  QSM_NIFTI_FLOAT32 = 16,
+  QSM_NIFTI_FLOAT64 = 64,
+  QSM_NIFTI_INT8 = 256,
+  QSM_NIFTI_UINT16 = 512,
+  QSM_NIFTI_UINT32 = 768,
+  QSM_NIFTI_INT64 = 1024,
+  QSM_NIFTI_UINT64 = 1280
+} qsm_nifti_datatype;
+
+/* NiftiData's metadata (io.rs:13-27) and what decoding needs. */
+typedef struct {
+  size_t nx, ny, nz, nt;  /* dim[1..4]; nt = 1 for 3D */
+  double voxel_size[3];   /* pixdim[1..3] */
+  double affine[16];      /* row-major: sform rows when sform_code > 0, else diag(pixdim) (io.rs:226-253) */
+  double scl_slope;       /* 1 when the file stores 0 (io.rs:96) */
+  double scl_inter;
+  double raw_slope;       /* scl_slope as stored: voxels are raw * slope + inter unless it is 0 */
+  int datatype;           /* qsm_nifti_datatype of the stored voxels */
+  int ndim;               /* dim[0] */
+  int big_endian;
+  int gzip;
+  size_t vox_offset;      /* byte offset of the voxels in the uncompressed image */
+} qsm_nifti_header;
+
+QSM_API qsm_status qsm_nifti_parse_header(const uint8_t* bytes, size_t len, qsm_nifti_header* out, char* err,
+                                          size_t err_cap);
+/* io::load_nifti (all_volumes = 0: nx*ny*nz values, the first volume of 4D data) and
+ * io::load_nifti_4d (all_volumes = 1: nx*ny*nz*nt values); x fastest.  out_len must be
+ * that count (QSM_ERR_DIMENSION_MISMATCH otherwise).  hdr may be NULL. */
+QSM_API qsm_status qsm_nifti_load(const uint8_t* bytes, size_t len, int all_volumes, double* out, size_t out_len,
+                                  qsm_nifti_header* hdr, char* err, size_t err_cap);
+/* io::save_nifti / io::save_nifti_gz (gzip = 1): float32 voxels after a 352-byte
+ * header.  out == NULL: *out_len = the size (uncompressed), or an upper bound (gzip). */
+QSM_API qsm_status qsm_nifti_save(const double* data, size_t nx, size_t ny, size_t nz, const double voxel_size[3],
+                                  const double affine[16], int gzip, uint8_t* out, size_t out_cap, size_t* out_len,
+                                  char* err, size_t err_cap);
+/* io::read_nifti_dims (io.rs:366-421). */
+QSM_API qsm_status qsm_nifti_read_dims(const char* path, size_t dims[3], char* err, size_t err_cap);
+QSM_API qsm_status qsm_nifti_read_file_header(const char* path, qsm_nifti_header* out, char* err, size_t err_cap);
+/* io::read_nifti_file (io.rs:424-431), with the all_volumes choice of qsm_nifti_load. */
+QSM_API qsm_status qsm_nifti_read_file(const char* path, int all_volumes, double* out, size_t out_len,
+                                       qsm_nifti_header* hdr, char* err, size_t err_cap);
+/* io::save_nifti_to_file (io.rs:434-452): gzip when the path ends in .nii.gz. */
+QSM_API qsm_status qsm_nifti_save_file(const char* path, const double* data, size_t nx, size_t ny, size_t nz,
+                                       const double voxel_size[3], const double affine[16], char* err,
+                                       size_t err_cap);
+/* qsm_nifti_load into device memory (no counterpart in the reference): the stored voxels
+ * cross to the GPU in their own type through pinned staging buffers and are decoded
+ * and scaled there. */
+QSM_API qsm_status qsm_nifti_load_device(qsm_ctx* ctx, const uint8_t* bytes, size_t len, int all_volumes,
+                                         double* d_out, size_t out_len, qsm_nifti_header* hdr);
+/* qsm_nifti_save from device memory (no counterpart in the reference): float32
+ * conversion on the GPU, 4 bytes per voxel back to the host through pinned staging. */
+QSM_API qsm_status qsm_nifti_save_device(qsm_ctx* ctx, const double* d_data, size_t nx, size_t ny, size_t nz,
+                                         const double voxel_size[3], const double affine[16], int gzip, uint8_t* out,
+                                         size_t out_cap, size_t* out_len);
 
 /* QsmReference — src/pipeline/config.rs:69-72. */
 typedef enum { QSM_REFERENCE_MEAN = 0, QSM_REFERENCE_NONE = 1 } qsm_reference;

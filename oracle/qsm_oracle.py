@@ -1670,3 +1670,84 @@ def multi_echo_linear_fit(phases, mags, tes, mask, estimate_offset=True, reliabi
     else:
         rel_mask = m.astype(np.uint8).copy()
     return field, offset, resid, rel_mask
+
+
+# ---------------------------------------------------------------------------
+# NIfTI-1 (src/io.rs; decoding restated from the `nifti` crate 0.17.0 the reference calls)
+# ---------------------------------------------------------------------------
+NIFTI_DTYPES = {2: "u1", 4: "i2", 8: "i4", 16: "f4", 64: "f8", 256: "i1", 512: "u2", 768: "u4", 1024: "i8",
+                1280: "u8"}
+
+
+def nifti_save_bytes(data, dims, voxel_size, affine) -> bytes:
+    """save_nifti (src/io.rs:255-338): 348-byte header + 4 zero bytes + float32 LE voxels."""
+    import struct
+    nx, ny, nz = dims
+    h = bytearray(348)
+    struct.pack_into("<i", h, 0, 348)
+    struct.pack_into("<8h", h, 40, 3, nx, ny, nz, 1, 1, 1, 1)
+    struct.pack_into("<hh", h, 70, 16, 32)
+    struct.pack_into("<8f", h, 76, 1.0, voxel_size[0], voxel_size[1], voxel_size[2], 1.0, 1.0, 1.0, 1.0)
+    struct.pack_into("<fff", h, 108, 352.0, 1.0, 0.0)
+    struct.pack_into("<h", h, 254, 1)
+    struct.pack_into("<12f", h, 280, *[float(a) for a in list(affine)[:12]])
+    h[344:348] = b"n+1\0"
+    return bytes(h) + b"\0\0\0\0" + np.asarray(data, np.float64).astype("<f4").tobytes()
+
+
+def nifti_load(raw: bytes, all_volumes=False):
+    """load_nifti / load_nifti_4d (src/io.rs:62-224): header fields either byte order,
+    voxels from vox_offset cast to float64 and, when scl_slope != 0, raw * slope + inter;
+    x fastest; first volume unless all_volumes.  Returns a dict."""
+    import gzip as _gz
+    import struct
+    if len(raw) >= 2 and raw[0] == 0x1F and raw[1] == 0x8B:
+        raw = _gz.decompress(raw)
+    if len(raw) < 348:
+        raise ValueError("header too short")
+    e = "<" if struct.unpack_from("<i", raw, 0)[0] == 348 else ">"
+    if struct.unpack_from(e + "i", raw, 0)[0] != 348 or raw[344:348] != b"n+1\0":
+        raise ValueError("not a NIfTI-1 single file")
+    dim = struct.unpack_from(e + "8h", raw, 40)
+    if dim[0] < 3:
+        raise ValueError("Expected at least 3D volume")
+    dt = struct.unpack_from(e + "h", raw, 70)[0]
+    pix = struct.unpack_from(e + "8f", raw, 76)
+    vo = int(struct.unpack_from(e + "f", raw, 108)[0])
+    vo = 352 if vo < 348 else vo
+    slope, inter = struct.unpack_from(e + "ff", raw, 112)
+    sform = struct.unpack_from(e + "h", raw, 254)[0]
+    nx, ny, nz = dim[1], dim[2], dim[3]
+    nt = dim[4] if dim[0] >= 4 else 1
+    count = nx * ny * nz * (nt if all_volumes else 1)
+    vals = np.frombuffer(raw, np.dtype(NIFTI_DTYPES[dt]).newbyteorder(e), count, vo).astype(np.float64)
+    if slope != 0.0:
+        vals = vals * np.float64(slope) + np.float64(inter)
+    if sform > 0:
+        aff = list(np.float64(v) for v in struct.unpack_from(e + "12f", raw, 280)) + [0.0, 0.0, 0.0, 1.0]
+    else:
+        aff = [pix[1], 0, 0, 0, 0, pix[2], 0, 0, 0, 0, pix[3], 0, 0, 0, 0, 1.0]
+    return {"data": vals, "dims": (nx, ny, nz, nt), "voxel_size": (float(pix[1]), float(pix[2]), float(pix[3])),
+            "affine": np.array(aff, np.float64), "scl_slope": 1.0 if slope == 0.0 else float(slope),
+            "scl_inter": float(inter), "datatype": dt}
+
+
+def nifti_craft(data, dims4, datatype, big_endian=False, slope=0.0, inter=0.0, voxel_size=(1.0, 1.0, 1.0),
+                sform=None, ndim=None) -> bytes:
+    """A NIfTI-1 single-file image with any stored datatype and byte order (test input)."""
+    import struct
+    e = ">" if big_endian else "<"
+    nx, ny, nz, nt = dims4
+    nd = ndim if ndim is not None else (4 if nt > 1 else 3)
+    h = bytearray(348)
+    struct.pack_into(e + "i", h, 0, 348)
+    struct.pack_into(e + "8h", h, 40, nd, nx, ny, nz, nt, 1, 1, 1)
+    struct.pack_into(e + "hh", h, 70, datatype, 8 * np.dtype(NIFTI_DTYPES[datatype]).itemsize)
+    struct.pack_into(e + "8f", h, 76, 1.0, *voxel_size, 1.0, 1.0, 1.0, 1.0)
+    struct.pack_into(e + "fff", h, 108, 352.0, slope, inter)
+    if sform is not None:
+        struct.pack_into(e + "h", h, 254, 1)
+        struct.pack_into(e + "12f", h, 280, *sform)
+    h[344:348] = b"n+1\0"
+    vals = np.asarray(data).astype(np.dtype(NIFTI_DTYPES[datatype]).newbyteorder(e))
+    return bytes(h) + b"\0\0\0\0" + vals.tobytes()

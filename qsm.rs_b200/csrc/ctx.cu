@@ -134,6 +134,60 @@ void d2h(qsm_ctx* ctx, void* dst, const void* src, size_t bytes) {
 }
 void sync(qsm_ctx* ctx) { QSM_CUDA(cudaStreamSynchronize(ctx->stream)); }
 
+namespace {
+void ensure_pinned(qsm_ctx* ctx) {
+  for (int k = 0; k < 2; ++k) {
+    if (!ctx->pinned[k]) {
+      if (cudaHostAlloc(&ctx->pinned[k], kStageBytes, cudaHostAllocDefault) != cudaSuccess) {
+        (void)cudaGetLastError();
+        ctx->pinned[k] = nullptr;
+        throw QsmError(QSM_ERR_ALLOC, "pinned staging allocation failed");
+      }
+    }
+    if (!ctx->pinned_ev[k]) QSM_CUDA(cudaEventCreateWithFlags(&ctx->pinned_ev[k], cudaEventDisableTiming));
+  }
+}
+}  // namespace
+
+void staged_h2d(qsm_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  ensure_pinned(ctx);
+  const uint8_t* s = static_cast<const uint8_t*>(src);
+  uint8_t* d = static_cast<uint8_t*>(dst);
+  bool used[2] = {false, false};
+  for (size_t off = 0, c = 0; off < bytes; off += kStageBytes, ++c) {
+    const int k = (int)(c % 2);
+    const size_t n = std::min(kStageBytes, bytes - off);
+    if (used[k]) QSM_CUDA(cudaEventSynchronize(ctx->pinned_ev[k]));  // this slot's previous DMA is done
+    std::memcpy(ctx->pinned[k], s + off, n);
+    QSM_CUDA(cudaMemcpyAsync(d + off, ctx->pinned[k], n, cudaMemcpyHostToDevice, ctx->stream));
+    QSM_CUDA(cudaEventRecord(ctx->pinned_ev[k], ctx->stream));
+    used[k] = true;
+  }
+  sync(ctx);
+}
+
+void staged_d2h(qsm_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  ensure_pinned(ctx);
+  const uint8_t* s = static_cast<const uint8_t*>(src);
+  uint8_t* d = static_cast<uint8_t*>(dst);
+  const size_t nchunks = (bytes + kStageBytes - 1) / kStageBytes;
+  auto issue = [&](size_t c) {
+    const int k = (int)(c % 2);
+    const size_t off = c * kStageBytes;
+    QSM_CUDA(cudaMemcpyAsync(ctx->pinned[k], s + off, std::min(kStageBytes, bytes - off), cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    QSM_CUDA(cudaEventRecord(ctx->pinned_ev[k], ctx->stream));
+  };
+  if (nchunks > 0) issue(0);
+  for (size_t c = 0; c < nchunks; ++c) {
+    if (c + 1 < nchunks) issue(c + 1);  // the other slot was drained in the previous step
+    const int k = (int)(c % 2);
+    QSM_CUDA(cudaEventSynchronize(ctx->pinned_ev[k]));
+    const size_t off = c * kStageBytes;
+    std::memcpy(d + off, ctx->pinned[k], std::min(kStageBytes, bytes - off));
+  }
+}
+
 void LaunchScope::done() {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) throw QsmError(QSM_ERR_CUDA, std::string("kernel launch (") + name + "): " + cudaGetErrorString(e));
@@ -204,6 +258,10 @@ qsm_status qsm_ctx_destroy(qsm_ctx* ctx) {
   for (auto& kv : ctx->twiddles) cudaFree(kv.second);
   for (auto& kv : ctx->tables) cudaFree(kv.second);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  for (int k = 0; k < 2; ++k) {
+    if (ctx->pinned[k]) cudaFreeHost(ctx->pinned[k]);
+    if (ctx->pinned_ev[k]) cudaEventDestroy(ctx->pinned_ev[k]);
+  }
   delete ctx;
   return QSM_OK;
 }

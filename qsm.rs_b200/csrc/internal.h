@@ -71,6 +71,9 @@ struct qsm_ctx {
   std::string prof_prefix;
   std::vector<qsm::ProfRec> prof_pending;
   std::vector<std::pair<std::string, qsm::ProfStat>> prof_stats;
+  // pinned host staging ring for host<->device streaming (staged_h2d / staged_d2h)
+  void* pinned[2] = {nullptr, nullptr};
+  cudaEvent_t pinned_ev[2] = {nullptr, nullptr};
 };
 
 namespace qsm {
@@ -100,6 +103,11 @@ void check_ptr(const void* p, const char* name);
 void check_finite(double v, const char* name);
 
 // Host <-> device staging used by the host-pointer entry points.
+// Copies through two pinned staging buffers (kStageBytes each): the host copy of one
+// chunk overlaps the DMA of the previous one.  Both return with the copies complete.
+constexpr size_t kStageBytes = (size_t)32 << 20;
+void staged_h2d(qsm_ctx* ctx, void* dst, const void* src, size_t bytes);
+void staged_d2h(qsm_ctx* ctx, void* dst, const void* src, size_t bytes);
 void h2d(qsm_ctx* ctx, void* dst, const void* src, size_t bytes);
 void d2h(qsm_ctx* ctx, void* dst, const void* src, size_t bytes);
 void sync(qsm_ctx* ctx);

@@ -232,4 +232,4 @@ def _check_len(arr: np.ndarray, grid: Grid, name: str):
         raise ValueError(f"{name} has {arr.size} values, grid needs {grid.n_total()}")
 
 
-from . import inversion, unwrap, bgremove, pipeline, fft, multi_echo  # noqa: E402
+from . import inversion, unwrap, bgremove, pipeline, fft, multi_echo, nifti  # noqa: E402

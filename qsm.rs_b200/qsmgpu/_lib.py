@@ -22,6 +22,7 @@ STATUS_NAMES = {
     5: "QSM_ERR_CUDA",
     6: "QSM_ERR_INVALID_CONFIG",
     7: "QSM_ERR_NO_DEVICE",
+    8: "QSM_ERR_IO",
 }
 
 PRECISION_F64 = 0
@@ -77,6 +78,13 @@ class QsmNltvParams(C.Structure):
 
 class QsmLinearFitParams(C.Structure):
     _fields_ = [("estimate_offset", C.c_int), ("reliability_threshold_percentile", C.c_double)]
+
+
+class QsmNiftiHeader(C.Structure):
+    _fields_ = [("nx", C.c_size_t), ("ny", C.c_size_t), ("nz", C.c_size_t), ("nt", C.c_size_t),
+                ("voxel_size", C.c_double * 3), ("affine", C.c_double * 16), ("scl_slope", C.c_double),
+                ("scl_inter", C.c_double), ("raw_slope", C.c_double), ("datatype", C.c_int), ("ndim", C.c_int),
+                ("big_endian", C.c_int), ("gzip", C.c_int), ("vox_offset", C.c_size_t)]
 
 
 class QsmIlsqrParams(C.Structure):
@@ -225,6 +233,21 @@ _SIGS = [
                                      C.POINTER(QsmBgRemovalConfig), PROGRESS_FN, C.c_void_p, c_double_p,
                                      c_u8_p]),
     ("qsm_fft3d_real", C.c_int, [C.c_void_p, c_double_p, C.POINTER(QsmGrid), c_double_p]),
+    ("qsm_nifti_parse_header", C.c_int, [c_u8_p, C.c_size_t, C.POINTER(QsmNiftiHeader), C.c_char_p, C.c_size_t]),
+    ("qsm_nifti_load", C.c_int, [c_u8_p, C.c_size_t, C.c_int, c_double_p, C.c_size_t, C.POINTER(QsmNiftiHeader),
+                                 C.c_char_p, C.c_size_t]),
+    ("qsm_nifti_save", C.c_int, [c_double_p, C.c_size_t, C.c_size_t, C.c_size_t, c_double_p, c_double_p, C.c_int,
+                                 c_u8_p, C.c_size_t, C.POINTER(C.c_size_t), C.c_char_p, C.c_size_t]),
+    ("qsm_nifti_read_dims", C.c_int, [C.c_char_p, C.POINTER(C.c_size_t), C.c_char_p, C.c_size_t]),
+    ("qsm_nifti_read_file_header", C.c_int, [C.c_char_p, C.POINTER(QsmNiftiHeader), C.c_char_p, C.c_size_t]),
+    ("qsm_nifti_read_file", C.c_int, [C.c_char_p, C.c_int, c_double_p, C.c_size_t, C.POINTER(QsmNiftiHeader),
+                                      C.c_char_p, C.c_size_t]),
+    ("qsm_nifti_save_file", C.c_int, [C.c_char_p, c_double_p, C.c_size_t, C.c_size_t, C.c_size_t, c_double_p,
+                                      c_double_p, C.c_char_p, C.c_size_t]),
+    ("qsm_nifti_load_device", C.c_int, [C.c_void_p, c_u8_p, C.c_size_t, C.c_int, C.c_void_p, C.c_size_t,
+                                        C.POINTER(QsmNiftiHeader)]),
+    ("qsm_nifti_save_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_size_t, C.c_size_t, c_double_p,
+                                        c_double_p, C.c_int, c_u8_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     ("qsm_linear_fit_params_default", None, [C.POINTER(QsmLinearFitParams)]),
     ("qsm_calculate_b0_weighted", C.c_int, [C.c_void_p, c_double_p, c_double_p, c_double_p, C.c_size_t, c_u8_p,
                                             C.c_size_t, C.c_int, c_double_p]),
