@@ -332,6 +332,136 @@ def bench_batch(local, dev, n_vol=32, seed=7):
             "tkd_batched": {"volumes_per_s": round(n_vol / (t_tkd / 1e3), 3), "ms": round(t_tkd, 3)}}
 
 
+def bench_adjoint(local, dev):
+    """Unrolled TV-ADMM at 160x192x160: K = 50 iterations with no early exit, states
+    checkpointed every 10, lambda 1e-3, rho 2e-2, mixed precision.  Times the forward pass
+    alone and the forward pass plus the hand-written vector-Jacobian product (dL/dfield
+    and dL/dlambda for L = ||chi_K - chi_true||^2)."""
+    import torch
+    import qsmgpu
+    from qsmgpu import Grid, inversion, phantom
+    dims = (160, 192, 160)
+    case = phantom.tv_case(dims, seed=4, n_ellipsoids=12, mask_radius=70.0)
+    grid = Grid.new(*dims)
+    out = {"workload": "unrolled tv_admm 160x192x160, K=50, checkpoint every 10, lambda 1e-3, rho 2e-2, mixed; "
+                       "ellipsoid phantom"}
+    for prec in ("mixed", "f64"):
+        ctx = qsmgpu.Context(local, prec)
+        s = torch.cuda.ExternalStream(ctx.stream_handle(), device=dev)
+        f = torch.from_numpy(np.ascontiguousarray(case.local_field).ravel()).to(dev)
+        m = torch.from_numpy(np.ascontiguousarray(case.mask).ravel()).to(dev)
+        truth = torch.from_numpy(np.ascontiguousarray(case.chi).ravel()).to(dev)
+        chi = torch.empty_like(f)
+        gf = torch.empty_like(f)
+        gchi = torch.empty_like(f)
+
+        def fwd():
+            inversion.tv_admm_unrolled_vjp_device(ctx, f.data_ptr(), m.data_ptr(), grid, (0.0, 0.0, 1.0), 1e-3, 2e-2,
+                                                  50, 10, 0, chi.data_ptr())
+
+        def fwd_bwd():
+            inversion.tv_admm_unrolled_vjp_device(ctx, f.data_ptr(), m.data_ptr(), grid, (0.0, 0.0, 1.0), 1e-3, 2e-2,
+                                                  50, 10, gchi.data_ptr(), chi.data_ptr(), gf.data_ptr())
+
+        fwd()
+        gchi.copy_(2.0 * (chi - truth))
+        fwd_bwd()
+        t_f = _timed(s, fwd, reps=2)
+        t_fb = _timed(s, fwd_bwd, reps=2)
+        out[prec] = {"forward_ms": round(t_f, 2), "forward_plus_vjp_ms": round(t_fb, 2),
+                     "vjp_over_forward": round((t_fb - t_f) / t_f, 3)}
+        ctx.close()
+    return out
+
+
+def bench_multi_echo(local, dev, seed=5):
+    """384x384x256 at 0.6 mm, 3 T, 4 echoes (TE 4/12/20/28 ms): ellipsoid brain mask with 40
+    cylinders at chi 0.3-0.6 ppm over a weak ellipsoid background.  Echo phases are the
+    dipole field times TE (plus noise), magnitudes decay with T2* = 40 ms.  Times the
+    magnitude-weighted linear fit with its 90th-percentile reliability mask (FP64),
+    iLSQR (mixed) on the fitted field, and 1000 iterations of TGV (float32, as in the
+    reference) on the wrapped 20 ms echo."""
+    import torch
+    import qsmgpu
+    from qsmgpu import Grid, inversion, multi_echo as me
+    nx, ny, nz = 384, 384, 256
+    vs = (0.6, 0.6, 0.6)
+    grid = Grid.new(nx, ny, nz, *vs)
+    N = nx * ny * nz
+    g = torch.Generator(device=dev).manual_seed(seed)
+    z, y, x = torch.meshgrid(torch.arange(nz, device=dev, dtype=torch.float32),
+                             torch.arange(ny, device=dev, dtype=torch.float32),
+                             torch.arange(nx, device=dev, dtype=torch.float32), indexing="ij")
+    cx, cy, cz = (nx - 1) / 2, (ny - 1) / 2, (nz - 1) / 2
+    mask = (((x - cx) / (0.42 * nx)) ** 2 + ((y - cy) / (0.45 * ny)) ** 2 + ((z - cz) / (0.40 * nz)) ** 2) < 1
+    chi = 0.02 * ((((x - cx) / (0.3 * nx)) ** 2 + ((y - cy) / (0.3 * ny)) ** 2 + ((z - cz) / (0.3 * nz)) ** 2) < 1)
+    chi = chi.to(torch.float32)
+    for _ in range(40):
+        c = torch.rand(3, generator=g, device=dev) * 0.5 + 0.25
+        c = c * torch.tensor([nx, ny, nz], device=dev, dtype=torch.float32)
+        a = torch.randn(3, generator=g, device=dev)
+        a = a / a.norm()
+        r = 2.0 + 4.0 * torch.rand(1, generator=g, device=dev)
+        length = 20.0 + 40.0 * torch.rand(1, generator=g, device=dev)
+        val = 0.3 + 0.3 * torch.rand(1, generator=g, device=dev)
+        px, py, pz = x - c[0], y - c[1], z - c[2]
+        t = px * a[0] + py * a[1] + pz * a[2]
+        d2 = (px - t * a[0]) ** 2 + (py - t * a[1]) ** 2 + (pz - t * a[2]) ** 2
+        chi = torch.where((t.abs() < length / 2) & (d2 < r * r), val, chi)
+    del x, y, z
+    chi = (chi * mask).to(torch.float64).reshape(-1).contiguous()
+    m8 = mask.reshape(-1).to(torch.uint8).contiguous()
+    ctx = qsmgpu.Context(local, "f64")
+    s = torch.cuda.ExternalStream(ctx.stream_handle(), device=dev)
+    field = torch.empty_like(chi)
+    inversion.dipole_forward_device(ctx, chi.data_ptr(), grid, (0.0, 0.0, 1.0), field.data_ptr())
+    tes = [0.004, 0.012, 0.020, 0.028]
+    w0 = 2.0 * np.pi * 42.58 * 3.0  # rad/s per ppm
+    mags = torch.stack([m8.to(torch.float64) * float(np.exp(-te / 0.04)) for te in tes]).contiguous()
+    noise = torch.randn(len(tes), N, generator=g, device=dev, dtype=torch.float64)
+    phases = torch.stack([field * (w0 * te) for te in tes]) + 0.02 * noise / mags.clamp_min(0.05)
+    phases = (phases * m8.to(torch.float64)).contiguous()
+    fit_f, fit_o, fit_r = (torch.empty(N, dtype=torch.float64, device=dev) for _ in range(3))
+    fit_rel = torch.empty(N, dtype=torch.uint8, device=dev)
+    lp = me.LinearFitParams(True, 90.0)
+
+    def fit():
+        me.multi_echo_linear_fit_device(ctx, phases.data_ptr(), mags.data_ptr(), tes, len(tes), m8.data_ptr(), N, lp,
+                                        fit_f.data_ptr(), fit_o.data_ptr(), fit_r.data_ptr(), fit_rel.data_ptr())
+
+    fit()
+    t_fit = _timed(s, fit, reps=3)
+    fit_bytes = (2 * len(tes) * 8 + 1 + 3 * 8 + 1) * N
+    ppm = (fit_f / w0).contiguous()
+    ctx.close()
+    cm = qsmgpu.Context(local, "mixed")
+    sm = torch.cuda.ExternalStream(cm.stream_handle(), device=dev)
+    chi_out = torch.empty_like(field)
+    il = inversion.IlsqrParams()
+
+    def run_ilsqr():
+        inversion.ilsqr_device(cm, ppm.data_ptr(), m8.data_ptr(), grid, (0.0, 0.0, 1.0), il, chi_out.data_ptr())
+
+    run_ilsqr()
+    t_il = _timed(sm, run_ilsqr)
+    wrapped = torch.remainder(phases[2] + np.pi, 2 * np.pi) - np.pi
+    wrapped = (wrapped * m8.to(torch.float64)).contiguous()
+    tg = inversion.TgvParams(iterations=1000, tol=0.0, fieldstrength=3.0, te=0.020)
+    tgv_out = torch.empty_like(field)
+
+    def run_tgv():
+        inversion.tgv_qsm_device(cm, wrapped.data_ptr(), m8.data_ptr(), grid, tg, (0.0, 0.0, 1.0), tgv_out.data_ptr())
+
+    run_tgv()
+    t_tgv = _timed(sm, run_tgv)
+    cm.close()
+    return {"workload": "384x384x256 at 0.6 mm, 3 T, 4 echoes TE 4/12/20/28 ms, 40 cylinders chi 0.3-0.6 ppm; "
+                        "synthetic phantom",
+            "linear_fit_fp64": {"ms": round(t_fit, 3), "fit_kernel_alg_gb": round(fit_bytes / 1e9, 3),
+                                "note": "ms covers the fit kernel and the reliability percentile (radix select)"},
+            "ilsqr_mixed_ms": round(t_il, 2), "tgv_1000_iterations_ms": round(t_tgv, 2)}
+
+
 def run_reference(args):
     """Reference arm: the reference (Rust) cannot be built here, so its CPU algorithm is
     timed through the f64 restatement in oracle/ on this host's cores, same workload.
@@ -516,6 +646,8 @@ def main():
     if rank == 0 and world == 1 and not args.skip_extras:
         extra["chain_256x256x176"] = bench_chain(local, dev)
         extra["batch_32_volumes"] = bench_batch(local, dev)
+        extra["unrolled_adjoint_160x192x160"] = bench_adjoint(local, dev)
+        extra["multi_echo_384x384x256"] = bench_multi_echo(local, dev)
 
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu_baseline:

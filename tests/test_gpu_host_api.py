@@ -24,7 +24,7 @@ def test_cpp_host_api(tmp_path):
     assert r.returncode == 0, r.stdout + r.stderr
     n = 16
     N = n ** 3
-    res = np.fromfile(out, dtype=np.float64).reshape(4, N)
+    res = np.fromfile(out, dtype=np.float64).reshape(9, N)
     grid = O.Grid.new(n, n, n)
     field = (0.01 * np.sin(0.7 * np.arange(N))).reshape(grid.shape)
     mask = np.ones(grid.shape, np.uint8)
@@ -32,7 +32,17 @@ def test_cpp_host_api(tmp_path):
     refs = [O.tkd(field, mask, grid, (0, 0, 1), O.TkdParams(0.15)),
             O.tv_admm(field, mask, grid, (0, 0, 1), O.TvParams(2e-4, 2e-2, 0.0, 10)),
             O.laplacian_unwrap(phase.reshape(grid.shape), mask, grid),
-            O.sharp(field, mask, grid, O.SharpParams(0.05, 3.0))[0]]
+            O.sharp(field, mask, grid, O.SharpParams(0.05, 3.0))[0],
+            O.rts(field, mask, grid, (0, 0, 1), O.RtsParams(0.15, 1e5, 10.0, 0.0, 7, 4), exact_dc=True),
+            O.nltv(field, mask, grid, (0, 0, 1), O.NltvParams(1e-3, 1.0, 0.0, 5, 2), exact_dc=True),
+            O.ismv(field, mask, grid, O.IsmvParams(1e-6, 20, 3.0))[0],
+            O.resharp(field, mask, grid, O.ResharpParams(3.0, 1e-4, 1e-6, 20))[0]]
+    idx = np.arange(N, dtype=np.float64)
+    tes = [0.005, 0.010, 0.015]
+    ph3 = [0.3 + 150.0 * np.sin(0.01 * idx) * te + 0.01 * np.cos(3.0 * idx + te) for te in tes]
+    mg3 = [1.0 + 0.5 * np.sin(0.2 * idx)] * 3
+    fit = O.multi_echo_linear_fit(ph3, mg3, tes, mask.ravel(), True, 90.0)[0]
+    assert np.array_equal(res[8], fit)
     for got, ref in zip(res, refs):
         ref = ref.ravel()
         assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-9
