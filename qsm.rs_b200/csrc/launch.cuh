@@ -81,8 +81,61 @@ template <typename T> inline long long x_blocks(const Fft3<T>& f) {
   return (npairs + P - 1) / P;
 }
 
+// Compile-time X kernels (float) for the lengths of QSM_FIXED_PLANS; false when the
+// plan is not one of them.
+template <typename T, class Load>
+bool run_x_r2c_fixed(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* spec, const Load& ld, const int* done) {
+  if constexpr (!std::is_same<T, float>::value) {
+    return false;
+  } else {
+    using C = cplx_t<T>;
+#define QSM_TRY_XR(N_, T_, R0_, R1_, R2_)                                                          \
+    if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(f.px)) {                                         \
+      using FP = FixedPlan<N_, T_, R0_, R1_, R2_>;                                                 \
+      const int Tt = x_block_t(T_);                                                                \
+      const int P = x_pencils_per_block<T>(T_);                                                    \
+      const size_t smem = (size_t)(N_ + P * x_rowlen<T>(N_)) * sizeof(C);                          \
+      auto kern = k_x_r2c_fx<T, FP, Load>;                                                         \
+      ensure_smem(kern, smem);                                                                     \
+      LaunchScope ls(ctx, "fft_x_r2c");                                                            \
+      kern<<<(unsigned)x_blocks(f), dim3(Tt, P), smem, ctx->stream>>>(f.g, f.twx, spec, ld, done); \
+      ls.done();                                                                                   \
+      return true;                                                                                 \
+    }
+    QSM_FIXED_PLANS(QSM_TRY_XR)
+#undef QSM_TRY_XR
+    return false;
+  }
+}
+
+template <typename T, class Store>
+bool run_x_c2r_fixed(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* spec, const Store& st, const int* done) {
+  if constexpr (!std::is_same<T, float>::value) {
+    return false;
+  } else {
+    using C = cplx_t<T>;
+#define QSM_TRY_XC(N_, T_, R0_, R1_, R2_)                                                          \
+    if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(f.px)) {                                         \
+      using FP = FixedPlan<N_, T_, R0_, R1_, R2_>;                                                 \
+      const int Tt = x_block_t(T_);                                                                \
+      const int P = x_pencils_per_block<T>(T_);                                                    \
+      const size_t smem = (size_t)(N_ + P * x_rowlen<T>(N_)) * sizeof(C);                          \
+      auto kern = k_x_c2r_fx<T, FP, Store>;                                                        \
+      ensure_smem(kern, smem);                                                                     \
+      LaunchScope ls(ctx, "fft_x_c2r");                                                            \
+      kern<<<(unsigned)x_blocks(f), dim3(Tt, P), smem, ctx->stream>>>(f.g, f.twx, spec, st, done); \
+      ls.done();                                                                                   \
+      return true;                                                                                 \
+    }
+    QSM_FIXED_PLANS(QSM_TRY_XC)
+#undef QSM_TRY_XC
+    return false;
+  }
+}
+
 template <typename T, class Load>
 void run_x_r2c(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* spec, const Load& ld, const int* done) {
+  if (run_x_r2c_fixed<T>(ctx, f, spec, ld, done)) return;
   using C = cplx_t<T>;
   const int Tt = x_block_t(f.px.T);
   const int P = x_pencils_per_block<T>(f.px.T);
@@ -96,6 +149,7 @@ void run_x_r2c(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* spec, const Load& ld, 
 
 template <typename T, class Store>
 void run_x_c2r(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* spec, const Store& st, const int* done) {
+  if (run_x_c2r_fixed<T>(ctx, f, spec, st, done)) return;
   using C = cplx_t<T>;
   const int Tt = x_block_t(f.px.T);
   const int P = x_pencils_per_block<T>(f.px.T);

@@ -261,6 +261,95 @@ __global__ void k_x_c2r(Geom g, const __grid_constant__ FftPlan1D pl, const cplx
 }
 
 // ---------------------------------------------------------------------------
+// Compile-time X passes (FP a FixedPlan): the first Stockham stage reads its inputs
+// straight from global memory through the loader (r2c) or through the Hermitian
+// rebuild of the two half-spectrum rows (c2r), and the c2r's last stage hands its
+// values straight to the store functor, so each pass makes one shared-memory round
+// trip fewer than k_x_r2c / k_x_c2r and runs with constant loop bounds.
+// blockDim = (Tb >= FP::T, P) as for the runtime kernels.
+// ---------------------------------------------------------------------------
+template <typename T, class FP, class Load>
+__global__ void k_x_r2c_fx(Geom g, const cplx_t<T>* __restrict__ twg, cplx_t<T>* __restrict__ spec, Load ld,
+                           const int* __restrict__ done) {
+  using C = cplx_t<T>;
+  constexpr int N = FP::n, TT = FP::T, NXH = N / 2 + 1;
+  if (done != nullptr && *done) return;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* tw = reinterpret_cast<C*>(smraw);
+  C* sm = tw + N;
+  const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+  for (int i = tid; i < N; i += blockDim.x * blockDim.y) tw[i] = twg[i];
+  const int t = threadIdx.x;
+  const int p = threadIdx.y;
+  const int nrows = g.nrows();
+  const int a = 2 * (blockIdx.x * blockDim.y + p), b = a + 1;
+  const bool active = a < nrows && t < TT;
+  const bool hasb = b < nrows;
+  C* sp = sm + p * x_rowlen<T>(N);
+  SAPadded<PadG<T>::G> sa;
+  auto fetch = [&](int e) -> C { return mk<C>(ld(a, e), hasb ? ld(b, e) : T(0)); };
+  auto emit = [&](int e, C v) { sp[sa(e)] = v; };
+  FP::template run<-1>(t, active, sp, sa, tw, fetch, emit);
+  if (active) {
+    const T half = T(0.5);
+    C* ra = spec + (long long)a * g.pitch;
+    C* rb = spec + (long long)b * g.pitch;
+#pragma unroll
+    for (int c = 0; c < (NXH + TT - 1) / TT; ++c) {
+      const int k = t + c * TT;
+      if (k < NXH) {
+        const C zk = sp[sa(k)];
+        const C zn = sp[sa(k == 0 ? 0 : N - k)];
+        ra[k] = mk<C>((zk.x + zn.x) * half, (zk.y - zn.y) * half);
+        if (hasb) rb[k] = mk<C>((zk.y + zn.y) * half, (zn.x - zk.x) * half);
+      }
+    }
+  }
+}
+
+template <typename T, class FP, class Store>
+__global__ void k_x_c2r_fx(Geom g, const cplx_t<T>* __restrict__ twg, const cplx_t<T>* __restrict__ spec, Store st0,
+                           const int* __restrict__ done) {
+  using C = cplx_t<T>;
+  constexpr int N = FP::n, TT = FP::T;
+  if (done != nullptr && *done) return;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* tw = reinterpret_cast<C*>(smraw);
+  C* sm = tw + N;
+  const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+  for (int i = tid; i < N; i += blockDim.x * blockDim.y) tw[i] = twg[i];
+  const int t = threadIdx.x;
+  const int p = threadIdx.y;
+  const int nrows = g.nrows();
+  const int a = 2 * (blockIdx.x * blockDim.y + p), b = a + 1;
+  const bool active = a < nrows && t < TT;
+  const bool hasb = b < nrows;
+  C* sp = sm + p * x_rowlen<T>(N);
+  SAPadded<PadG<T>::G> sa;
+  const C* ra = spec + (long long)a * g.pitch;
+  const C* rb = spec + (long long)b * g.pitch;
+  // z[e] = A[e] + i B[e] from the two half spectra (A, B Hermitian)
+  auto fetch = [&](int e) -> C {
+    const bool lo = e <= N / 2;
+    const int k = lo ? e : N - e;
+    C xa = ra[k];
+    C xb = hasb ? rb[k] : mk<C>(T(0), T(0));
+    if (k == 0 || 2 * k == N) {
+      xa.y = T(0);
+      xb.y = T(0);
+    }
+    return lo ? mk<C>(xa.x - xb.y, xa.y + xb.x) : mk<C>(xa.x + xb.y, xb.x - xa.y);
+  };
+  Store st = st0;
+  auto emit = [&](int e, C v) {
+    st(a, e, v.x);
+    if (hasb) st(b, e, v.y);
+  };
+  FP::template run<+1>(t, active, sp, sa, tw, fetch, emit);
+  st.finish();
+}
+
+// ---------------------------------------------------------------------------
 // Tiled Y/Z passes.  A tile is P consecutive x' columns (P*sizeof(C) = 128 bytes, or
 // narrower for long axes) at one outer index, all n elements along the transform
 // axis.  blockDim = (P, T);
