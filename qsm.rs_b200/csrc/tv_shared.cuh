@@ -420,6 +420,231 @@ __global__ void __launch_bounds__(kStepBX* kStepBY)
   }
 }
 
+// k_tv_step_v (float, unweighted, full update) with every global read of the plane loop
+// staged through shared memory by cp.async.  A four-slot ring per block holds, for
+// plane k: x0 and y at plane k+1 for the block's 8 rows and its two halo rows (the
+// rows j-1 of the first and j+1 of the last), y_{i-2} and u at plane k, uy of the
+// lower halo row, and per row the x-halo scalars (x0, y at the neighbour across the
+// warp's ends, ux at the lower one).  Two planes are in flight while one is computed,
+// so loads hold no registers and no warp waits on L2 inside the loop.
+// Slot s(kk) = (kk - k0 + 1) % 4; slot s(k0 - 1) holds only the plane-k0 part.
+// Same arithmetic per voxel as k_tv_step.
+constexpr int kStageSlots = 4;
+struct StepSlot {
+  float4 a[6][kStepBY][kStepBX];  // x0(k+1), y(k+1), y_{i-2}(k), ux(k), uy(k), uz(k)
+  float4 hx0[2][kStepBX];         // halo rows (0: lower, 1: upper) of x0(k+1)
+  float4 hy[2][kStepBX];          // ... and of y(k+1)
+  float4 huy[kStepBX];            // uy(k) of the lower halo row
+  float xm[kStepBY][4];           // x0(k+1), y(k+1), ux(k) at the lower x neighbour
+  float xp[kStepBY][4];           // x0(k+1), y(k+1) at the upper x neighbour
+};
+constexpr size_t kStepStagedSmem = (size_t)kStageSlots * sizeof(StepSlot);
+
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kStepBX* kStepBY, 2)
+    k_tv_step_s(int nx, int ny, int nz, int zchunk, float hx, float hy, float hz, float thr,
+                const float* __restrict__ x0, const float* __restrict__ ycur, const float* __restrict__ yprev,
+                const float* __restrict__ ui, float* __restrict__ uo, float* __restrict__ div,
+                double2* __restrict__ partials, TvState* st) {
+  static_assert(std::is_same<T, float>::value, "the staged stencil is single precision");
+  using W = Vec16<float>;
+  using V = W::V;
+  constexpr int NV = W::n;
+  if (st->done) return;
+  extern __shared__ __align__(16) unsigned char stage_raw[];
+  StepSlot* ring = reinterpret_cast<StepSlot*>(stage_raw);
+  const int kiter = st->k;
+  const bool check = kiter >= 2;
+  const long long N = (long long)nx * ny * nz;
+  const long long sz = (long long)nx * ny;
+  const int lane = threadIdx.x, ty = threadIdx.y;
+  const int nxv = nx / NV;
+  const int v0 = blockIdx.x * kStepBX + lane;
+  const int jb = blockIdx.y * kStepBY;
+  const int j0 = jb + ty;
+  const bool in = v0 < nxv && j0 < ny;
+  const int i = (v0 < nxv ? v0 : nxv - 1) * NV;
+  const int j = j0 < ny ? j0 : ny - 1;
+  const int ip = i + NV < nx ? i + NV : 0, im = i > 0 ? i - 1 : nx - 1;
+  const int k0 = blockIdx.z * zchunk;
+  const int k1 = k0 + zchunk < nz ? k0 + zchunk : nz;
+  const bool shf_p = (lane < 31) && (v0 + 1 < nxv);
+  const bool shf_m = (lane > 0) && (v0 > 0) && (v0 < nxv);
+  const bool need_p = v0 < nxv && !shf_p;  // the row's last vector: x-halo above
+  const bool need_m = v0 < nxv && !shf_m;  // the row's first vector: x-halo below
+  // y-neighbours staged by the sibling row (exactly rows j +- 1), else the halo rows
+  const bool stj_p = ty + 1 < kStepBY && j0 + 1 < ny;
+  const bool stj_m = ty > 0 && j0 < ny;
+  const int jlast = jb + kStepBY - 1 < ny ? jb + kStepBY - 1 : ny - 1;
+  const long long row_lo = (long long)(jb > 0 ? jb - 1 : ny - 1) * nx;  // row below the block
+  const long long row_hi = (long long)(jlast + 1 < ny ? jlast + 1 : 0) * nx;  // row above its last row
+  const int ilane = (v0 < nxv ? v0 : nxv - 1) * NV;
+  const long long rowj = (long long)j * nx;
+  auto slot = [&](int kk) -> StepSlot& { return ring[(kk - k0 + 1) & (kStageSlots - 1)]; };
+  auto issue = [&](int kk) {  // stage for plane kk (kk = k0 - 1: the plane-k0 part only)
+    StepSlot& S = slot(kk);
+    const int kn = kk + 1 < nz ? kk + 1 : 0;
+    const long long pn = (long long)kn * sz;
+    cp_async16(&S.a[0][ty][lane], x0 + pn + rowj + i, true);
+    cp_async16(&S.a[1][ty][lane], ycur + pn + rowj + i, true);
+    if (ty == 0) {
+      cp_async16(&S.hx0[0][lane], x0 + pn + row_lo + ilane, true);
+      cp_async16(&S.hy[0][lane], ycur + pn + row_lo + ilane, true);
+    } else if (ty == kStepBY - 1) {
+      cp_async16(&S.hx0[1][lane], x0 + pn + row_hi + ilane, true);
+      cp_async16(&S.hy[1][lane], ycur + pn + row_hi + ilane, true);
+    }
+    if (need_m) {
+      cp_async4(&S.xm[ty][0], x0 + pn + rowj + im);
+      cp_async4(&S.xm[ty][1], ycur + pn + rowj + im);
+    }
+    if (need_p) {
+      cp_async4(&S.xp[ty][0], x0 + pn + rowj + ip);
+      cp_async4(&S.xp[ty][1], ycur + pn + rowj + ip);
+    }
+    if (kk >= k0) {
+      const long long pk = (long long)kk * sz;
+      const long long c = pk + rowj + i;
+      if (check) cp_async16(&S.a[2][ty][lane], yprev + c, true);
+      cp_async16(&S.a[3][ty][lane], ui + c, true);
+      cp_async16(&S.a[4][ty][lane], ui + N + c, true);
+      cp_async16(&S.a[5][ty][lane], ui + 2 * N + c, true);
+      if (ty == 0) cp_async16(&S.huy[lane], ui + N + pk + row_lo + ilane, true);
+      if (need_m) cp_async4(&S.xm[ty][2], ui + pk + rowj + im);
+    }
+  };
+  auto ldv = [](const float4& a) -> V { return V{{a.x, a.y, a.z, a.w}}; };
+  auto diffv = [](const float4& a, const float4& b) -> V { return V{{a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w}}; };
+  auto X = [&](long long q) -> V {
+    const V a = W::ld(x0 + q), b = W::ld(ycur + q);
+    V r;
+#pragma unroll
+    for (int e = 0; e < NV; ++e) r.v[e] = a.v[e] - b.v[e];
+    return r;
+  };
+  const int kmm = k0 > 0 ? k0 - 1 : nz - 1;
+  V x_km = X(kmm * sz + rowj + i);
+  V uz_km = W::ld(ui + 2 * N + kmm * sz + rowj + i);
+  issue(k0 - 1);
+  cp_async_commit();
+  issue(k0);
+  cp_async_commit();
+  if (k0 + 1 < k1) issue(k0 + 1);
+  cp_async_commit();
+  double sd = 0.0, sx = 0.0;
+  for (int k = k0; k < k1; ++k) {
+    if (k + 2 < k1) issue(k + 2);
+    cp_async_commit();
+    cp_async_wait<2>();  // the stages of planes k - 1 and k have landed
+    __syncthreads();
+    const StepSlot& Sp = slot(k - 1);  // x0, y at plane k
+    const StepSlot& Sk = slot(k);      // x0, y at plane k + 1; y_{i-2}, u at plane k
+    const long long c = (long long)k * sz + rowj + i;
+    const V x_k = diffv(Sp.a[0][ty][lane], Sp.a[1][ty][lane]);
+    const V x_kp = diffv(Sk.a[0][ty][lane], Sk.a[1][ty][lane]);
+    if (check && in) {
+      const V a = ldv(Sp.a[0][ty][lane]), b = ldv(Sk.a[2][ty][lane]);
+#pragma unroll
+      for (int e = 0; e < NV; ++e) {
+        const double dd = (double)x_k.v[e] - (double)(a.v[e] - b.v[e]);
+        sd += dd * dd;
+        sx += (double)x_k.v[e] * (double)x_k.v[e];
+      }
+    }
+    const V ux = ldv(Sk.a[3][ty][lane]), uy = ldv(Sk.a[4][ty][lane]), uz = ldv(Sk.a[5][ty][lane]);
+    float xnext = __shfl_down_sync(0xffffffffu, x_k.v[0], 1);
+    float xprev = __shfl_up_sync(0xffffffffu, x_k.v[NV - 1], 1);
+    float uxprev = __shfl_up_sync(0xffffffffu, ux.v[NV - 1], 1);
+    if (need_p) xnext = Sp.xp[ty][0] - Sp.xp[ty][1];
+    if (need_m) {
+      xprev = Sp.xm[ty][0] - Sp.xm[ty][1];
+      uxprev = Sk.xm[ty][2];
+    }
+    const V xjp = stj_p ? diffv(Sp.a[0][ty + 1][lane], Sp.a[1][ty + 1][lane]) : diffv(Sp.hx0[1][lane], Sp.hy[1][lane]);
+    const V xjm = stj_m ? diffv(Sp.a[0][ty - 1][lane], Sp.a[1][ty - 1][lane]) : diffv(Sp.hx0[0][lane], Sp.hy[0][lane]);
+    const V uym = stj_m ? ldv(Sk.a[4][ty - 1][lane]) : ldv(Sk.huy[lane]);
+    V ox, oy, oz, dv;
+#pragma unroll
+    for (int e = 0; e < NV; ++e) {
+      const float xe = x_k.v[e];
+      const float xip = e + 1 < NV ? x_k.v[e + 1] : xnext;
+      const float xim = e > 0 ? x_k.v[e - 1] : xprev;
+      const float uxm = e > 0 ? ux.v[e - 1] : uxprev;
+      const float vx = (xip - xe) * hx + ux.v[e];
+      const float vy = (xjp.v[e] - xe) * hy + uy.v[e];
+      const float vz = (x_kp.v[e] - xe) * hz + uz.v[e];
+      const float zx = shrink(vx, thr), zy = shrink(vy, thr), zz = shrink(vz, thr);
+      const float gx = 2.0f * zx - vx, gy = 2.0f * zy - vy, gz = 2.0f * zz - vz;
+      const float vxm = (xe - xim) * hx + uxm;
+      const float vym = (xe - xjm.v[e]) * hy + uym.v[e];
+      const float vzm = (xe - x_km.v[e]) * hz + uz_km.v[e];
+      const float gxm = 2.0f * shrink(vxm, thr) - vxm;
+      const float gym = 2.0f * shrink(vym, thr) - vym;
+      const float gzm = 2.0f * shrink(vzm, thr) - vzm;
+      ox.v[e] = vx - zx;
+      oy.v[e] = vy - zy;
+      oz.v[e] = vz - zz;
+      dv.v[e] = (gx - gxm) * hx + (gy - gym) * hy + (gz - gzm) * hz;
+    }
+    if (in) {
+      if (kiter == 1) {  // first update: x_0 = u = g = 0 (see k_tv_step)
+        ox = V{};
+        oy = V{};
+        oz = V{};
+        dv = V{};
+      }
+      W::st(uo + c, ox);
+      W::st(uo + N + c, oy);
+      W::st(uo + 2 * N + c, oz);
+      W::st(div + c, dv);
+    }
+    uz_km = uz;
+    x_km = x_k;
+    __syncthreads();  // slot s(k - 1) is refilled by the next iteration
+  }
+  cp_async_wait<0>();
+  __shared__ int am_last;
+  double a = sd, b = sx;
+  block_sum2(a, b);
+  const int tid = threadIdx.x + kStepBX * threadIdx.y;
+  const int nblocks = gridDim.x * gridDim.y * gridDim.z;
+  const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+  if (tid == 0) {
+    partials[bid] = make_double2(a, b);
+    __threadfence();
+    const unsigned prev = atomicAdd(&st->counter, 1u);
+    am_last = (prev == (unsigned)nblocks - 1);
+  }
+  __syncthreads();
+  if (am_last) {
+    __threadfence();
+    double pa = 0.0, pb = 0.0;
+    for (int q = tid; q < nblocks; q += kStepBX * kStepBY) {
+      const double2 p = __ldcg(&partials[q]);
+      pa += p.x;
+      pb += p.y;
+    }
+    block_sum2(pa, pb);
+    if (tid == 0) {
+      if (check) {
+        const double rc = sqrt(pa) / (sqrt(pb) + 1e-20);  // src/utils/mod.rs:69-77
+        st->rc = rc;
+        if (rc < st->tol) {
+          st->done = 1;
+          st->conv_iter = kiter - 1;
+        }
+      }
+      st->k = kiter + 1;
+      st->counter = 0u;
+    }
+  }
+}
+
 template <typename T>
 __global__ void k_tv_out(long long N, const T* __restrict__ x0, const T* __restrict__ y,
                          const uint8_t* __restrict__ mask, double* __restrict__ out) {
@@ -443,6 +668,9 @@ template <typename T> struct TvVol {
   dim3 sgrid;
   int zchunk;
   bool vec, use_mult;
+  bool staged = false;  // k_tv_step_s for the full update (float, unweighted, 16-byte rows)
+  dim3 sgrid_s;
+  int zchunk_s = 0;
   T hx, hy, hz, thr, scale;
   const T* w = nullptr;  // per-voxel shrink weights (NLTV); nullptr: unweighted
   const uint8_t* mask;
@@ -477,7 +705,17 @@ void tv_alloc(qsm_ctx* ctx, TvVol<T>& v, const std::string& pre, const GridDims&
   if (zchunk > d.nz) zchunk = d.nz;
   v.zchunk = zchunk;
   v.sgrid = dim3(gbx, gby, (d.nz + zchunk - 1) / zchunk);
-  v.partials = ws<double2>(ctx, nm("partials"), (size_t)v.sgrid.x * v.sgrid.y * v.sgrid.z);
+  size_t nblk = (size_t)v.sgrid.x * v.sgrid.y * v.sgrid.z;
+  if (v.vec) {
+    // staged stencil: about two waves of 2 blocks per SM, each block marching >= 4 planes
+    const long long resident = 2LL * sm_count(ctx);
+    const long long zc = std::max<long long>(1, 2 * resident / ((long long)gbx * gby));
+    v.zchunk_s = (int)std::min<long long>(d.nz, std::max<long long>(4, (d.nz + zc - 1) / zc));
+    v.sgrid_s = dim3(gbx, gby, (d.nz + v.zchunk_s - 1) / v.zchunk_s);
+    v.staged = true;
+    nblk = std::max(nblk, (size_t)v.sgrid_s.x * v.sgrid_s.y * v.sgrid_s.z);
+  }
+  v.partials = ws<double2>(ctx, nm("partials"), nblk);
   v.st = st;
   v.scale = (T)(1.0 / (double)N);
   v.hx = (T)(1.0 / d.vsx);
@@ -525,6 +763,17 @@ void tv_setup(qsm_ctx* ctx, TvVol<T>& v, const std::string& pre, const GridDims&
 // iteration i with parity q = i % 2: reads y_{i-1} = yb[1-q], y_{i-2} = yb[q],
 // u = ub[1-q]; writes u' = ub[q], y_i = yb[q]
 template <typename T> void tv_step_launch(qsm_ctx* ctx, const TvVol<T>& v, int q, int check_only) {
+  if constexpr (std::is_same<T, float>::value) {
+    if (v.staged && !v.w && !check_only) {
+      ensure_smem(k_tv_step_s<T>, kStepStagedSmem);
+      LaunchScope ls(ctx, "tv_step");
+      k_tv_step_s<T><<<v.sgrid_s, dim3(kStepBX, kStepBY), kStepStagedSmem, ctx->stream>>>(
+          v.d.nx, v.d.ny, v.d.nz, v.zchunk_s, v.hx, v.hy, v.hz, v.thr, v.x0, v.yb[1 - q], v.yb[q], v.ub[1 - q],
+          v.ub[q], v.div, v.partials, v.st);
+      ls.done();
+      return;
+    }
+  }
   LaunchScope ls(ctx, "tv_step");
   auto kern = v.w ? (v.vec ? k_tv_step_v<T, true> : k_tv_step<T, true>)
                   : (v.vec ? k_tv_step_v<T, false> : k_tv_step<T, false>);
