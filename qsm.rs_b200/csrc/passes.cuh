@@ -702,9 +702,10 @@ __global__ void __maxnreg__(YzRegCap<T>::value) k_z_fused_m(Geom g, const __grid
   cp_async_wait<0>();
 }
 
-// Compile-time form of k_z_fused_m (see k_pass_yz_fx).
+// Compile-time form of k_z_fused_m (see k_pass_yz_fx).  Both transforms are inlined,
+// so it is compiled for two blocks per SM: the three-block register cap spills.
 template <typename T, class FP, int P>
-__global__ void __launch_bounds__(P* FP::T, (P * FP::T <= 256 ? 3 : 1))
+__global__ void __launch_bounds__(P* FP::T, (P * FP::T <= 256 ? 2 : 1))
     k_z_fused_m_fx(Geom g, TileWalk w, const cplx_t<T>* __restrict__ twg, const cplx_t<T>* src, cplx_t<T>* dst,
                    const T* __restrict__ mult, const int* __restrict__ done) {
   using C = cplx_t<T>;
