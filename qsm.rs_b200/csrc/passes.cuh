@@ -385,6 +385,9 @@ __device__ __forceinline__ void issue_tile(const C* __restrict__ src, C* buf, co
 // Register cap of the tiled Y/Z kernels: three 256-thread CTAs per SM in single
 // precision, three 128-thread CTAs in double.
 template <typename T> struct YzRegCap { static constexpr int value = sizeof(T) == 4 ? 80 : 128; };
+// The fused Z kernels run two transforms around a pointwise op; under the Y/Z cap they
+// spill (float: ~0.1 KB, double: ~1.5 KB per thread), so they get a larger one.
+template <typename T> struct ZRegCap { static constexpr int value = sizeof(T) == 4 ? 128 : 168; };
 
 template <typename T, int DIR, int AXIS, class Op>
 __global__ void __maxnreg__(YzRegCap<T>::value)
@@ -650,7 +653,7 @@ __device__ __forceinline__ void issue_mtile(const T* __restrict__ src, T* buf, c
 // multiplier (spectrum layout, real) is staged with the spectrum tile, so the
 // pointwise step is one shared-memory read per element.  Needs P*sizeof(T) >= 16.
 template <typename T>
-__global__ void __maxnreg__(YzRegCap<T>::value) k_z_fused_m(Geom g, const __grid_constant__ FftPlan1D pl, TileWalk w,
+__global__ void __maxnreg__(ZRegCap<T>::value) k_z_fused_m(Geom g, const __grid_constant__ FftPlan1D pl, TileWalk w,
                             const cplx_t<T>* __restrict__ twg, const cplx_t<T>* src, cplx_t<T>* dst,
                             const T* __restrict__ mult, const int* __restrict__ done) {
   using C = cplx_t<T>;
@@ -758,7 +761,7 @@ __global__ void __launch_bounds__(P* FP::T, (P * FP::T <= 256 ? 2 : 1))
 
 // Z forward -> Op::mid pointwise -> Z inverse, tiled like k_pass_yz (outer = y).
 template <typename T, class Op>
-__global__ void __maxnreg__(YzRegCap<T>::value)
+__global__ void __maxnreg__(ZRegCap<T>::value)
     k_z_fused(Geom g, const __grid_constant__ FftPlan1D pl, TileWalk w, const cplx_t<T>* __restrict__ twg,
                           const cplx_t<T>* src, cplx_t<T>* dst, Op op, const int* __restrict__ done) {
   using C = cplx_t<T>;
