@@ -228,6 +228,11 @@ template <typename T> TileWalk tile_walk(const Fft3<T>& f, int axis, int P) {
   return w;
 }
 
+// shared memory of the direct-fetch kernels: twiddles + one tile (the stage exchange)
+template <typename T> inline size_t dx_smem(int n, int P) {
+  return (size_t)(((n + 7) & ~7) + (size_t)n * P) * sizeof(cplx_t<T>);
+}
+
 template <typename T> inline size_t yz_smem(int n, int P) {
   return (size_t)(((n + 7) & ~7) + 2 * (size_t)n * P) * sizeof(cplx_t<T>);
 }
@@ -279,8 +284,8 @@ bool run_yz_fixed(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T
 #define QSM_TRY_YZ(N_, T_, R0_, R1_, R2_)                                                         \
     if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(pl) && kFxCols * T_ <= 1024) {                   \
       using FP = FixedPlan<N_, T_, R0_, R1_, R2_>;                                                \
-      auto kern = k_pass_yz_fx<T, DIR, FP, kFxCols>;                                              \
-      const size_t smem = yz_smem<T>(N_, kFxCols);                                                \
+      auto kern = k_pass_yz_dx<T, DIR, FP, kFxCols>;                                              \
+      const size_t smem = dx_smem<T>(N_, kFxCols);                                                \
       const TileWalk w = tile_walk(f, AXIS, kFxCols);                                             \
       unsigned grid = 0;                                                                          \
       if (!fx_launch_ok(ctx, kern, kFxCols * T_, smem, &grid, w.ntiles)) return false;            \
