@@ -259,6 +259,7 @@ template <typename T, class K> int yz_tile_width(K kernel, int n, int Tn) {
 // Compile-time Y/Z kernels (float, 16-column tiles) for the axis lengths of
 // QSM_FIXED_PLANS; returns false when the plan is not one of them.
 constexpr int kFxCols = 16;
+constexpr int kZmCols = 8;  // columns per tile of the fused Z pass
 template <class K> bool fx_launch_ok(qsm_ctx* ctx, K kern, int threads, size_t smem, unsigned* grid, long long work) {
   if (smem > 227u * 1024u) return false;
   ensure_smem(kern, smem);
@@ -364,15 +365,15 @@ void run_z_fused_m(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<
   const FftPlan1D& pl = f.pz;
   if constexpr (std::is_same<T, float>::value) {
 #define QSM_TRY_ZM(N_, T_, R0_, R1_, R2_)                                                         \
-    if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(pl) && kFxCols * T_ <= 1024) {                   \
+    if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(pl) && kZmCols * T_ <= 1024) {                   \
       using FP = FixedPlan<N_, T_, R0_, R1_, R2_>;                                                \
-      auto kfx = k_z_fused_m_fx<T, FP, kFxCols>;                                                  \
-      const size_t smem = zm_smem<T>(N_, kFxCols);                                                \
-      const TileWalk w = tile_walk(f, 2, kFxCols);                                                \
+      auto kfx = k_z_fused_m_fx<T, FP, kZmCols>;                                                  \
+      const size_t smem = zm_smem<T>(N_, kZmCols);                                                \
+      const TileWalk w = tile_walk(f, 2, kZmCols);                                                \
       unsigned grid = 0;                                                                          \
-      if (fx_launch_ok(ctx, kfx, kFxCols * T_, smem, &grid, w.ntiles)) {                          \
+      if (fx_launch_ok(ctx, kfx, kZmCols * T_, smem, &grid, w.ntiles)) {                          \
         LaunchScope ls(ctx, "fft_z_fused");                                                       \
-        kfx<<<grid, dim3(kFxCols, T_), smem, ctx->stream>>>(f.g, w, f.twz, src, dst, mult, done); \
+        kfx<<<grid, dim3(kZmCols, T_), smem, ctx->stream>>>(f.g, w, f.twz, src, dst, mult, done); \
         ls.done();                                                                                \
         return;                                                                                   \
       }                                                                                           \
