@@ -420,7 +420,7 @@ __global__ void __launch_bounds__(kStepBX* kStepBY)
   }
 }
 
-// k_tv_step_v (float, unweighted, full update) with every global read of the plane loop
+// k_tv_step_v (unweighted, full update; float4 or double2 vectors) with every global read of the plane loop
 // staged through shared memory by cp.async.  A four-slot ring per block holds, for
 // plane k: x0 and y at plane k+1 for the block's 8 rows and its two halo rows (the
 // rows j-1 of the first and j+1 of the last), y_{i-2} and u at plane k, uy of the
@@ -430,34 +430,36 @@ __global__ void __launch_bounds__(kStepBX* kStepBY)
 // Slot s(kk) = (kk - k0 + 1) % 4; slot s(k0 - 1) holds only the plane-k0 part.
 // Same arithmetic per voxel as k_tv_step.
 constexpr int kStageSlots = 4;
-struct StepSlot {
-  float4 a[6][kStepBY][kStepBX];  // x0(k+1), y(k+1), y_{i-2}(k), ux(k), uy(k), uz(k)
-  float4 hx0[2][kStepBX];         // halo rows (0: lower, 1: upper) of x0(k+1)
-  float4 hy[2][kStepBX];          // ... and of y(k+1)
-  float4 huy[kStepBX];            // uy(k) of the lower halo row
-  float xm[kStepBY][4];           // x0(k+1), y(k+1), ux(k) at the lower x neighbour
-  float xp[kStepBY][4];           // x0(k+1), y(k+1) at the upper x neighbour
+// One ring slot; the vector entries are 16-byte chunks (4 floats or 2 doubles).
+template <typename T> struct StepSlot {
+  uint4 a[6][kStepBY][kStepBX];  // x0(k+1), y(k+1), y_{i-2}(k), ux(k), uy(k), uz(k)
+  uint4 hx0[2][kStepBX];         // halo rows (0: lower, 1: upper) of x0(k+1)
+  uint4 hy[2][kStepBX];          // ... and of y(k+1)
+  uint4 huy[kStepBX];            // uy(k) of the lower halo row
+  T xm[kStepBY][4];              // x0(k+1), y(k+1), ux(k) at the lower x neighbour
+  T xp[kStepBY][4];              // x0(k+1), y(k+1) at the upper x neighbour
 };
-constexpr size_t kStepStagedSmem = (size_t)kStageSlots * sizeof(StepSlot);
+template <typename T> constexpr size_t step_staged_smem() { return (size_t)kStageSlots * sizeof(StepSlot<T>); }
 
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+// cp.async of one element (4 or 8 bytes)
+template <typename T> __device__ __forceinline__ void cp_async_elem(void* smem, const void* gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+  if constexpr (sizeof(T) == 4) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 
 template <typename T>
 __global__ void __launch_bounds__(kStepBX* kStepBY, 2)
-    k_tv_step_s(int nx, int ny, int nz, int zchunk, float hx, float hy, float hz, float thr,
-                const float* __restrict__ x0, const float* __restrict__ ycur, const float* __restrict__ yprev,
-                const float* __restrict__ ui, float* __restrict__ uo, float* __restrict__ div,
-                double2* __restrict__ partials, TvState* st) {
-  static_assert(std::is_same<T, float>::value, "the staged stencil is single precision");
-  using W = Vec16<float>;
-  using V = W::V;
+    k_tv_step_s(int nx, int ny, int nz, int zchunk, T hx, T hy, T hz, T thr, const T* __restrict__ x0,
+                const T* __restrict__ ycur, const T* __restrict__ yprev, const T* __restrict__ ui,
+                T* __restrict__ uo, T* __restrict__ div, double2* __restrict__ partials, TvState* st) {
+  using W = Vec16<T>;
+  using V = typename W::V;
+  using Slot = StepSlot<T>;
   constexpr int NV = W::n;
   if (st->done) return;
   extern __shared__ __align__(16) unsigned char stage_raw[];
-  StepSlot* ring = reinterpret_cast<StepSlot*>(stage_raw);
+  Slot* ring = reinterpret_cast<Slot*>(stage_raw);
   const int kiter = st->k;
   const bool check = kiter >= 2;
   const long long N = (long long)nx * ny * nz;
@@ -485,9 +487,9 @@ __global__ void __launch_bounds__(kStepBX* kStepBY, 2)
   const long long row_hi = (long long)(jlast + 1 < ny ? jlast + 1 : 0) * nx;  // row above its last row
   const int ilane = (v0 < nxv ? v0 : nxv - 1) * NV;
   const long long rowj = (long long)j * nx;
-  auto slot = [&](int kk) -> StepSlot& { return ring[(kk - k0 + 1) & (kStageSlots - 1)]; };
+  auto slot = [&](int kk) -> Slot& { return ring[(kk - k0 + 1) & (kStageSlots - 1)]; };
   auto issue = [&](int kk) {  // stage for plane kk (kk = k0 - 1: the plane-k0 part only)
-    StepSlot& S = slot(kk);
+    Slot& S = slot(kk);
     const int kn = kk + 1 < nz ? kk + 1 : 0;
     const long long pn = (long long)kn * sz;
     cp_async16(&S.a[0][ty][lane], x0 + pn + rowj + i, true);
@@ -500,12 +502,12 @@ __global__ void __launch_bounds__(kStepBX* kStepBY, 2)
       cp_async16(&S.hy[1][lane], ycur + pn + row_hi + ilane, true);
     }
     if (need_m) {
-      cp_async4(&S.xm[ty][0], x0 + pn + rowj + im);
-      cp_async4(&S.xm[ty][1], ycur + pn + rowj + im);
+      cp_async_elem<T>(&S.xm[ty][0], x0 + pn + rowj + im);
+      cp_async_elem<T>(&S.xm[ty][1], ycur + pn + rowj + im);
     }
     if (need_p) {
-      cp_async4(&S.xp[ty][0], x0 + pn + rowj + ip);
-      cp_async4(&S.xp[ty][1], ycur + pn + rowj + ip);
+      cp_async_elem<T>(&S.xp[ty][0], x0 + pn + rowj + ip);
+      cp_async_elem<T>(&S.xp[ty][1], ycur + pn + rowj + ip);
     }
     if (kk >= k0) {
       const long long pk = (long long)kk * sz;
@@ -515,11 +517,21 @@ __global__ void __launch_bounds__(kStepBX* kStepBY, 2)
       cp_async16(&S.a[4][ty][lane], ui + N + c, true);
       cp_async16(&S.a[5][ty][lane], ui + 2 * N + c, true);
       if (ty == 0) cp_async16(&S.huy[lane], ui + N + pk + row_lo + ilane, true);
-      if (need_m) cp_async4(&S.xm[ty][2], ui + pk + rowj + im);
+      if (need_m) cp_async_elem<T>(&S.xm[ty][2], ui + pk + rowj + im);
     }
   };
-  auto ldv = [](const float4& a) -> V { return V{{a.x, a.y, a.z, a.w}}; };
-  auto diffv = [](const float4& a, const float4& b) -> V { return V{{a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w}}; };
+  auto ldv = [](const uint4& a) -> V {
+    V r;
+    memcpy(&r, &a, sizeof(V));
+    return r;
+  };
+  auto diffv = [&](const uint4& a, const uint4& b) -> V {
+    const V va = ldv(a), vb = ldv(b);
+    V r;
+#pragma unroll
+    for (int e = 0; e < NV; ++e) r.v[e] = va.v[e] - vb.v[e];
+    return r;
+  };
   auto X = [&](long long q) -> V {
     const V a = W::ld(x0 + q), b = W::ld(ycur + q);
     V r;
@@ -542,8 +554,8 @@ __global__ void __launch_bounds__(kStepBX* kStepBY, 2)
     cp_async_commit();
     cp_async_wait<2>();  // the stages of planes k - 1 and k have landed
     __syncthreads();
-    const StepSlot& Sp = slot(k - 1);  // x0, y at plane k
-    const StepSlot& Sk = slot(k);      // x0, y at plane k + 1; y_{i-2}, u at plane k
+    const Slot& Sp = slot(k - 1);  // x0, y at plane k
+    const Slot& Sk = slot(k);      // x0, y at plane k + 1; y_{i-2}, u at plane k
     const long long c = (long long)k * sz + rowj + i;
     const V x_k = diffv(Sp.a[0][ty][lane], Sp.a[1][ty][lane]);
     const V x_kp = diffv(Sk.a[0][ty][lane], Sk.a[1][ty][lane]);
@@ -557,9 +569,9 @@ __global__ void __launch_bounds__(kStepBX* kStepBY, 2)
       }
     }
     const V ux = ldv(Sk.a[3][ty][lane]), uy = ldv(Sk.a[4][ty][lane]), uz = ldv(Sk.a[5][ty][lane]);
-    float xnext = __shfl_down_sync(0xffffffffu, x_k.v[0], 1);
-    float xprev = __shfl_up_sync(0xffffffffu, x_k.v[NV - 1], 1);
-    float uxprev = __shfl_up_sync(0xffffffffu, ux.v[NV - 1], 1);
+    T xnext = __shfl_down_sync(0xffffffffu, x_k.v[0], 1);
+    T xprev = __shfl_up_sync(0xffffffffu, x_k.v[NV - 1], 1);
+    T uxprev = __shfl_up_sync(0xffffffffu, ux.v[NV - 1], 1);
     if (need_p) xnext = Sp.xp[ty][0] - Sp.xp[ty][1];
     if (need_m) {
       xprev = Sp.xm[ty][0] - Sp.xm[ty][1];
@@ -571,21 +583,21 @@ __global__ void __launch_bounds__(kStepBX* kStepBY, 2)
     V ox, oy, oz, dv;
 #pragma unroll
     for (int e = 0; e < NV; ++e) {
-      const float xe = x_k.v[e];
-      const float xip = e + 1 < NV ? x_k.v[e + 1] : xnext;
-      const float xim = e > 0 ? x_k.v[e - 1] : xprev;
-      const float uxm = e > 0 ? ux.v[e - 1] : uxprev;
-      const float vx = (xip - xe) * hx + ux.v[e];
-      const float vy = (xjp.v[e] - xe) * hy + uy.v[e];
-      const float vz = (x_kp.v[e] - xe) * hz + uz.v[e];
-      const float zx = shrink(vx, thr), zy = shrink(vy, thr), zz = shrink(vz, thr);
-      const float gx = 2.0f * zx - vx, gy = 2.0f * zy - vy, gz = 2.0f * zz - vz;
-      const float vxm = (xe - xim) * hx + uxm;
-      const float vym = (xe - xjm.v[e]) * hy + uym.v[e];
-      const float vzm = (xe - x_km.v[e]) * hz + uz_km.v[e];
-      const float gxm = 2.0f * shrink(vxm, thr) - vxm;
-      const float gym = 2.0f * shrink(vym, thr) - vym;
-      const float gzm = 2.0f * shrink(vzm, thr) - vzm;
+      const T xe = x_k.v[e];
+      const T xip = e + 1 < NV ? x_k.v[e + 1] : xnext;
+      const T xim = e > 0 ? x_k.v[e - 1] : xprev;
+      const T uxm = e > 0 ? ux.v[e - 1] : uxprev;
+      const T vx = (xip - xe) * hx + ux.v[e];
+      const T vy = (xjp.v[e] - xe) * hy + uy.v[e];
+      const T vz = (x_kp.v[e] - xe) * hz + uz.v[e];
+      const T zx = shrink(vx, thr), zy = shrink(vy, thr), zz = shrink(vz, thr);
+      const T gx = T(2) * zx - vx, gy = T(2) * zy - vy, gz = T(2) * zz - vz;
+      const T vxm = (xe - xim) * hx + uxm;
+      const T vym = (xe - xjm.v[e]) * hy + uym.v[e];
+      const T vzm = (xe - x_km.v[e]) * hz + uz_km.v[e];
+      const T gxm = T(2) * shrink(vxm, thr) - vxm;
+      const T gym = T(2) * shrink(vym, thr) - vym;
+      const T gzm = T(2) * shrink(vzm, thr) - vzm;
       ox.v[e] = vx - zx;
       oy.v[e] = vy - zy;
       oz.v[e] = vz - zz;
@@ -668,7 +680,7 @@ template <typename T> struct TvVol {
   dim3 sgrid;
   int zchunk;
   bool vec, use_mult;
-  bool staged = false;  // k_tv_step_s for the full update (float, unweighted, 16-byte rows)
+  bool staged = false;  // k_tv_step_s for the full update (unweighted, 16-byte vectors)
   dim3 sgrid_s;
   int zchunk_s = 0;
   T hx, hy, hz, thr, scale;
@@ -706,12 +718,14 @@ void tv_alloc(qsm_ctx* ctx, TvVol<T>& v, const std::string& pre, const GridDims&
   v.zchunk = zchunk;
   v.sgrid = dim3(gbx, gby, (d.nz + zchunk - 1) / zchunk);
   size_t nblk = (size_t)v.sgrid.x * v.sgrid.y * v.sgrid.z;
-  if (v.vec) {
-    // staged stencil: about two waves of 2 blocks per SM, each block marching >= 4 planes
+  if (d.nx % Vec16<T>::n == 0) {
+    // staged stencil (16-byte vectors): about two waves of 2 blocks per SM, each block
+    // marching >= 4 planes
+    const int gbxs = (d.nx / Vec16<T>::n + kStepBX - 1) / kStepBX;
     const long long resident = 2LL * sm_count(ctx);
-    const long long zc = std::max<long long>(1, 2 * resident / ((long long)gbx * gby));
+    const long long zc = std::max<long long>(1, 2 * resident / ((long long)gbxs * gby));
     v.zchunk_s = (int)std::min<long long>(d.nz, std::max<long long>(4, (d.nz + zc - 1) / zc));
-    v.sgrid_s = dim3(gbx, gby, (d.nz + v.zchunk_s - 1) / v.zchunk_s);
+    v.sgrid_s = dim3(gbxs, gby, (d.nz + v.zchunk_s - 1) / v.zchunk_s);
     v.staged = true;
     nblk = std::max(nblk, (size_t)v.sgrid_s.x * v.sgrid_s.y * v.sgrid_s.z);
   }
@@ -763,11 +777,11 @@ void tv_setup(qsm_ctx* ctx, TvVol<T>& v, const std::string& pre, const GridDims&
 // iteration i with parity q = i % 2: reads y_{i-1} = yb[1-q], y_{i-2} = yb[q],
 // u = ub[1-q]; writes u' = ub[q], y_i = yb[q]
 template <typename T> void tv_step_launch(qsm_ctx* ctx, const TvVol<T>& v, int q, int check_only) {
-  if constexpr (std::is_same<T, float>::value) {
+  {
     if (v.staged && !v.w && !check_only) {
-      ensure_smem(k_tv_step_s<T>, kStepStagedSmem);
+      ensure_smem(k_tv_step_s<T>, step_staged_smem<T>());
       LaunchScope ls(ctx, "tv_step");
-      k_tv_step_s<T><<<v.sgrid_s, dim3(kStepBX, kStepBY), kStepStagedSmem, ctx->stream>>>(
+      k_tv_step_s<T><<<v.sgrid_s, dim3(kStepBX, kStepBY), step_staged_smem<T>(), ctx->stream>>>(
           v.d.nx, v.d.ny, v.d.nz, v.zchunk_s, v.hx, v.hy, v.hz, v.thr, v.x0, v.yb[1 - q], v.yb[q], v.ub[1 - q],
           v.ub[q], v.div, v.partials, v.st);
       ls.done();
