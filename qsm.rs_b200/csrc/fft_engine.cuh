@@ -301,6 +301,17 @@ template <int N, int TT, int R0, int R1, int R2 = 1> struct FixedPlan {
   X(64, 4, 16, 4, 1) X(96, 8, 16, 6, 1) X(128, 8, 16, 8, 1) X(160, 16, 16, 10, 1)                 \
   X(176, 16, 16, 11, 1) X(192, 16, 16, 12, 1) X(256, 16, 16, 16, 1) X(384, 26, 16, 8, 3)
 
+// Further 5- and 7-smooth lengths from 72 to 240 (the planner's own radices and threads
+// per pencil): compiled only for the passes of the TV-ADMM iteration, whose launchers
+// take the wide list (W = true), so that uneven clinical grids avoid the runtime engine
+// in the loop that runs hundreds of times per solve.
+#define QSM_FIXED_PLANS_WIDE(X)                                                                   \
+  X(72, 6, 12, 6, 1) X(75, 5, 15, 5, 1) X(80, 6, 16, 5, 1) X(81, 9, 9, 9, 1) X(90, 8, 15, 6, 1)   \
+  X(100, 10, 10, 10, 1) X(108, 12, 12, 9, 1) X(112, 8, 16, 7, 1) X(120, 8, 15, 8, 1)              \
+  X(125, 9, 5, 5, 5) X(135, 15, 15, 9, 1) X(144, 12, 12, 12, 1) X(150, 15, 15, 10, 1)             \
+  X(162, 18, 9, 9, 2) X(168, 12, 8, 7, 3) X(180, 15, 15, 12, 1) X(200, 14, 8, 5, 5)               \
+  X(216, 18, 12, 6, 3) X(224, 16, 16, 7, 2) X(225, 15, 15, 15, 1) X(240, 16, 16, 15, 1)
+
 // Full 1D transform of one pencil. DIR = -1 forward (exp(-2 pi i nk/n)), +1 inverse
 // (unnormalised).  tw points at the forward table W_n^k, k in [0, n).
 //

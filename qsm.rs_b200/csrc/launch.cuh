@@ -81,9 +81,9 @@ template <typename T> inline long long x_blocks(const Fft3<T>& f) {
   return (npairs + P - 1) / P;
 }
 
-// Compile-time X kernels (float) for the lengths of QSM_FIXED_PLANS; false when the
-// plan is not one of them.
-template <typename T, class Load>
+// Compile-time X kernels (float) for the lengths of QSM_FIXED_PLANS (and of
+// QSM_FIXED_PLANS_WIDE when W); false when the plan is not one of them.
+template <typename T, bool W, class Load>
 bool run_x_r2c_fixed(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* spec, const Load& ld, const int* done) {
   if constexpr (!std::is_same<T, float>::value) {
     return false;
@@ -103,12 +103,15 @@ bool run_x_r2c_fixed(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* spec, const Load
       return true;                                                                                 \
     }
     QSM_FIXED_PLANS(QSM_TRY_XR)
+    if constexpr (W) {
+      QSM_FIXED_PLANS_WIDE(QSM_TRY_XR)
+    }
 #undef QSM_TRY_XR
     return false;
   }
 }
 
-template <typename T, class Store>
+template <typename T, bool W, class Store>
 bool run_x_c2r_fixed(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* spec, const Store& st, const int* done) {
   if constexpr (!std::is_same<T, float>::value) {
     return false;
@@ -128,14 +131,17 @@ bool run_x_c2r_fixed(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* spec, cons
       return true;                                                                                 \
     }
     QSM_FIXED_PLANS(QSM_TRY_XC)
+    if constexpr (W) {
+      QSM_FIXED_PLANS_WIDE(QSM_TRY_XC)
+    }
 #undef QSM_TRY_XC
     return false;
   }
 }
 
-template <typename T, class Load>
+template <typename T, bool W = false, class Load>
 void run_x_r2c(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* spec, const Load& ld, const int* done) {
-  if (run_x_r2c_fixed<T>(ctx, f, spec, ld, done)) return;
+  if (run_x_r2c_fixed<T, W>(ctx, f, spec, ld, done)) return;
   using C = cplx_t<T>;
   const int Tt = x_block_t(f.px.T);
   const int P = x_pencils_per_block<T>(f.px.T);
@@ -147,9 +153,9 @@ void run_x_r2c(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* spec, const Load& ld, 
   ls.done();
 }
 
-template <typename T, class Store>
+template <typename T, bool W = false, class Store>
 void run_x_c2r(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* spec, const Store& st, const int* done) {
-  if (run_x_c2r_fixed<T>(ctx, f, spec, st, done)) return;
+  if (run_x_c2r_fixed<T, W>(ctx, f, spec, st, done)) return;
   using C = cplx_t<T>;
   const int Tt = x_block_t(f.px.T);
   const int P = x_pencils_per_block<T>(f.px.T);
@@ -257,7 +263,8 @@ template <typename T, class K> int yz_tile_width(K kernel, int n, int Tn) {
 }
 
 // Compile-time Y/Z kernels (float, 16-column tiles) for the axis lengths of
-// QSM_FIXED_PLANS; returns false when the plan is not one of them.
+// QSM_FIXED_PLANS (and QSM_FIXED_PLANS_WIDE when W); returns false when the plan is not
+// one of them.
 constexpr int kFxCols = 16;
 constexpr int kZmCols = 8;  // columns per tile of the fused Z pass
 template <class K> bool fx_launch_ok(qsm_ctx* ctx, K kern, int threads, size_t smem, unsigned* grid, long long work) {
@@ -275,7 +282,7 @@ template <class K> bool fx_launch_ok(qsm_ctx* ctx, K kern, int threads, size_t s
   return true;
 }
 
-template <typename T, int DIR, int AXIS>
+template <typename T, int DIR, int AXIS, bool W>
 bool run_yz_fixed(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst, const int* done) {
   if constexpr (!std::is_same<T, float>::value) {
     return false;
@@ -296,16 +303,19 @@ bool run_yz_fixed(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T
       return true;                                                                                \
     }
     QSM_FIXED_PLANS(QSM_TRY_YZ)
+    if constexpr (W) {
+      QSM_FIXED_PLANS_WIDE(QSM_TRY_YZ)
+    }
 #undef QSM_TRY_YZ
     return false;
   }
 }
 
-// AXIS 1 = y, 2 = z; DIR -1 forward, +1 inverse.
-template <typename T, int DIR, int AXIS, class Op>
+// AXIS 1 = y, 2 = z; DIR -1 forward, +1 inverse; W adds QSM_FIXED_PLANS_WIDE.
+template <typename T, int DIR, int AXIS, bool W = false, class Op>
 void run_yz(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst, const Op& op, const int* done) {
   if constexpr (IsPlainOp<Op>::value) {
-    if (run_yz_fixed<T, DIR, AXIS>(ctx, f, src, dst, done)) return;
+    if (run_yz_fixed<T, DIR, AXIS, W>(ctx, f, src, dst, done)) return;
   }
   const FftPlan1D& pl = (AXIS == 1) ? f.py : f.pz;
   const cplx_t<T>* tw = (AXIS == 1) ? f.twy : f.twz;
@@ -358,8 +368,9 @@ template <typename T> int zm_tile_width(int n, int Tn) {
   return 0;
 }
 
-// Z fused pass with a precomputed real multiplier array (spectrum layout).
-template <typename T>
+// Z fused pass with a precomputed real multiplier array (spectrum layout); W adds
+// QSM_FIXED_PLANS_WIDE.
+template <typename T, bool W = false>
 void run_z_fused_m(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst, const T* mult,
                    const int* done) {
   const FftPlan1D& pl = f.pz;
@@ -379,6 +390,9 @@ void run_z_fused_m(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<
       }                                                                                           \
     }
     QSM_FIXED_PLANS(QSM_TRY_ZM)
+    if constexpr (W) {
+      QSM_FIXED_PLANS_WIDE(QSM_TRY_ZM)
+    }
 #undef QSM_TRY_ZM
   }
   auto kern = k_z_fused_m<T>;

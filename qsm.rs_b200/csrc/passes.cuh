@@ -706,9 +706,15 @@ __global__ void __launch_bounds__(P* FP::T, (P * FP::T <= 256 ? 3 : 1))
 }
 
 // Compile-time form of k_z_fused_m (FP a FixedPlan, P columns per tile).  Both transforms are inlined,
-// so it is compiled for 512 threads per SM (128 registers): the 768-thread cap spills.
+// so it is compiled for 512 threads per SM (128 registers): the 768-thread cap spills.  A
+// block whose size is not a multiple of 32 still occupies whole warps, so the block
+// count per SM is taken on the warp-rounded size.
+template <int THREADS> constexpr int zm_min_blocks() {
+  constexpr int rounded = (THREADS + 31) / 32 * 32;
+  return rounded <= 512 ? 512 / rounded : 1;
+}
 template <typename T, class FP, int P>
-__global__ void __launch_bounds__(P* FP::T, (P * FP::T <= 512 ? 512 / (P * FP::T) : 1))
+__global__ void __launch_bounds__(P* FP::T, zm_min_blocks<P * FP::T>())
     k_z_fused_m_fx(Geom g, TileWalk w, const cplx_t<T>* __restrict__ twg, const cplx_t<T>* src, cplx_t<T>* dst,
                    const T* __restrict__ mult, const int* __restrict__ done) {
   using C = cplx_t<T>;

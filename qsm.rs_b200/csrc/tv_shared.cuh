@@ -798,15 +798,18 @@ template <typename T> void tv_step_launch(qsm_ctx* ctx, const TvVol<T>& v, int q
 }
 
 // y_i = Re IFFT(rho * sym(inv_a) * F(div)) into yb[q], skipped once the state is done
+// (compile-time passes for the wide length list; instantiated once, in tv_fft.cu)
 template <typename T> void tv_fft(qsm_ctx* ctx, const TvVol<T>& v, int q) {
   const int* done = &v.st->done;
-  run_x_r2c<T>(ctx, v.f, v.spec, LoadCast<T, T>{v.div, v.d.nx}, done);
-  run_yz<T, -1, 1>(ctx, v.f, v.spec, v.spec, OpId<T>{}, done);
-  if (v.use_mult) run_z_fused_m<T>(ctx, v.f, v.spec, v.spec, v.mult, done);
+  run_x_r2c<T, true>(ctx, v.f, v.spec, LoadCast<T, T>{v.div, v.d.nx}, done);
+  run_yz<T, -1, 1, true>(ctx, v.f, v.spec, v.spec, OpId<T>{}, done);
+  if (v.use_mult) run_z_fused_m<T, true>(ctx, v.f, v.spec, v.spec, v.mult, done);
   else run_z_fused<T>(ctx, v.f, v.spec, v.spec, v.mul, done);
-  run_yz<T, +1, 1>(ctx, v.f, v.spec, v.spec, OpId<T>{}, done);
-  run_x_c2r<T>(ctx, v.f, v.spec, StoreReal<T>{v.yb[q], v.d.nx, v.scale}, done);
+  run_yz<T, +1, 1, true>(ctx, v.f, v.spec, v.spec, OpId<T>{}, done);
+  run_x_c2r<T, true>(ctx, v.f, v.spec, StoreReal<T>{v.yb[q], v.d.nx, v.scale}, done);
 }
+extern template void tv_fft<float>(qsm_ctx*, const TvVol<float>&, int);
+extern template void tv_fft<double>(qsm_ctx*, const TvVol<double>&, int);
 
 template <typename T> void tv_iter(qsm_ctx* ctx, const TvVol<T>& v, int q) {
   tv_step_launch(ctx, v, q, 0);
