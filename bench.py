@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--one-shot", type=int, default=0, metavar="ITERS",
                     help="profiling aid: run one TV-ADMM solve of ITERS iterations (mixed) and exit")
     ap.add_argument("--one-shot-precision", default="mixed", choices=["mixed", "f64"])
+    ap.add_argument("--one-shot-dims", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
+                    help="one-shot on a seeded N(0, 0.01) field of this grid (full mask) instead of the phantom")
     return ap.parse_args()
 
 
@@ -61,13 +63,20 @@ def one_shot(args):
     import torch
     import qsmgpu
     from qsmgpu import Grid, inversion
-    f, mask = make_case(0)
+    dims = DIMS
+    if args.one_shot_dims:
+        dims = tuple(args.one_shot_dims)
+        n = dims[0] * dims[1] * dims[2]
+        f = np.random.default_rng(3).normal(0.0, 0.01, n)
+        mask = np.ones(n, np.uint8)
+    else:
+        f, mask = make_case(0)
     dev = torch.device("cuda", 0)
     d_f = torch.from_numpy(f.ravel()).to(dev)
     d_m = torch.from_numpy(mask.ravel()).to(dev)
     d_o = torch.empty(f.size, dtype=torch.float64, device=dev)
     with qsmgpu.Context(0, args.one_shot_precision) as ctx:
-        inversion.tv_admm_device(ctx, d_f.data_ptr(), d_m.data_ptr(), Grid.new(*DIMS), (0.0, 0.0, 1.0),
+        inversion.tv_admm_device(ctx, d_f.data_ptr(), d_m.data_ptr(), Grid.new(*dims), (0.0, 0.0, 1.0),
                                  inversion.TvParams(2e-4, 2e-2, 0.0, args.one_shot), d_o.data_ptr())
     torch.cuda.synchronize()
     print(f"one-shot ok: {args.one_shot} iterations, |chi|max={float(d_o.abs().max()):.4g}")
