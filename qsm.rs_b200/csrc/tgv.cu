@@ -404,19 +404,26 @@ __device__ __forceinline__ bool interior(int i, int j, int k, const Box& b) {
   return !(i == 0 || j == 0 || k == 0 || i + 1 >= b.bx || j + 1 >= b.by || k + 1 >= b.bz);
 }
 
+// The primal and dual kernels run 32x8 (x, y) tiles, each thread marching through
+// `zchunk` planes of one (i, j) column: no index division, and the y/z neighbours of a
+// voxel are the tile's own recent loads (L1) rather than another block's (L2).
+constexpr int kTgvBX = 32, kTgvBY = 8;
+
 // Dual update (tgv.rs:1157-1213).  q selects the buffers holding phi_, chi_, w_.
-__global__ void __launch_bounds__(256) k_tgv_dual(Box b, TgvArrays A, TgvScalars c, TgvConst K, int q,
-                                                  const TgvFlag* flag) {
+__global__ void __launch_bounds__(kTgvBX* kTgvBY) k_tgv_dual(Box b, TgvArrays A, TgvScalars c, TgvConst K, int q,
+                                                             int zchunk, const TgvFlag* flag) {
   if (flag->done) return;
-  const long long N = b.n(), sxy = (long long)b.bx * b.by;
+  const long long sxy = (long long)b.bx * b.by;
   const float* phb = A.phi[q];
   const float* chb = A.chi[q];
   const float* wbx = A.w[q][0];
   const float* wby = A.w[q][1];
   const float* wbz = A.w[q][2];
-  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < N; s += (long long)gridDim.x * blockDim.x) {
-    const unsigned r = (unsigned)(s / b.bx);
-    const int i = (int)(s - (long long)r * b.bx), j = (int)(r % (unsigned)b.by), k = (int)(r / (unsigned)b.by);
+  const int i = blockIdx.x * kTgvBX + threadIdx.x, j = blockIdx.y * kTgvBY + threadIdx.y;
+  if (i >= b.bx || j >= b.by) return;
+  const int kend = min(b.bz, (int)(blockIdx.z + 1) * zchunk);
+  for (int k = blockIdx.z * zchunk; k < kend; ++k) {
+    const long long s = (long long)k * sxy + (long long)j * b.bx + i;
     const bool in0 = A.m0[s] != 0, inm = A.me[s] != 0;
     const float cb = chb[s];
     if (in0) {
@@ -480,17 +487,19 @@ __global__ void __launch_bounds__(256) k_tgv_dual(Box b, TgvArrays A, TgvScalars
 // Primal update and extrapolation (tgv.rs:1215-1271).  Buffers [1-q] hold the current
 // iterate x (read), [q] the extrapolation consumed by the dual step (overwritten with
 // x_new); [1-q] then receives 2 x_new - x.
-__global__ void __launch_bounds__(256) k_tgv_primal(Box b, TgvArrays A, TgvScalars c, TgvConst K, int q,
-                                                    const TgvFlag* flag) {
+__global__ void __launch_bounds__(kTgvBX* kTgvBY) k_tgv_primal(Box b, TgvArrays A, TgvScalars c, TgvConst K, int q,
+                                                               int zchunk, const TgvFlag* flag) {
   if (flag->done) return;
-  const long long N = b.n(), sxy = (long long)b.bx * b.by;
+  const long long sxy = (long long)b.bx * b.by;
   // eta and q are only ever updated inside mask0 (k_tgv_dual) and start at zero, so
   // m0*eta = eta and m0*q = q
   auto eta_m = [&](long long t) { return A.eta[t]; };
   auto mq = [&](int comp, long long t) { return A.q[comp][t]; };
-  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < N; s += (long long)gridDim.x * blockDim.x) {
-    const unsigned r = (unsigned)(s / b.bx);
-    const int i = (int)(s - (long long)r * b.bx), j = (int)(r % (unsigned)b.by), k = (int)(r / (unsigned)b.by);
+  const int i = blockIdx.x * kTgvBX + threadIdx.x, j = blockIdx.y * kTgvBY + threadIdx.y;
+  if (i >= b.bx || j >= b.by) return;
+  const int kend = min(b.bz, (int)(blockIdx.z + 1) * zchunk);
+  for (int k = blockIdx.z * zchunk; k < kend; ++k) {
+    const long long s = (long long)k * sxy + (long long)j * b.bx + i;
     const bool in0 = A.m0[s] != 0, inm = A.me[s] != 0;
     // phi
     const float lap = in0 ? lap_neumann(eta_m, s, i, j, k, b, sxy, c) : 0.0f;
@@ -714,15 +723,20 @@ void tgv_device(qsm_ctx* ctx, const double* phase, const uint8_t* mask, const qs
   // before iteration t the current iterate sits in [t % 2] and its extrapolation in
   // [(t + 1) % 2]; the dual step reads the extrapolation
   const unsigned gblocks = grid1d(B);
+  // primal/dual tiles: ~16 blocks per SM in all, each marching zchunk planes
+  const unsigned tgx = (unsigned)((b.bx + kTgvBX - 1) / kTgvBX), tgy = (unsigned)((b.by + kTgvBY - 1) / kTgvBY);
+  const long long nzc = std::max<long long>(1, 16LL * sm_count(ctx) / ((long long)tgx * tgy));
+  const int zchunk = (int)((b.bz + nzc - 1) / nzc);
+  const dim3 tgrid(tgx, tgy, (unsigned)((b.bz + zchunk - 1) / zchunk)), tblock(kTgvBX, kTgvBY);
   auto one_iter = [&](size_t t) {
     const int q = (int)((t + 1) % 2);
     {
       LaunchScope ls(ctx, "tgv_dual");
-      k_tgv_dual<<<gblocks, 256, 0, ctx->stream>>>(b, A, c, K, q, flag);
+      k_tgv_dual<<<tgrid, tblock, 0, ctx->stream>>>(b, A, c, K, q, zchunk, flag);
       ls.done();
     }
     LaunchScope ls(ctx, "tgv_primal");
-    k_tgv_primal<<<gblocks, 256, 0, ctx->stream>>>(b, A, c, K, q, flag);
+    k_tgv_primal<<<tgrid, tblock, 0, ctx->stream>>>(b, A, c, K, q, zchunk, flag);
     ls.done();
   };
   auto check = [&](size_t t) {
