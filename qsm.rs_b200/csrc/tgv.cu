@@ -484,10 +484,12 @@ __global__ void __launch_bounds__(kTgvBX* kTgvBY) k_tgv_dual(Box b, TgvArrays A,
   }
 }
 
-// Primal update and extrapolation (tgv.rs:1215-1271).  Buffers [1-q] hold the current
+// Primal update and extrapolation (tgv.rs:1215-1271).  Compiled for six blocks per SM
+// (<= 42 registers): more columns in flight hide its dependent loads better than the
+// unbounded 43-register form (555 vs 712 us per launch at a 23 M-voxel box).  Buffers [1-q] hold the current
 // iterate x (read), [q] the extrapolation consumed by the dual step (overwritten with
 // x_new); [1-q] then receives 2 x_new - x.
-__global__ void __launch_bounds__(kTgvBX* kTgvBY) k_tgv_primal(Box b, TgvArrays A, TgvScalars c, TgvConst K, int q,
+__global__ void __launch_bounds__(kTgvBX* kTgvBY, 6) k_tgv_primal(Box b, TgvArrays A, TgvScalars c, TgvConst K, int q,
                                                                int zchunk, const TgvFlag* flag) {
   if (flag->done) return;
   const long long sxy = (long long)b.bx * b.by;
