@@ -85,7 +85,7 @@ template <typename T> inline long long x_blocks(const Fft3<T>& f) {
 // QSM_FIXED_PLANS_WIDE when W); false when the plan is not one of them.
 template <typename T, bool W, class Load>
 bool run_x_r2c_fixed(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* spec, const Load& ld, const int* done) {
-  if constexpr (!std::is_same<T, float>::value) {
+  if constexpr (!std::is_same<T, float>::value && !W) {
     return false;
   } else {
     using C = cplx_t<T>;
@@ -113,7 +113,7 @@ bool run_x_r2c_fixed(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* spec, const Load
 
 template <typename T, bool W, class Store>
 bool run_x_c2r_fixed(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* spec, const Store& st, const int* done) {
-  if constexpr (!std::is_same<T, float>::value) {
+  if constexpr (!std::is_same<T, float>::value && !W) {
     return false;
   } else {
     using C = cplx_t<T>;
