@@ -270,7 +270,7 @@ void vsharp_impl(qsm_ctx* ctx, const GridDims& d, const double* field, const uin
     double2* Sr = (idx == 0) ? S0 : S;
     smv_spectrum(ctx, f64, d, radii[idx], Sr);
     erode_smv(ctx, f64, d, Fm, Sr, delta, eroded);
-    run_yz<T, +1, 2>(ctx, f, Ff, tmp, OpMulS<T>{Sr, 1}, nullptr);
+    run_yz<T, +1, 2, true>(ctx, f, Ff, tmp, OpMulS<T>{Sr, 1}, nullptr);
     run_yz<T, +1, 1>(ctx, f, tmp, tmp, OpId<T>{}, nullptr);
     run_x_c2r<T>(ctx, f, tmp, StoreSelect<T>{eroded, out_mask, local, d.nx, scale}, nullptr);
   }

@@ -772,15 +772,17 @@ void ilsqr_impl(qsm_ctx* ctx, const GridDims& d, const double* f, const uint8_t*
   run_x_full<T, -1, 0>(ctx, ff, LoadRealProduct<double, T>{f, wl, d.nx}, MidId<T>{}, StoreSpecRow<T>{t, ff.g.pitch},
                        nullptr, "fft_x_c2c");
   run_yz<T, -1, 1>(ctx, ff, t, t, OpId<T>{}, nullptr);
-  run_yz_acc<T, -1, 2>(ctx, ff, t, ub, OpLsqrOut<T>{K, nullptr, lst, 2}, partials, counter, nullptr, "fft_z_lsqr");
+  run_yz_acc<T, -1, 2, true>(ctx, ff, t, ub, OpLsqrOut<T>{K, nullptr, lst, 2}, partials, counter, nullptr, "fft_z_lsqr");
   // y = A(s*x) written to dst with the given epilogue mode
   auto apply_a = [&](const C* x, const double* s, C* dst, const C* old, int mode) {
+    // (the staged runtime pass: evaluating the dipole scale inside a direct-fetch first
+    // stage ran 309 us against 256 us at 384x384x256)
     run_yz<T, +1, 2>(ctx, ff, x, t, OpScaleD<T>{K, s}, ldone);
     run_yz<T, +1, 1>(ctx, ff, t, t, OpId<T>{}, ldone);
     run_x_full<T, +1, -1>(ctx, ff, LoadSpecRow<T>{t, ff.g.pitch}, MidWeightRe<T>{wl, d.nx, invn},
                           StoreSpecRow<T>{t, ff.g.pitch}, ldone, "fft_x_lsqr");
     run_yz<T, -1, 1>(ctx, ff, t, t, OpId<T>{}, ldone);
-    run_yz_acc<T, -1, 2>(ctx, ff, t, dst, OpLsqrOut<T>{K, old, lst, mode}, partials, counter, ldone, "fft_z_lsqr");
+    run_yz_acc<T, -1, 2, true>(ctx, ff, t, dst, OpLsqrOut<T>{K, old, lst, mode}, partials, counter, ldone, "fft_z_lsqr");
   };
   // v = A^H u, alpha; w = v
   apply_a(ub, &lst->su, vb, nullptr, 3);

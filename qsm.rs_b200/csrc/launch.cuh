@@ -311,11 +311,49 @@ bool run_yz_fixed(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T
   }
 }
 
-// AXIS 1 = y, 2 = z; DIR -1 forward, +1 inverse; W adds QSM_FIXED_PLANS_WIDE.
+constexpr int kMaxPersistentBlocks = 4096;
+
+// Compile-time Y/Z pass that carries an operator (k_pass_yz_dx_op), float, lengths of
+// QSM_FIXED_PLANS; ACC as in run_yz_acc.  Returns false when the plan is not one of them.
+template <typename T, int DIR, int AXIS, bool ACC, class Op>
+bool run_yz_op_fixed(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst, const Op& op,
+                     double* partials, unsigned* counter, const int* done, const char* name) {
+  if constexpr (!std::is_same<T, float>::value) {
+    return false;
+  } else {
+    const FftPlan1D& pl = (AXIS == 1) ? f.py : f.pz;
+    const cplx_t<T>* tw = (AXIS == 1) ? f.twy : f.twz;
+#define QSM_TRY_YZO(N_, T_, R0_, R1_, R2_)                                                         \
+    if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(pl) && kFxCols * T_ <= 1024) {                   \
+      using FP = FixedPlan<N_, T_, R0_, R1_, R2_>;                                                \
+      auto kern = k_pass_yz_dx_op<T, DIR, AXIS, FP, kFxCols, Op, ACC>;                            \
+      const size_t smem = dx_smem<T>(N_, kFxCols);                                                \
+      const TileWalk w = tile_walk(f, AXIS, kFxCols);                                             \
+      unsigned grid = 0;                                                                          \
+      if (!fx_launch_ok(ctx, kern, kFxCols * T_, smem, &grid, w.ntiles)) return false;            \
+      if (ACC && grid > (unsigned)kMaxPersistentBlocks) return false;                             \
+      LaunchScope ls(ctx, name);                                                                  \
+      kern<<<grid, dim3(kFxCols, T_), smem, ctx->stream>>>(f.g, w, tw, src, dst, op, partials, counter, done); \
+      ls.done();                                                                                  \
+      return true;                                                                                \
+    }
+    QSM_FIXED_PLANS(QSM_TRY_YZO)
+#undef QSM_TRY_YZO
+    return false;
+  }
+}
+
+// AXIS 1 = y, 2 = z; DIR -1 forward, +1 inverse; W adds QSM_FIXED_PLANS_WIDE for plain
+// passes and the compile-time operator pass (QSM_FIXED_PLANS) for the others.
 template <typename T, int DIR, int AXIS, bool W = false, class Op>
 void run_yz(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst, const Op& op, const int* done) {
   if constexpr (IsPlainOp<Op>::value) {
     if (run_yz_fixed<T, DIR, AXIS, W>(ctx, f, src, dst, done)) return;
+  } else if constexpr (W) {
+    if (run_yz_op_fixed<T, DIR, AXIS, false>(ctx, f, src, dst, op, nullptr, nullptr, done,
+                                             AXIS == 1 ? (DIR < 0 ? "fft_y_fwd" : "fft_y_inv")
+                                                       : (DIR < 0 ? "fft_z_fwd" : "fft_z_inv")))
+      return;
   }
   const FftPlan1D& pl = (AXIS == 1) ? f.py : f.pz;
   const cplx_t<T>* tw = (AXIS == 1) ? f.twy : f.twz;
@@ -331,10 +369,12 @@ void run_yz(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst
 
 // Y/Z pass with an FP64 accumulation in its post hook (k_pass_yz_acc).  `partials`
 // holds at least kMaxPersistentBlocks doubles; `counter` is 0 between launches.
-constexpr int kMaxPersistentBlocks = 4096;
-template <typename T, int DIR, int AXIS, class Op>
+template <typename T, int DIR, int AXIS, bool W = false, class Op>
 void run_yz_acc(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst, const Op& op,
                 double* partials, unsigned* counter, const int* done, const char* name) {
+  if constexpr (W) {
+    if (run_yz_op_fixed<T, DIR, AXIS, true>(ctx, f, src, dst, op, partials, counter, done, name)) return;
+  }
   const FftPlan1D& pl = (AXIS == 1) ? f.py : f.pz;
   const cplx_t<T>* tw = (AXIS == 1) ? f.twy : f.twz;
   auto kern = k_pass_yz_acc<T, DIR, AXIS, Op>;

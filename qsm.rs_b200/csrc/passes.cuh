@@ -705,6 +705,53 @@ __global__ void __launch_bounds__(P* FP::T, (P * FP::T <= 256 ? 3 : 1))
   }
 }
 
+// k_pass_yz_dx with the pass's operator applied as elements are fetched (op.pre) and
+// stored (op.post), for passes that carry one (k-space scalings, fused LSQR epilogues).
+// ACC: op.post also adds to a per-thread FP64 sum that is reduced over the grid at the
+// end (grid_sum_last) and handed to op.last, as in k_pass_yz_acc.  The element order of
+// that sum follows the fixed plan's last stage, so the total is deterministic for a
+// given launch shape.
+template <typename T, int DIR, int AXIS, class FP, int P, class Op, bool ACC>
+__global__ void __launch_bounds__(P* FP::T, (P * FP::T <= 256 ? 3 : 1))
+    k_pass_yz_dx_op(Geom g, TileWalk w, const cplx_t<T>* __restrict__ twg, const cplx_t<T>* src, cplx_t<T>* dst,
+                    Op op, double* __restrict__ partials, unsigned* counter, const int* __restrict__ done) {
+  using C = cplx_t<T>;
+  constexpr int n = FP::n;
+  if (done != nullptr && *done) return;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* tw = reinterpret_cast<C*>(smraw);
+  C* buf = tw + ((n + 7) & ~7);
+  const int tid = threadIdx.x + threadIdx.y * P;
+  for (int i = tid; i < n; i += P * FP::T) tw[i] = twg[i];
+  const int px = threadIdx.x;
+  const int t = threadIdx.y;
+  SAStridedC<P> sa;
+  C* sp = buf + px;
+  double acc[1] = {0.0};
+  for (int tile = blockIdx.x; tile < w.ntiles; tile += gridDim.x) {
+    const int tx = tile % w.ntx, outer = tile / w.ntx;
+    const int col = tx * P + px;
+    const bool active = col < g.nxh;
+    const long long base = col + (long long)outer * w.ostride;
+    auto fetch = [&](int e) -> C {
+      const long long idx = base + e * w.estride;
+      const C v = src[idx];
+      return (AXIS == 1) ? op.pre(v, col, e, outer, idx) : op.pre(v, col, outer, e, idx);
+    };
+    auto emit = [&](int e, C v) {
+      const long long idx = base + e * w.estride;
+      if constexpr (ACC)
+        dst[idx] = (AXIS == 1) ? op.post(v, col, e, outer, idx, acc[0]) : op.post(v, col, outer, e, idx, acc[0]);
+      else
+        dst[idx] = (AXIS == 1) ? op.post(v, col, e, outer, idx) : op.post(v, col, outer, e, idx);
+    };
+    FP::template run<DIR>(t, active, sp, sa, tw, fetch, emit);
+  }
+  if constexpr (ACC) {
+    if (grid_sum_last<1>(acc, partials, counter) && tid == 0) op.last(acc[0]);
+  }
+}
+
 // Compile-time form of k_z_fused_m (FP a FixedPlan, P columns per tile).  Both transforms are inlined,
 // so it is compiled for 512 threads per SM (128 registers): the 768-thread cap spills.  A
 // block whose size is not a multiple of 32 still occupies whole warps, so the block
