@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--one-shot-precision", default="mixed", choices=["mixed", "f64"])
     ap.add_argument("--one-shot-dims", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
                     help="one-shot on a seeded N(0, 0.01) field of this grid (full mask) instead of the phantom")
+    ap.add_argument("--one-shot-tgv", type=int, nargs=4, default=None, metavar=("NX", "NY", "NZ", "ITERS"),
+                    help="profiling aid: one TGV solve (ellipsoid mask, seeded uniform wrapped phase, 0.6 mm) and exit")
     return ap.parse_args()
 
 
@@ -80,6 +82,32 @@ def one_shot(args):
                                  inversion.TvParams(2e-4, 2e-2, 0.0, args.one_shot), d_o.data_ptr())
     torch.cuda.synchronize()
     print(f"one-shot ok: {args.one_shot} iterations, |chi|max={float(d_o.abs().max()):.4g}")
+
+
+def one_shot_tgv(args):
+    """Small, self-contained TGV run for ncu captures: ellipsoid mask (semi-axes 0.42/0.45/0.40
+    of the grid), phase uniform in [-3, 3] rad inside it, 0.6 mm voxels, tol 0."""
+    import torch
+    import qsmgpu
+    from qsmgpu import Grid, inversion
+    nx, ny, nz, iters = args.one_shot_tgv
+    dev = torch.device("cuda", 0)
+    z, y, x = torch.meshgrid(torch.arange(nz, device=dev, dtype=torch.float32),
+                             torch.arange(ny, device=dev, dtype=torch.float32),
+                             torch.arange(nx, device=dev, dtype=torch.float32), indexing="ij")
+    cx, cy, cz = (nx - 1) / 2, (ny - 1) / 2, (nz - 1) / 2
+    mask = (((x - cx) / (0.42 * nx)) ** 2 + ((y - cy) / (0.45 * ny)) ** 2 + ((z - cz) / (0.40 * nz)) ** 2) < 1
+    m8 = mask.reshape(-1).to(torch.uint8).contiguous()
+    g = torch.Generator(device=dev).manual_seed(1)
+    ph = ((torch.rand(nx * ny * nz, generator=g, device=dev, dtype=torch.float64) * 2 - 1) * 3.0 * m8.double())
+    ph = ph.contiguous()
+    out = torch.empty_like(ph)
+    with qsmgpu.Context(0, "mixed") as ctx:
+        inversion.tgv_qsm_device(ctx, ph.data_ptr(), m8.data_ptr(), Grid.new(nx, ny, nz, 0.6, 0.6, 0.6),
+                                 inversion.TgvParams(iterations=iters, tol=0.0, fieldstrength=3.0, te=0.020),
+                                 (0.0, 0.0, 1.0), out.data_ptr())
+    torch.cuda.synchronize()
+    print(f"one-shot tgv ok: {iters} iterations, |chi|max={float(out.abs().max()):.4g}")
 
 
 def make_case(seed):
@@ -510,6 +538,9 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.one_shot_tgv:
+        one_shot_tgv(args)
         return
     if args.one_shot:
         one_shot(args)
