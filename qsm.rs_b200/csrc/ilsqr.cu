@@ -779,7 +779,7 @@ void ilsqr_impl(qsm_ctx* ctx, const GridDims& d, const double* f, const uint8_t*
     // stage ran 309 us against 256 us at 384x384x256)
     run_yz<T, +1, 2>(ctx, ff, x, t, OpScaleD<T>{K, s}, ldone);
     run_yz<T, +1, 1>(ctx, ff, t, t, OpId<T>{}, ldone);
-    run_x_full<T, +1, -1>(ctx, ff, LoadSpecRow<T>{t, ff.g.pitch}, MidWeightRe<T>{wl, d.nx, invn},
+    run_x_full<T, +1, -1, true>(ctx, ff, LoadSpecRow<T>{t, ff.g.pitch}, MidWeightRe<T>{wl, d.nx, invn},
                           StoreSpecRow<T>{t, ff.g.pitch}, ldone, "fft_x_lsqr");
     run_yz<T, -1, 1>(ctx, ff, t, t, OpId<T>{}, ldone);
     run_yz_acc<T, -1, 2, true>(ctx, ff, t, dst, OpLsqrOut<T>{K, old, lst, mode}, partials, counter, ldone, "fft_z_lsqr");

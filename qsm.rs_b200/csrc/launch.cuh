@@ -182,10 +182,30 @@ template <typename T> struct MidId {
 };
 
 // X pass over full complex rows: load -> FFT(D1) -> mid -> FFT(D2) -> store.
-template <typename T, int D1, int D2, class Load, class Mid, class Store>
+// W: a hot loop's pass; with both transforms in float it takes the compile-time kernel
+// (k_x_full_fx) for the lengths of QSM_FIXED_PLANS.
+template <typename T, int D1, int D2, bool W = false, class Load, class Mid, class Store>
 void run_x_full(qsm_ctx* ctx, const Fft3<T>& f, const Load& ld, const Mid& mid, const Store& st, const int* done,
                 const char* name) {
   using C = cplx_t<T>;
+  if constexpr (W && D1 != 0 && D2 != 0 && std::is_same<T, float>::value) {
+#define QSM_TRY_XF(N_, T_, R0_, R1_, R2_)                                                          \
+    if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(f.px)) {                                         \
+      using FP = FixedPlan<N_, T_, R0_, R1_, R2_>;                                                 \
+      const int Tt = x_block_t(T_);                                                                \
+      const int P = x_pencils_per_block<T>(T_);                                                    \
+      const size_t smem = (size_t)(N_ + P * x_rowlen<T>(N_)) * sizeof(C);                          \
+      auto kern = k_x_full_fx<T, FP, D1, D2, Load, Mid, Store>;                                    \
+      ensure_smem(kern, smem);                                                                     \
+      const long long blocks = ((long long)f.g.nrows() + P - 1) / P;                              \
+      LaunchScope ls(ctx, name);                                                                   \
+      kern<<<(unsigned)blocks, dim3(Tt, P), smem, ctx->stream>>>(f.g, f.twx, ld, mid, st, done);   \
+      ls.done();                                                                                   \
+      return;                                                                                      \
+    }
+    QSM_FIXED_PLANS(QSM_TRY_XF)
+#undef QSM_TRY_XF
+  }
   if ((f.px.n + f.px.T - 1) / f.px.T > kFftEmax)
     throw QsmError(QSM_ERR_UNSUPPORTED_SIZE, "x length outside the per-thread register budget");
   const int Tt = x_block_t(f.px.T);

@@ -183,6 +183,41 @@ __global__ void k_x_full(Geom g, const __grid_constant__ FftPlan1D pl, const cpl
   st.finish();
 }
 
+// Compile-time form of k_x_full with both transforms (FP a FixedPlan): the first
+// transform's first stage fetches through the loader, its last stage applies the mid
+// hook on the way into shared memory, and the second transform's last stage hands its
+// values straight to the store functor, so a row makes two shared-memory round trips
+// fewer than in k_x_full.  Every element of a row is fetched in the first stage, before
+// any store of that row, so the loader and the store may address the same rows.
+template <typename T, class FP, int D1, int D2, class Load, class Mid, class Store>
+__global__ void k_x_full_fx(Geom g, const cplx_t<T>* __restrict__ twg, Load ld, Mid mid, Store st0,
+                            const int* __restrict__ done) {
+  using C = cplx_t<T>;
+  constexpr int N = FP::n, TT = FP::T;
+  static_assert(D1 != 0 && D2 != 0, "both transforms");
+  if (done != nullptr && *done) return;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* tw = reinterpret_cast<C*>(smraw);
+  C* sm = tw + N;
+  const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+  for (int i = tid; i < N; i += blockDim.x * blockDim.y) tw[i] = twg[i];
+  const int t = threadIdx.x;
+  const int row = blockIdx.x * blockDim.y + threadIdx.y;
+  const bool active = row < g.nrows() && t < TT;
+  C* sp = sm + threadIdx.y * x_rowlen<T>(N);
+  SAPadded<PadG<T>::G> sa;
+  Store st = st0;
+  auto fetch_g = [&](int e) -> C { return ld(row, e); };
+  auto emit_mid = [&](int e, C v) { sp[sa(e)] = mid(v, row, e); };
+  auto fetch_s = [&](int e) -> C { return sp[sa(e)]; };
+  auto emit_g = [&](int e, C v) { st(row, e, v); };
+  // the first transform's last stage ends with a block barrier, so the second one's
+  // first stage sees every mid-weighted element
+  FP::template run<D1>(t, active, sp, sa, tw, fetch_g, emit_mid);
+  FP::template run<D2>(t, active, sp, sa, tw, fetch_s, emit_g);
+  st.finish();
+}
+
 // ---------------------------------------------------------------------------
 // X inverse: half spectrum -> real rows.  blockDim = (Tb, P) as for k_x_r2c.
 // A thread loads at most 9 half-spectrum entries per row (nx/2+1 <= 9T), issued as
