@@ -112,17 +112,7 @@ def one_shot_tgv(args):
 
 def make_case(seed):
     from qsmgpu import phantom
-    nx, ny, nz = DIMS
-    rng = np.random.default_rng(seed)
-    shape = (nz, ny, nx)
-    mask = phantom.ellipsoid_mask(shape, (100.0, 120.0, 75.0))
-    chi = np.zeros(shape)
-    ctr = ((nx - 1) / 2, (ny - 1) / 2, (nz - 1) / 2)
-    box = [(ctr[0] - 60, ctr[0] + 60), (ctr[1] - 72, ctr[1] + 72), (ctr[2] - 45, ctr[2] + 45)]
-    phantom.add_ellipsoids(chi, rng, 12, box)
-    chi *= mask
-    f = phantom.forward_field(chi) + rng.normal(0.0, 0.01, size=shape) * mask
-    return np.ascontiguousarray(f), np.ascontiguousarray(mask)
+    return phantom.brain_tv_case(seed, DIMS)
 
 
 class ClockSampler:

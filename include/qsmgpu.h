@@ -36,7 +36,7 @@ typedef enum {
   QSM_OK = 0,
   QSM_ERR_INVALID_ARGUMENT = 1, /* null pointer, non-finite or out-of-range parameter */
   QSM_ERR_DIMENSION_MISMATCH = 2, /* PipelineError::DimensionMismatch (src/pipeline/config.rs:343-368) */
-  QSM_ERR_UNSUPPORTED_SIZE = 3, /* an axis length with a prime factor > 13, or too large */
+  QSM_ERR_UNSUPPORTED_SIZE = 3, /* an axis length above 4096, or above 2048 with a prime factor > 13 */
   QSM_ERR_ALLOC = 4,
   QSM_ERR_CUDA = 5,
   QSM_ERR_INVALID_CONFIG = 6, /* PipelineError::InvalidConfig */
@@ -84,7 +84,27 @@ QSM_API qsm_status qsm_ctx_profile_reset(qsm_ctx* ctx);
 QSM_API size_t qsm_ctx_profile_count(qsm_ctx* ctx);
 QSM_API qsm_status qsm_ctx_profile_entry(qsm_ctx* ctx, size_t i, char* name, size_t name_cap, uint64_t* launches,
                                          double* total_ms);
-/* 1 when every axis length of `grid` has a transform plan (factors 2..13). */
+/* Which FFT pass kernels a context launches.  QSM_PLANS_COMPILED (the default) takes
+ * the compile-time pass kernel wherever an axis length has one (loop bounds, radices and
+ * shared-memory addressing folded into constants) and the runtime Stockham engine
+ * elsewhere.  QSM_PLANS_RUNTIME takes the runtime engine for every pass: the same plan
+ * and radices, so results agree to rounding.  No reference counterpart (rustfft has one
+ * transform per length); tests use it to pin each compile-time pass against the runtime
+ * engine. */
+typedef enum { QSM_PLANS_COMPILED = 0, QSM_PLANS_RUNTIME = 1 } qsm_plan_mode;
+QSM_API qsm_status qsm_ctx_set_plan_mode(qsm_ctx* ctx, int mode);
+QSM_API int qsm_ctx_get_plan_mode(const qsm_ctx* ctx);
+/* Arithmetic of the Krylov solvers inside iLSQR (its LSQR and LSMR steps) in a mixed
+ * context; no reference counterpart.  QSM_PRECISION_F64 (the default) runs their vectors
+ * and operator transforms in double: the reference stops LSQR after 50 iterations short
+ * of its tolerance, so its result is the truncated Krylov iterate, and float rounding in
+ * the operator moves that iterate by ~1e-3 (amplified about a thousandfold).
+ * QSM_PRECISION_MIXED runs them in float with FP64 norms and recurrences (faster, about
+ * 2e-3 relative L2 from the reference).  An FP64 context always runs double. */
+QSM_API qsm_status qsm_ctx_set_krylov_precision(qsm_ctx* ctx, int precision);
+QSM_API int qsm_ctx_get_krylov_precision(const qsm_ctx* ctx);
+/* 1 when every axis length of `grid` has a transform plan: lengths up to 4096 whose prime
+ * factors are at most 13, and any length up to 2048 (a Bluestein transform). */
 QSM_API int qsm_grid_supported(const qsm_grid* grid);
 
 /* ---------------------------------------------------------------- params --- */
@@ -163,6 +183,17 @@ QSM_API qsm_status qsm_tv_admm_batch(qsm_ctx* ctx, const qsm_volume* volumes, si
 QSM_API qsm_status qsm_tv_admm_batch_device(qsm_ctx* ctx, const qsm_volume* volumes, size_t n,
                                             const qsm_tv_params* params, qsm_progress_fn progress, void* user,
                                             size_t* out_iterations);
+/* Placement of a batch over n_parts GPUs (no counterpart in the reference, which solves
+ * one volume per call on one host).  Volumes are independent, so a batch shards with no
+ * exchange: each GPU (one process or context per GPU) solves the volumes placed on it as
+ * one batched call, and the results are gathered on the host at the end.  Placement is
+ * longest-processing-time-first on cost N*log2(N)*iterations (N = voxels; iterations may
+ * be NULL for equal counts): volumes in decreasing cost (ties in batch order), each on
+ * the part with the least total cost so far (ties to the lowest index).  out_part[b]
+ * receives volume b's part; out_load (may be NULL) the n_parts total costs.  Host only:
+ * needs no GPU and no context. */
+QSM_API qsm_status qsm_batch_partition(const qsm_grid* grids, const size_t* iterations, size_t n, size_t n_parts,
+                                       uint32_t* out_part, double* out_load);
 /* inversion::tkd over a batch of volumes (no counterpart in the reference). */
 QSM_API qsm_status qsm_tkd_batch_device(qsm_ctx* ctx, const qsm_volume* volumes, size_t n,
                                         const qsm_tkd_params* params);
@@ -213,8 +244,10 @@ QSM_API qsm_status qsm_tkd_device(qsm_ctx* ctx, const double* d_local_field, con
  * is a 48 MiB array in the library's own device memory (held by every GPU that loads
  * the library); volumes whose scratch exceeds it (above about 160^3) return
  * QSM_ERR_UNSUPPORTED_SIZE.  Calls share that array, so calls that overlap on the GPU
- * race and must be serialised by the caller.  The first call on a device resolves
- * the array's address and should come before any stream capture. */
+ * race and must be serialised by the caller.  Every call resolves the array's address
+ * on the current device.  The call uploads small tables and synchronises its stream,
+ * so it must never be called while that stream is capturing a CUDA graph (refused with
+ * QSM_ERR_INVALID_ARGUMENT). */
 QSM_API qsm_status qsm_tkd_device_noalloc(const double* d_local_field, const uint8_t* d_mask, const qsm_grid* grid,
                                           const double bdir[3], const qsm_tkd_params* params, double* d_out_chi,
                                           void* stream);

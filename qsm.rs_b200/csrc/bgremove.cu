@@ -435,7 +435,7 @@ void ismv_impl(qsm_ctx* ctx, const GridDims& d, const double* field, const uint8
     ls.done();
   }
   const int* done = &st->done;
-  const bool use_m = zm_tile_width<T>(d.nz, f.pz.T) > 0;
+  const bool use_m = zm_tile_width<T>(d.nz, f.pz.m, f.pz.T) > 0;
   const T scale = (T)(1.0 / (double)N);
   const int maxi = (int)std::min<size_t>(p.max_iter, (size_t)1 << 30);
   // iteration k reads fb[(k-1) % 2] and writes fb[k % 2]

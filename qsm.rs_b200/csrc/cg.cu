@@ -221,7 +221,7 @@ size_t cg_normal_impl(qsm_ctx* ctx, const GridDims& d, const T* Kh, const T* w, 
     h2d(ctx, st, &s0, sizeof(s0));
   }
   const int* done = &st->done;
-  const bool use_m = zm_tile_width<T>(d.nz, f.pz.T) > 0;
+  const bool use_m = zm_tile_width<T>(d.nz, f.pz.m, f.pz.T) > 0;
   const T invn = (T)(1.0 / (double)N);
   const T lam = (T)lambda;
   // x = x0
@@ -333,7 +333,7 @@ void resharp_impl(qsm_ctx* ctx, const GridDims& d, const double* field, const ui
     ls.done();
   }
   // b = H^T H field (resharp.rs:84-85)
-  const bool use_m = zm_tile_width<T>(d.nz, f.pz.T) > 0;
+  const bool use_m = zm_tile_width<T>(d.nz, f.pz.m, f.pz.T) > 0;
   const T invn = (T)(1.0 / (double)N);
   k_filter<T>(ctx, f, spec, Kh, use_m, LoadImg<T>{fld, d.nx}, StoreWeighted<T>{t, w, d.nx, invn}, nullptr);
   k_filter<T>(ctx, f, spec, Kh, use_m, LoadImg<T>{t, d.nx}, StoreWeighted<T>{b, nullptr, d.nx, invn}, nullptr);

@@ -49,28 +49,60 @@ FftPlan1D plan_or_throw(int n) {
   FftPlan1D pl;
   if (!make_fft_plan(n, &pl))
     throw QsmError(QSM_ERR_UNSUPPORTED_SIZE,
-                   "axis length " + std::to_string(n) + " has no transform plan (prime factors must be <= 13, n <= " +
-                       std::to_string(kFftMaxLen) + ")");
+                   "axis length " + std::to_string(n) + " has no transform plan (n <= " + std::to_string(kFftMaxLen) +
+                       ", and n <= " + std::to_string(kBluesteinMaxLen) + " when n has a prime factor above 13)");
   return pl;
 }
 
-const void* twiddle_table(qsm_ctx* ctx, int n, bool dbl) {
-  const long long key = (long long)n * 2 + (dbl ? 1 : 0);
-  auto it = ctx->twiddles.find(key);
-  if (it != ctx->twiddles.end()) return it->second;
-  size_t elem = dbl ? sizeof(double2) : sizeof(float2);
-  std::vector<unsigned char> host(elem * (size_t)n);
-  for (int k = 0; k < n; ++k) {
-    // forward twiddle exp(-2 pi i k / n)
-    double c = cos2pi(k, n), s = -sin2pi(k, n);
+std::vector<unsigned char> transform_table(const FftPlan1D& pl, bool dbl) {
+  const int n = pl.n, m = pl.m;
+  const size_t elem = dbl ? sizeof(double2) : sizeof(float2);
+  const size_t count = (size_t)m + (m != n ? (size_t)n + (size_t)m : 0);
+  std::vector<unsigned char> host(elem * count);
+  auto put = [&](size_t i, double re, double im) {
     if (dbl) {
-      double2 v = make_double2(c, s);
-      std::memcpy(&host[elem * k], &v, elem);
+      const double2 v = make_double2(re, im);
+      std::memcpy(&host[elem * i], &v, elem);
     } else {
-      float2 v = make_float2((float)c, (float)s);
-      std::memcpy(&host[elem * k], &v, elem);
+      const float2 v = make_float2((float)re, (float)im);
+      std::memcpy(&host[elem * i], &v, elem);
+    }
+  };
+  // forward twiddles exp(-2 pi i k / m) of the stages
+  for (int k = 0; k < m; ++k) put((size_t)k, cos2pi(k, m), -sin2pi(k, m));
+  if (m != n) {
+    // chirp c_j = exp(-i pi j^2 / n) = exp(-2 pi i (j^2 mod 2n) / 2n)
+    std::vector<double> cre((size_t)n), cim((size_t)n), cosm((size_t)m);
+    for (int j = 0; j < n; ++j) {
+      const long long jj = ((long long)j * j) % (2LL * n);
+      cre[(size_t)j] = cos2pi(jj, 2LL * n);
+      cim[(size_t)j] = sin2pi(jj, 2LL * n);
+      put((size_t)m + j, cre[(size_t)j], -cim[(size_t)j]);
+    }
+    for (int x = 0; x < m; ++x) cosm[(size_t)x] = cos2pi(x, m);
+    // K_k = (1/m) DFT_m(conj chirp wrapped cyclically)_k
+    //     = (1/m) (1 + 2 sum_{l=1}^{n-1} cos(2 pi l k / m) exp(i pi l^2 / n)), an even sequence
+    for (int k = 0; k < m; ++k) {
+      long double re = 1.0L, im = 0.0L;
+      long long lk = 0;
+      for (int l = 1; l < n; ++l) {
+        lk += k;
+        if (lk >= m) lk %= m;
+        const long double c = 2.0L * (long double)cosm[(size_t)lk];
+        re += c * (long double)cre[(size_t)l];
+        im += c * (long double)cim[(size_t)l];
+      }
+      put((size_t)m + n + k, (double)(re / m), (double)(im / m));
     }
   }
+  return host;
+}
+
+const void* twiddle_table(qsm_ctx* ctx, const FftPlan1D& pl, bool dbl) {
+  const long long key = (long long)pl.n * 2 + (dbl ? 1 : 0);
+  auto it = ctx->twiddles.find(key);
+  if (it != ctx->twiddles.end()) return it->second;
+  const std::vector<unsigned char> host = transform_table(pl, dbl);
   void* d = nullptr;
   cudaError_t e = cudaMalloc(&d, host.size());
   if (e != cudaSuccess) {
@@ -277,6 +309,30 @@ qsm_status qsm_ctx_set_precision(qsm_ctx* ctx, int precision) {
 }
 
 int qsm_ctx_get_precision(const qsm_ctx* ctx) { return ctx ? ctx->precision : -1; }
+
+qsm_status qsm_ctx_set_plan_mode(qsm_ctx* ctx, int mode) {
+  if (ctx == nullptr) return QSM_ERR_INVALID_ARGUMENT;
+  if (mode != QSM_PLANS_COMPILED && mode != QSM_PLANS_RUNTIME) {
+    ctx->err = "unknown plan mode";
+    return QSM_ERR_INVALID_ARGUMENT;
+  }
+  ctx->plan_mode = mode;
+  return QSM_OK;
+}
+
+int qsm_ctx_get_plan_mode(const qsm_ctx* ctx) { return ctx ? ctx->plan_mode : -1; }
+
+qsm_status qsm_ctx_set_krylov_precision(qsm_ctx* ctx, int precision) {
+  if (ctx == nullptr) return QSM_ERR_INVALID_ARGUMENT;
+  if (precision != QSM_PRECISION_F64 && precision != QSM_PRECISION_MIXED) {
+    ctx->err = "unknown precision";
+    return QSM_ERR_INVALID_ARGUMENT;
+  }
+  ctx->krylov_precision = precision;
+  return QSM_OK;
+}
+
+int qsm_ctx_get_krylov_precision(const qsm_ctx* ctx) { return ctx ? ctx->krylov_precision : -1; }
 
 qsm_status qsm_ctx_release_workspace(qsm_ctx* ctx) {
   if (ctx == nullptr) return QSM_ERR_INVALID_ARGUMENT;

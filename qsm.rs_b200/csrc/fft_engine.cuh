@@ -173,7 +173,7 @@ template <int R, int DIR, int EMAX, typename C, class SA, class Fetch, class Emi
 __device__ __forceinline__ void fft_stage(C (&v)[EMAX], const FftPlan1D& pl, int s, int t, bool active,
                                           C* sp, const SA& sa, const C* tw, Fetch& fetch, Emit& emit) {
   constexpr int CM = EMAX / R;
-  const int n = pl.n;
+  const int n = pl.m;
   const int nb = n / R;
   const int T = pl.T;
   const int Ns = pl.ns[s];
@@ -277,7 +277,7 @@ __device__ __forceinline__ void fft_stage_fixed(C (&v)[kFftEmax], int t, bool ac
 template <int N, int TT, int R0, int R1, int R2 = 1> struct FixedPlan {
   static constexpr int n = N, T = TT;
   static __host__ __device__ constexpr bool matches(const FftPlan1D& pl) {
-    return pl.n == N && pl.T == TT && pl.radix[0] == R0 && pl.radix[1] == R1 &&
+    return pl.n == N && pl.m == N && pl.T == TT && pl.radix[0] == R0 && pl.radix[1] == R1 &&
            (R2 == 1 ? pl.nstages == 2 : (pl.nstages == 3 && pl.radix[2] == R2));
   }
   template <int DIR, typename C, class SA, class Fetch, class Emit>
@@ -312,37 +312,11 @@ template <int N, int TT, int R0, int R1, int R2 = 1> struct FixedPlan {
   X(162, 18, 9, 9, 2) X(168, 12, 8, 7, 3) X(180, 15, 15, 12, 1) X(200, 14, 8, 5, 5)               \
   X(216, 18, 12, 6, 3) X(224, 16, 16, 7, 2) X(225, 15, 15, 15, 1) X(240, 16, 16, 15, 1)
 
-// Full 1D transform of one pencil. DIR = -1 forward (exp(-2 pi i nk/n)), +1 inverse
-// (unnormalised).  tw points at the forward table W_n^k, k in [0, n).
-//
-// The pencil is read from global memory (SRC_G: gsrc[base + e*stride]) or from its
-// shared-memory slot (sp[sa(e)]), and written likewise (DST_G).  Solver-specific
-// work (loaders, multipliers, stores) runs in coalesced loops around this call, so
-// the engine is compiled once per I/O shape instead of once per solver operator.
-template <int DIR, typename C, class SA, bool SRC_G, bool DST_G>
-__device__ __noinline__ void fft_pencil(const FftPlan1D* plp, int t, bool active, C* sp, SA sa, const C* tw,
-                                        const C* gsrc, C* gdst, long long base, long long stride) {
-  const FftPlan1D& pl = *plp;
-  auto fetch = [&](int e) -> C {
-    if constexpr (SRC_G) return gsrc[base + e * stride];
-    else return sp[sa(e)];
-  };
-  auto emit = [&](int e, C v) {
-    if constexpr (DST_G) gdst[base + e * stride] = v;
-    else sp[sa(e)] = v;
-  };
-  // Compile-time plans only for the contiguous (X) passes in single precision:
-  // inlining every plan into the strided Y/Z engine, or into the double-precision
-  // engine, raises the register count past the occupancy budget.
-  if constexpr (!std::is_same<SA, SAStrided>::value && sizeof(C) == 8) {
-#define QSM_TRY_FIXED(N_, T_, R0_, R1_, R2_)                                                \
-    if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(pl)) {                                    \
-      FixedPlan<N_, T_, R0_, R1_, R2_>::template run<DIR>(t, active, sp, sa, tw, fetch, emit); \
-      return;                                                                               \
-    }
-    QSM_FIXED_PLANS(QSM_TRY_FIXED)
-#undef QSM_TRY_FIXED
-  }
+// The runtime stages of a plan's length-m transform, reading through fetch (first
+// stage) and writing through emit (last stage).
+template <int DIR, typename C, class SA, class Fetch, class Emit>
+__device__ __forceinline__ void run_stages(const FftPlan1D& pl, int t, bool active, C* sp, const SA& sa, const C* tw,
+                                           Fetch& fetch, Emit& emit) {
   constexpr int EMAX = kFftEmax;
   C v[EMAX];
   for (int s = 0; s < pl.nstages; ++s) {
@@ -364,6 +338,94 @@ __device__ __noinline__ void fft_pencil(const FftPlan1D* plp, int t, bool active
       default: fft_stage<16, DIR>(v, pl, s, t, active, sp, sa, tw, fetch, emit); break;
     }
   }
+}
+
+// Bluestein (chirp-z) transform of one pencil of length n through a cyclic convolution
+// of length m >= 2n - 1 (Bluestein 1970; Rabiner, Schafer and Rader 1969).  With
+// q_j = exp(DIR i pi j^2 / n), jk = (j^2 + k^2 - (k - j)^2) / 2 gives
+//   X_k = q_k * sum_j (x_j q_j) conj(q_{k-j}),
+// a convolution of a_j = x_j q_j (zero-padded to m) with the conjugate chirp.  The table
+// holds c_j = exp(-i pi j^2 / n) (so q = c forward, conj(c) inverse) and K = DFT_m of the
+// conjugate chirp wrapped cyclically, divided by m.  That sequence is even, so K is even
+// and the inverse direction's kernel spectrum is conj(K).  The pencil's slot holds m
+// elements; the length-m transforms run in place with the plan's stages and twiddles.
+template <int DIR, typename C, class SA, bool SRC_G, bool DST_G>
+__device__ __forceinline__ void bluestein_pencil(const FftPlan1D& pl, int t, bool active, C* sp, const SA& sa,
+                                                 const C* tw, const C* gsrc, C* gdst, long long base,
+                                                 long long stride) {
+  const int n = pl.n, m = pl.m, T = pl.T;
+  const C* chirp = static_cast<const C*>(pl.ext);
+  const C* kspec = chirp + n;
+  if (active) {
+    for (int j = t; j < m; j += T) {
+      C a = mk<C>(decltype(a.x)(0), decltype(a.x)(0));
+      if (j < n) {
+        C x;
+        if constexpr (SRC_G) x = gsrc[base + j * stride];
+        else x = sp[sa(j)];
+        const C c = chirp[j];
+        a = (DIR < 0) ? cmul(x, c) : cmulc(x, c);
+      }
+      sp[sa(j)] = a;
+    }
+  }
+  __syncthreads();
+  auto fetch = [&](int e) -> C { return sp[sa(e)]; };
+  auto emit_k = [&](int e, C v) {
+    const C k = kspec[e];
+    sp[sa(e)] = (DIR < 0) ? cmul(v, k) : cmulc(v, k);
+  };
+  run_stages<-1>(pl, t, active, sp, sa, tw, fetch, emit_k);
+  auto emit_out = [&](int e, C v) {
+    if (e < n) {
+      const C c = chirp[e];
+      const C y = (DIR < 0) ? cmul(v, c) : cmulc(v, c);
+      if constexpr (DST_G) gdst[base + e * stride] = y;
+      else sp[sa(e)] = y;
+    }
+  };
+  // the last stage writes each output element once, after every thread has read its
+  // inputs (the stage's first barrier), so the in-place emit is safe
+  run_stages<+1>(pl, t, active, sp, sa, tw, fetch, emit_out);
+}
+
+// Full 1D transform of one pencil. DIR = -1 forward (exp(-2 pi i nk/n)), +1 inverse
+// (unnormalised).  tw points at the forward table W_m^k, k in [0, m) (m = n except for
+// Bluestein plans).
+//
+// The pencil is read from global memory (SRC_G: gsrc[base + e*stride]) or from its
+// shared-memory slot (sp[sa(e)]), and written likewise (DST_G).  Solver-specific
+// work (loaders, multipliers, stores) runs in coalesced loops around this call, so
+// the engine is compiled once per I/O shape instead of once per solver operator.
+template <int DIR, typename C, class SA, bool SRC_G, bool DST_G>
+__device__ __noinline__ void fft_pencil(const FftPlan1D* plp, int t, bool active, C* sp, SA sa, const C* tw,
+                                        const C* gsrc, C* gdst, long long base, long long stride) {
+  const FftPlan1D& pl = *plp;
+  if (pl.m != pl.n) {
+    bluestein_pencil<DIR, C, SA, SRC_G, DST_G>(pl, t, active, sp, sa, tw, gsrc, gdst, base, stride);
+    return;
+  }
+  auto fetch = [&](int e) -> C {
+    if constexpr (SRC_G) return gsrc[base + e * stride];
+    else return sp[sa(e)];
+  };
+  auto emit = [&](int e, C v) {
+    if constexpr (DST_G) gdst[base + e * stride] = v;
+    else sp[sa(e)] = v;
+  };
+  // Compile-time plans only for the contiguous (X) passes in single precision:
+  // inlining every plan into the strided Y/Z engine, or into the double-precision
+  // engine, raises the register count past the occupancy budget.
+  if constexpr (!std::is_same<SA, SAStrided>::value && sizeof(C) == 8) {
+#define QSM_TRY_FIXED(N_, T_, R0_, R1_, R2_)                                                \
+    if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(pl)) {                                    \
+      FixedPlan<N_, T_, R0_, R1_, R2_>::template run<DIR>(t, active, sp, sa, tw, fetch, emit); \
+      return;                                                                               \
+    }
+    QSM_FIXED_PLANS(QSM_TRY_FIXED)
+#undef QSM_TRY_FIXED
+  }
+  run_stages<DIR>(pl, t, active, sp, sa, tw, fetch, emit);
 }
 
 }  // namespace qsm

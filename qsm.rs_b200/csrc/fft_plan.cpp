@@ -1,6 +1,7 @@
 // Host-side radix planner for the Stockham engine (fft_engine.cuh).
 #include "fft_plan.h"
 
+#include <initializer_list>
 #include <vector>
 
 namespace qsm {
@@ -60,18 +61,30 @@ void search(int n, int rem, int max_r, std::vector<int>& seq, Best& best) {
   }
 }
 
+bool smooth(int n, std::initializer_list<int> primes) {
+  for (int p : primes)
+    while (n % p == 0) n /= p;
+  return n == 1;
+}
+
 }  // namespace
 
 bool make_fft_plan(int n, FftPlan1D* out) {
   if (n < 1 || n > kFftMaxLen) return false;
-  {
-    int m = n;
-    for (int p : {2, 3, 5, 7, 11, 13})
-      while (m % p == 0) m /= p;
-    if (m != 1) return false;
+  if (!smooth(n, {2, 3, 5, 7, 11, 13})) {
+    // Bluestein: an n-point DFT as a cyclic convolution of length m >= 2n - 1
+    if (n > kBluesteinMaxLen) return false;
+    int m = 2 * n - 1;
+    while (!smooth(m, {2, 3, 5, 7})) ++m;
+    FftPlan1D inner{};
+    if (!make_fft_plan(m, &inner)) return false;
+    inner.n = n;
+    if (out) *out = inner;
+    return true;
   }
   FftPlan1D pl{};
   pl.n = n;
+  pl.m = n;
   if (n == 1) {
     pl.nstages = 1;
     pl.T = 1;

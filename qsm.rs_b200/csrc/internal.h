@@ -56,6 +56,8 @@ struct ProfStat {
 struct qsm_ctx {
   int device = 0;
   int precision = QSM_PRECISION_F64;
+  int plan_mode = QSM_PLANS_COMPILED;  // qsm_ctx_set_plan_mode
+  int krylov_precision = QSM_PRECISION_F64;  // qsm_ctx_set_krylov_precision (mixed contexts)
   cudaStream_t stream = nullptr;
   std::string err;
   std::map<std::string, qsm::DevBuf> ws;
@@ -85,8 +87,12 @@ template <typename P> P* ws(qsm_ctx* ctx, const std::string& name, size_t count)
 }
 void ws_release(qsm_ctx* ctx);
 
-// Forward twiddle table W_n^k (k in [0,n)) on the device, float2 or double2.
-const void* twiddle_table(qsm_ctx* ctx, int n, bool dbl);
+// Device table of a plan, float2 or double2: the forward twiddles W_m^k (k in [0, m))
+// of its stages and, for Bluestein plans, the chirp (n values) and the convolution
+// kernel spectrum (m values) after them.  Cached per length and precision.
+const void* twiddle_table(qsm_ctx* ctx, const FftPlan1D& pl, bool dbl);
+// The same table on the host (bytes).
+std::vector<unsigned char> transform_table(const FftPlan1D& pl, bool dbl);
 FftPlan1D plan_or_throw(int n);
 
 // Upload a small host vector as a cached device table keyed by name.

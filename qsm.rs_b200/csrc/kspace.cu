@@ -105,13 +105,30 @@ std::vector<double> kspace_axis_table(const char* what, int n, double vs) {
   return poisson_axis(n, vs);
 }
 
-size_t& smem_limit_slot(const void* func, int device) {
+void raise_smem_limit(const void* func, int device, size_t bytes) {
+  // the compare, the attribute call and the update run under one lock, so contexts on
+  // other host threads never skip a raise that another thread has not finished
   static std::mutex mu;
   static std::map<std::pair<const void*, int>, size_t> limits;
   std::lock_guard<std::mutex> lock(mu);
   auto it = limits.find({func, device});
   if (it == limits.end()) it = limits.emplace(std::make_pair(func, device), (size_t)48 * 1024).first;
-  return it->second;
+  if (bytes > it->second) {
+    QSM_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    it->second = bytes;
+  }
+}
+
+int sm_count_of(int device) {
+  static std::mutex mu;
+  static std::map<int, int> counts;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = counts.find(device);
+  if (it != counts.end()) return it->second;
+  int c = 0;
+  QSM_CUDA(cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, device));
+  counts[device] = c;
+  return c;
 }
 
 KSpace make_kspace(qsm_ctx* ctx, const GridDims& d, const double bdir[3]) {

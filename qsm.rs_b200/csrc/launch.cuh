@@ -15,6 +15,14 @@ template <typename T> struct Fft3 {
   const cplx_t<T>* twz;
 };
 
+// Point each Bluestein plan at the chirp and kernel spectrum that follow the stage
+// twiddles in its table.
+template <typename T> void attach_tables(Fft3<T>& f) {
+  f.px.ext = f.px.m != f.px.n ? (const void*)(f.twx + f.px.m) : nullptr;
+  f.py.ext = f.py.m != f.py.n ? (const void*)(f.twy + f.py.m) : nullptr;
+  f.pz.ext = f.pz.m != f.pz.n ? (const void*)(f.twz + f.pz.m) : nullptr;
+}
+
 template <typename T> Fft3<T> make_fft3(qsm_ctx* ctx, const GridDims& d) {
   Fft3<T> f;
   f.g.nx = d.nx;
@@ -28,25 +36,25 @@ template <typename T> Fft3<T> make_fft3(qsm_ctx* ctx, const GridDims& d) {
   f.py = plan_or_throw(d.ny);
   f.pz = plan_or_throw(d.nz);
   const bool dbl = sizeof(T) == 8;
-  f.twx = (const cplx_t<T>*)twiddle_table(ctx, d.nx, dbl);
-  f.twy = (const cplx_t<T>*)twiddle_table(ctx, d.ny, dbl);
-  f.twz = (const cplx_t<T>*)twiddle_table(ctx, d.nz, dbl);
+  f.twx = (const cplx_t<T>*)twiddle_table(ctx, f.px, dbl);
+  f.twy = (const cplx_t<T>*)twiddle_table(ctx, f.py, dbl);
+  f.twz = (const cplx_t<T>*)twiddle_table(ctx, f.pz, dbl);
+  attach_tables(f);
   return f;
 }
 
 // Raise a kernel's dynamic shared-memory limit when a launch needs more than the
-// default 48 KB (tracked per kernel function and device).
-size_t& smem_limit_slot(const void* func, int device);
+// default 48 KB (tracked per kernel function and device, under a lock).
+void raise_smem_limit(const void* func, int device, size_t bytes);
 template <class K> void ensure_smem(K kernel, size_t bytes) {
   if (bytes > 227u * 1024u) throw QsmError(QSM_ERR_UNSUPPORTED_SIZE, "transform tile exceeds shared memory");
   int dev = 0;
   QSM_CUDA(cudaGetDevice(&dev));
-  size_t& done = smem_limit_slot(reinterpret_cast<const void*>(kernel), dev);
-  if (bytes > done) {
-    QSM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-    done = bytes;
-  }
+  raise_smem_limit(reinterpret_cast<const void*>(kernel), dev, bytes);
 }
+
+// False when the context runs every pass on the runtime engine (QSM_PLANS_RUNTIME).
+inline bool compiled_plans(const qsm_ctx* ctx) { return ctx->plan_mode == QSM_PLANS_COMPILED; }
 
 inline void after_launch(qsm_ctx* ctx) {
   cudaError_t e = cudaGetLastError();
@@ -85,6 +93,7 @@ template <typename T> inline long long x_blocks(const Fft3<T>& f) {
 // QSM_FIXED_PLANS_WIDE when W); false when the plan is not one of them.
 template <typename T, bool W, class Load>
 bool run_x_r2c_fixed(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* spec, const Load& ld, const int* done) {
+  if (!compiled_plans(ctx)) return false;
   if constexpr (!std::is_same<T, float>::value && !W) {
     return false;
   } else {
@@ -113,6 +122,7 @@ bool run_x_r2c_fixed(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* spec, const Load
 
 template <typename T, bool W, class Store>
 bool run_x_c2r_fixed(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* spec, const Store& st, const int* done) {
+  if (!compiled_plans(ctx)) return false;
   if constexpr (!std::is_same<T, float>::value && !W) {
     return false;
   } else {
@@ -145,7 +155,7 @@ void run_x_r2c(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* spec, const Load& ld, 
   using C = cplx_t<T>;
   const int Tt = x_block_t(f.px.T);
   const int P = x_pencils_per_block<T>(f.px.T);
-  const size_t smem = (size_t)(f.px.n + P * x_rowlen<T>(f.px.n)) * sizeof(C);
+  const size_t smem = (size_t)(f.px.m + P * x_rowlen<T>(f.px.m)) * sizeof(C);
   auto kern = k_x_r2c<T, Load>;
   ensure_smem(kern, smem);
   LaunchScope ls(ctx, "fft_x_r2c");
@@ -159,7 +169,7 @@ void run_x_c2r(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* spec, const Stor
   using C = cplx_t<T>;
   const int Tt = x_block_t(f.px.T);
   const int P = x_pencils_per_block<T>(f.px.T);
-  const size_t smem = (size_t)(f.px.n + P * x_rowlen<T>(f.px.n)) * sizeof(C);
+  const size_t smem = (size_t)(f.px.m + P * x_rowlen<T>(f.px.m)) * sizeof(C);
   auto kern = k_x_c2r<T, Store>;
   ensure_smem(kern, smem);
   LaunchScope ls(ctx, "fft_x_c2r");
@@ -189,6 +199,7 @@ void run_x_full(qsm_ctx* ctx, const Fft3<T>& f, const Load& ld, const Mid& mid, 
                 const char* name) {
   using C = cplx_t<T>;
   if constexpr (W && D1 != 0 && D2 != 0 && std::is_same<T, float>::value) {
+    if (compiled_plans(ctx)) {
 #define QSM_TRY_XF(N_, T_, R0_, R1_, R2_)                                                          \
     if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(f.px)) {                                         \
       using FP = FixedPlan<N_, T_, R0_, R1_, R2_>;                                                 \
@@ -205,12 +216,13 @@ void run_x_full(qsm_ctx* ctx, const Fft3<T>& f, const Load& ld, const Mid& mid, 
     }
     QSM_FIXED_PLANS(QSM_TRY_XF)
 #undef QSM_TRY_XF
+    }
   }
   if ((f.px.n + f.px.T - 1) / f.px.T > kFftEmax)
     throw QsmError(QSM_ERR_UNSUPPORTED_SIZE, "x length outside the per-thread register budget");
   const int Tt = x_block_t(f.px.T);
   const int P = x_pencils_per_block<T>(f.px.T);
-  const size_t smem = (size_t)(f.px.n + P * x_rowlen<T>(f.px.n)) * sizeof(C);
+  const size_t smem = (size_t)(f.px.m + P * x_rowlen<T>(f.px.m)) * sizeof(C);
   auto kern = k_x_full<T, D1, D2, Load, Mid, Store>;
   ensure_smem(kern, smem);
   const long long blocks = ((long long)f.g.nrows() + P - 1) / P;
@@ -221,12 +233,8 @@ void run_x_full(qsm_ctx* ctx, const Fft3<T>& f, const Load& ld, const Mid& mid, 
 
 template <typename T> inline int yz_cols() { return sizeof(T) == 4 ? 16 : 8; }
 
-inline int sm_count(qsm_ctx* ctx) {
-  static int cached[64] = {0};
-  const int d = ctx->device & 63;
-  if (cached[d] == 0) QSM_CUDA(cudaDeviceGetAttribute(&cached[d], cudaDevAttrMultiProcessorCount, ctx->device));
-  return cached[d];
-}
+int sm_count_of(int device);  // multiprocessor count, cached per device under a lock
+inline int sm_count(qsm_ctx* ctx) { return sm_count_of(ctx->device); }
 
 // Persistent grid: as many CTAs as fit on the device at once, capped by the work.
 template <class K> unsigned persistent_grid(qsm_ctx* ctx, K kernel, int threads, size_t smem, long long work) {
@@ -304,6 +312,7 @@ template <class K> bool fx_launch_ok(qsm_ctx* ctx, K kern, int threads, size_t s
 
 template <typename T, int DIR, int AXIS, bool W>
 bool run_yz_fixed(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst, const int* done) {
+  if (!compiled_plans(ctx)) return false;
   if constexpr (!std::is_same<T, float>::value) {
     return false;
   } else {
@@ -338,6 +347,7 @@ constexpr int kMaxPersistentBlocks = 4096;
 template <typename T, int DIR, int AXIS, bool ACC, class Op>
 bool run_yz_op_fixed(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst, const Op& op,
                      double* partials, unsigned* counter, const int* done, const char* name) {
+  if (!compiled_plans(ctx)) return false;
   if constexpr (!std::is_same<T, float>::value) {
     return false;
   } else {
@@ -378,8 +388,8 @@ void run_yz(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst
   const FftPlan1D& pl = (AXIS == 1) ? f.py : f.pz;
   const cplx_t<T>* tw = (AXIS == 1) ? f.twy : f.twz;
   auto kern = k_pass_yz<T, DIR, AXIS, Op>;
-  const int P = yz_tile_width<T>(kern, pl.n, pl.T);
-  const size_t smem = yz_smem<T>(pl.n, P);
+  const int P = yz_tile_width<T>(kern, pl.m, pl.T);
+  const size_t smem = yz_smem<T>(pl.m, P);
   const TileWalk w = tile_walk(f, AXIS, P);
   const unsigned grid = persistent_grid(ctx, kern, P * pl.T, smem, w.ntiles);
   LaunchScope ls(ctx, AXIS == 1 ? (DIR < 0 ? "fft_y_fwd" : "fft_y_inv") : (DIR < 0 ? "fft_z_fwd" : "fft_z_inv"));
@@ -398,8 +408,8 @@ void run_yz_acc(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>*
   const FftPlan1D& pl = (AXIS == 1) ? f.py : f.pz;
   const cplx_t<T>* tw = (AXIS == 1) ? f.twy : f.twz;
   auto kern = k_pass_yz_acc<T, DIR, AXIS, Op>;
-  const int P = yz_tile_width<T>(kern, pl.n, pl.T);
-  const size_t smem = yz_smem<T>(pl.n, P);
+  const int P = yz_tile_width<T>(kern, pl.m, pl.T);
+  const size_t smem = yz_smem<T>(pl.m, P);
   const TileWalk w = tile_walk(f, AXIS, P);
   unsigned grid = persistent_grid(ctx, kern, P * pl.T, smem, w.ntiles);
   if (grid > (unsigned)kMaxPersistentBlocks) grid = kMaxPersistentBlocks;
@@ -408,18 +418,19 @@ void run_yz_acc(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>*
   ls.done();
 }
 
-template <typename T> inline size_t zm_smem(int n, int P) {
-  return yz_smem<T>(n, P) + 2 * (((size_t)n * P + 3) & ~(size_t)3) * sizeof(T);
+// n multiplier rows, m tile-buffer rows (m = n except for Bluestein plans)
+template <typename T> inline size_t zm_smem(int n, int m, int P) {
+  return yz_smem<T>(m, P) + 2 * (((size_t)n * P + 3) & ~(size_t)3) * sizeof(T);
 }
 
 // Tile width of the multiplier-array Z pass, 0 when no width fits (very long axes).
-template <typename T> int zm_tile_width(int n, int Tn) {
+template <typename T> int zm_tile_width(int n, int m, int Tn) {
   auto kern = k_z_fused_m<T>;
   for (int p = yz_cols<T>(); p >= 16 / (int)sizeof(T); p /= 2) {
-    if (p * Tn > 1024 || zm_smem<T>(n, p) > 227u * 1024u) continue;
-    ensure_smem(kern, zm_smem<T>(n, p));
+    if (p * Tn > 1024 || zm_smem<T>(n, m, p) > 227u * 1024u) continue;
+    ensure_smem(kern, zm_smem<T>(n, m, p));
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, p * Tn, zm_smem<T>(n, p)) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, p * Tn, zm_smem<T>(n, m, p)) != cudaSuccess) {
       (void)cudaGetLastError();
       continue;
     }
@@ -435,11 +446,12 @@ void run_z_fused_m(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<
                    const int* done) {
   const FftPlan1D& pl = f.pz;
   if constexpr (std::is_same<T, float>::value) {
+    if (compiled_plans(ctx)) {
 #define QSM_TRY_ZM(N_, T_, R0_, R1_, R2_)                                                         \
     if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(pl) && kZmCols * T_ <= 1024) {                   \
       using FP = FixedPlan<N_, T_, R0_, R1_, R2_>;                                                \
       auto kfx = k_z_fused_m_fx<T, FP, kZmCols>;                                                  \
-      const size_t smem = zm_smem<T>(N_, kZmCols);                                                \
+      const size_t smem = zm_smem<T>(N_, N_, kZmCols);                                                \
       const TileWalk w = tile_walk(f, 2, kZmCols);                                                \
       unsigned grid = 0;                                                                          \
       if (fx_launch_ok(ctx, kfx, kZmCols * T_, smem, &grid, w.ntiles)) {                          \
@@ -454,11 +466,12 @@ void run_z_fused_m(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<
       QSM_FIXED_PLANS_WIDE(QSM_TRY_ZM)
     }
 #undef QSM_TRY_ZM
+    }
   }
   auto kern = k_z_fused_m<T>;
-  const int P = zm_tile_width<T>(pl.n, pl.T);
+  const int P = zm_tile_width<T>(pl.n, pl.m, pl.T);
   if (P == 0) throw QsmError(QSM_ERR_UNSUPPORTED_SIZE, "z axis does not fit one multiplier tile");
-  const size_t smem = zm_smem<T>(pl.n, P);
+  const size_t smem = zm_smem<T>(pl.n, pl.m, P);
   const TileWalk w = tile_walk(f, 2, P);
   const unsigned grid = persistent_grid(ctx, kern, P * pl.T, smem, w.ntiles);
   LaunchScope ls(ctx, "fft_z_fused");
@@ -471,8 +484,8 @@ void run_z_fused(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>
                  const int* done) {
   const FftPlan1D& pl = f.pz;
   auto kern = k_z_fused<T, Op>;
-  const int P = yz_tile_width<T>(kern, pl.n, pl.T);
-  const size_t smem = yz_smem<T>(pl.n, P);
+  const int P = yz_tile_width<T>(kern, pl.m, pl.T);
+  const size_t smem = yz_smem<T>(pl.m, P);
   const TileWalk w = tile_walk(f, 2, P);
   const unsigned grid = persistent_grid(ctx, kern, P * pl.T, smem, w.ntiles);
   LaunchScope ls(ctx, "fft_z_fused");

@@ -14,13 +14,15 @@
 //   * All calls on a device share the array and it keeps the last call's contents;
 //     calls that overlap on the GPU (different streams, or host threads racing) race
 //     on it and must be serialised by the caller.
-//   * The first call on a device resolves the array's device address with
-//     cudaGetSymbolAddress; make that first call before any stream capture.
+//   * Every call resolves the array's device address on the current device with
+//     cudaGetSymbolAddress (nothing is cached, so a context torn down and recreated
+//     by cudaDeviceReset cannot leave a stale address behind).
+//   * The call uploads its tables with cudaMemcpyAsync from pageable host memory and
+//     synchronises its stream, so it must not be called while that stream is being
+//     captured into a CUDA graph; such a call is refused with QSM_ERR_INVALID_ARGUMENT.
 #include "closed_form_ops.cuh"
 #include "functors.cuh"
 #include "solvers.h"
-
-#include <mutex>
 
 namespace qsm {
 
@@ -31,31 +33,16 @@ namespace {
 constexpr size_t kNoAllocScratchBytes = (size_t)48 << 20;
 __device__ __align__(256) unsigned char g_tkd_scratch[kNoAllocScratchBytes];
 
-constexpr int kMaxDevices = 128;
-std::mutex g_scratch_mu;
-void* g_scratch_addr[kMaxDevices] = {};
-
-// Device address of g_tkd_scratch on the current device (resolved once per device).
-unsigned char* scratch_address(int device) {
-  if (device < 0 || device >= kMaxDevices) throw QsmError(QSM_ERR_INVALID_ARGUMENT, "device index out of range");
-  std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (g_scratch_addr[device] == nullptr) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_tkd_scratch);
-    if (e != cudaSuccess || p == nullptr)
-      throw QsmError(QSM_ERR_CUDA, std::string("cudaGetSymbolAddress(g_tkd_scratch): ") + cudaGetErrorString(e));
-    g_scratch_addr[device] = p;
-  }
-  return static_cast<unsigned char*>(g_scratch_addr[device]);
+// Device address of g_tkd_scratch on the current device, resolved on every call.
+unsigned char* scratch_address() {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_tkd_scratch);
+  if (e != cudaSuccess || p == nullptr)
+    throw QsmError(QSM_ERR_CUDA, std::string("cudaGetSymbolAddress(g_tkd_scratch): ") + cudaGetErrorString(e));
+  return static_cast<unsigned char*>(p);
 }
 
 size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
-
-std::vector<double2> twiddles_f64(int n) {
-  std::vector<double2> t((size_t)n);
-  for (int k = 0; k < n; ++k) t[(size_t)k] = make_double2(cos2pi(k, n), -sin2pi(k, n));
-  return t;
-}
 
 }  // namespace
 }  // namespace qsm
@@ -73,6 +60,10 @@ extern "C" qsm_status qsm_tkd_device_noalloc(const double* d_local_field, const 
   local.precision = QSM_PRECISION_F64;
   local.stream = static_cast<cudaStream_t>(stream);
   return guarded(&local, [&] {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    QSM_CUDA(cudaStreamIsCapturing(local.stream, &cap));
+    if (cap != cudaStreamCaptureStatusNone)
+      throw QsmError(QSM_ERR_INVALID_ARGUMENT, "the allocation-free TKD cannot run while its stream is capturing");
     GridDims d = check_grid(grid);
     check_ptr(d_local_field, "local_field");
     check_ptr(d_mask, "mask");
@@ -91,10 +82,11 @@ extern "C" qsm_status qsm_tkd_device_noalloc(const double* d_local_field, const 
     f.py = plan_or_throw(d.ny);
     f.pz = plan_or_throw(d.nz);
 
-    // scratch layout: spectrum | twiddles x, y, z | 9 per-axis k-space tables
+    // scratch layout: spectrum | transform tables x, y, z | 9 per-axis k-space tables
     const size_t spec_b = round256((size_t)f.g.hsize() * sizeof(double2));
-    const size_t tw_b[3] = {round256((size_t)d.nx * sizeof(double2)), round256((size_t)d.ny * sizeof(double2)),
-                            round256((size_t)d.nz * sizeof(double2))};
+    const std::vector<unsigned char> tw_h[3] = {transform_table(f.px, true), transform_table(f.py, true),
+                                                transform_table(f.pz, true)};
+    const size_t tw_b[3] = {round256(tw_h[0].size()), round256(tw_h[1].size()), round256(tw_h[2].size())};
     const int ns[3] = {d.nx, d.ny, d.nz};
     const double vs[3] = {d.vsx, d.vsy, d.vsz};
     size_t tab_b = 0;
@@ -104,20 +96,20 @@ extern "C" qsm_status qsm_tkd_device_noalloc(const double* d_local_field, const 
       throw QsmError(QSM_ERR_UNSUPPORTED_SIZE, "volume needs " + std::to_string(need) +
                                                    " bytes of scratch; the allocation-free TKD holds " +
                                                    std::to_string(kNoAllocScratchBytes));
-    unsigned char* base = scratch_address(local.device);
+    unsigned char* base = scratch_address();
     unsigned char* cur = base;
     double2* spec = reinterpret_cast<double2*>(cur);
     cur += spec_b;
     const double2* tw[3];
     for (int a = 0; a < 3; ++a) {
-      const std::vector<double2> h = twiddles_f64(ns[a]);
-      QSM_CUDA(cudaMemcpyAsync(cur, h.data(), h.size() * sizeof(double2), cudaMemcpyHostToDevice, local.stream));
+      QSM_CUDA(cudaMemcpyAsync(cur, tw_h[a].data(), tw_h[a].size(), cudaMemcpyHostToDevice, local.stream));
       tw[a] = reinterpret_cast<const double2*>(cur);
       cur += tw_b[a];
     }
     f.twx = tw[0];
     f.twy = tw[1];
     f.twz = tw[2];
+    attach_tables(f);
     const double* tabs[3][3];  // [kind freq/lap/poi][axis]
     const char* kinds[3] = {"freq", "lap", "poi"};
     for (int kd = 0; kd < 3; ++kd)

@@ -75,10 +75,11 @@ __global__ void k_x_r2c(Geom g, const __grid_constant__ FftPlan1D pl, const cplx
   extern __shared__ __align__(16) unsigned char smraw[];
   C* tw = reinterpret_cast<C*>(smraw);
   const int n = pl.n;
-  const int rowlen = x_rowlen<T>(n);
-  C* sm = tw + n;
+  const int m = pl.m;  // slot length: n, or the Bluestein convolution length
+  const int rowlen = x_rowlen<T>(m);
+  C* sm = tw + m;
   const int tid = threadIdx.x + threadIdx.y * blockDim.x;
-  for (int i = tid; i < n; i += blockDim.x * blockDim.y) tw[i] = twg[i];
+  for (int i = tid; i < m; i += blockDim.x * blockDim.y) tw[i] = twg[i];
   const int t = threadIdx.x;
   const int p = threadIdx.y;
   const long long q = (long long)blockIdx.x * blockDim.y + p;
@@ -137,10 +138,11 @@ __global__ void k_x_full(Geom g, const __grid_constant__ FftPlan1D pl, const cpl
   extern __shared__ __align__(16) unsigned char smraw[];
   C* tw = reinterpret_cast<C*>(smraw);
   const int n = pl.n;
-  const int rowlen = x_rowlen<T>(n);
-  C* sm = tw + n;
+  const int m = pl.m;  // slot length: n, or the Bluestein convolution length
+  const int rowlen = x_rowlen<T>(m);
+  C* sm = tw + m;
   const int tid = threadIdx.x + threadIdx.y * blockDim.x;
-  for (int i = tid; i < n; i += blockDim.x * blockDim.y) tw[i] = twg[i];
+  for (int i = tid; i < m; i += blockDim.x * blockDim.y) tw[i] = twg[i];
   const int t = threadIdx.x;
   const long long row = (long long)blockIdx.x * blockDim.y + threadIdx.y;
   const bool active = row < g.nrows() && t < pl.T;
@@ -233,10 +235,11 @@ __global__ void k_x_c2r(Geom g, const __grid_constant__ FftPlan1D pl, const cplx
   extern __shared__ __align__(16) unsigned char smraw[];
   C* tw = reinterpret_cast<C*>(smraw);
   const int n = pl.n;
-  const int rowlen = x_rowlen<T>(n);
-  C* sm = tw + n;
+  const int m = pl.m;  // slot length: n, or the Bluestein convolution length
+  const int rowlen = x_rowlen<T>(m);
+  C* sm = tw + m;
   const int tid = threadIdx.x + threadIdx.y * blockDim.x;
-  for (int i = tid; i < n; i += blockDim.x * blockDim.y) tw[i] = twg[i];
+  for (int i = tid; i < m; i += blockDim.x * blockDim.y) tw[i] = twg[i];
   const int t = threadIdx.x;
   const int p = threadIdx.y;
   const long long q = (long long)blockIdx.x * blockDim.y + p;
@@ -433,11 +436,12 @@ __global__ void __maxnreg__(YzRegCap<T>::value)
   extern __shared__ __align__(16) unsigned char smraw[];
   C* tw = reinterpret_cast<C*>(smraw);
   const int n = pl.n;
+  const int m = pl.m;  // rows of a tile buffer: n, or the Bluestein convolution length
   const int P = blockDim.x;
-  C* buf0 = tw + ((n + 7) & ~7);
-  C* buf1 = buf0 + (size_t)n * P;
+  C* buf0 = tw + ((m + 7) & ~7);
+  C* buf1 = buf0 + (size_t)m * P;
   const int tid = threadIdx.x + threadIdx.y * blockDim.x;
-  for (int i = tid; i < n; i += blockDim.x * blockDim.y) tw[i] = twg[i];
+  for (int i = tid; i < m; i += blockDim.x * blockDim.y) tw[i] = twg[i];
   const int px = threadIdx.x;
   const int t = threadIdx.y;
   SAStrided sa{P};
@@ -563,11 +567,12 @@ __global__ void __maxnreg__(YzRegCap<T>::value)
   extern __shared__ __align__(16) unsigned char smraw[];
   C* tw = reinterpret_cast<C*>(smraw);
   const int n = pl.n;
+  const int m = pl.m;  // rows of a tile buffer: n, or the Bluestein convolution length
   const int P = blockDim.x;
-  C* buf0 = tw + ((n + 7) & ~7);
-  C* buf1 = buf0 + (size_t)n * P;
+  C* buf0 = tw + ((m + 7) & ~7);
+  C* buf1 = buf0 + (size_t)m * P;
   const int tid = threadIdx.x + threadIdx.y * blockDim.x;
-  for (int i = tid; i < n; i += blockDim.x * blockDim.y) tw[i] = twg[i];
+  for (int i = tid; i < m; i += blockDim.x * blockDim.y) tw[i] = twg[i];
   const int px = threadIdx.x;
   const int t = threadIdx.y;
   SAStrided sa{P};
@@ -657,13 +662,14 @@ __global__ void __maxnreg__(ZRegCap<T>::value) k_z_fused_m(Geom g, const __grid_
   extern __shared__ __align__(16) unsigned char smraw[];
   C* tw = reinterpret_cast<C*>(smraw);
   const int n = pl.n;
+  const int m = pl.m;  // rows of a tile buffer: n, or the Bluestein convolution length
   const int P = blockDim.x;
-  C* buf0 = tw + ((n + 7) & ~7);
-  C* buf1 = buf0 + (size_t)n * P;
-  T* mb0 = reinterpret_cast<T*>(buf1 + (size_t)n * P);
+  C* buf0 = tw + ((m + 7) & ~7);
+  C* buf1 = buf0 + (size_t)m * P;
+  T* mb0 = reinterpret_cast<T*>(buf1 + (size_t)m * P);
   T* mb1 = mb0 + (((size_t)n * P + 3) & ~(size_t)3);
   const int tid = threadIdx.x + threadIdx.y * blockDim.x;
-  for (int i = tid; i < n; i += blockDim.x * blockDim.y) tw[i] = twg[i];
+  for (int i = tid; i < m; i += blockDim.x * blockDim.y) tw[i] = twg[i];
   const int px = threadIdx.x;
   const int t = threadIdx.y;
   SAStrided sa{P};
@@ -857,11 +863,12 @@ __global__ void __maxnreg__(ZRegCap<T>::value)
   extern __shared__ __align__(16) unsigned char smraw[];
   C* tw = reinterpret_cast<C*>(smraw);
   const int n = pl.n;
+  const int m = pl.m;  // rows of a tile buffer: n, or the Bluestein convolution length
   const int P = blockDim.x;
-  C* buf0 = tw + ((n + 7) & ~7);
-  C* buf1 = buf0 + (size_t)n * P;
+  C* buf0 = tw + ((m + 7) & ~7);
+  C* buf1 = buf0 + (size_t)m * P;
   const int tid = threadIdx.x + threadIdx.y * blockDim.x;
-  for (int i = tid; i < n; i += blockDim.x * blockDim.y) tw[i] = twg[i];
+  for (int i = tid; i < m; i += blockDim.x * blockDim.y) tw[i] = twg[i];
   const int px = threadIdx.x;
   const int t = threadIdx.y;
   SAStrided sa{P};

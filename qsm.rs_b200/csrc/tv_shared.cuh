@@ -739,7 +739,7 @@ void tv_alloc(qsm_ctx* ctx, TvVol<T>& v, const std::string& pre, const GridDims&
   v.mask = d_mask;
   v.out = d_out;
   v.mult = ws<T>(ctx, pre + "mult", (size_t)v.f.g.hsize());
-  v.use_mult = zm_tile_width<T>(d.nz, v.f.pz.T) > 0;
+  v.use_mult = zm_tile_width<T>(d.nz, v.f.pz.m, v.f.pz.T) > 0;
 }
 
 // Initial state on ctx->stream: y_0 = x0 (x_0 = 0), u = 0, iteration counter 1.

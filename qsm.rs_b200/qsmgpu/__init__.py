@@ -131,6 +131,29 @@ class Context:
     def precision(self, p: str):
         _check(self, self._lib.qsm_ctx_set_precision(self._h, _prec_code(p)))
 
+    @property
+    def plan_mode(self) -> str:
+        """"compiled" (compile-time pass kernels where a length has one) or "runtime"
+        (the runtime Stockham engine for every pass)."""
+        return "runtime" if self._lib.qsm_ctx_get_plan_mode(self._h) == _lib.PLANS_RUNTIME else "compiled"
+
+    @plan_mode.setter
+    def plan_mode(self, m: str):
+        codes = {"compiled": _lib.PLANS_COMPILED, "runtime": _lib.PLANS_RUNTIME}
+        if m not in codes:
+            raise ValueError(f"plan mode must be one of {sorted(codes)}")
+        _check(self, self._lib.qsm_ctx_set_plan_mode(self._h, codes[m]))
+
+    @property
+    def krylov_precision(self) -> str:
+        """Arithmetic of iLSQR's LSQR/LSMR steps in a mixed context: "f64" (default) or
+        "mixed" (float vectors and transforms, FP64 norms and recurrences)."""
+        return "mixed" if self._lib.qsm_ctx_get_krylov_precision(self._h) == _lib.PRECISION_MIXED else "f64"
+
+    @krylov_precision.setter
+    def krylov_precision(self, p: str):
+        _check(self, self._lib.qsm_ctx_set_krylov_precision(self._h, _prec_code(p)))
+
     def last_error(self) -> str:
         s = self._lib.qsm_last_error(self._h)
         return s.decode() if s else ""

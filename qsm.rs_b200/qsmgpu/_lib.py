@@ -27,6 +27,8 @@ STATUS_NAMES = {
 
 PRECISION_F64 = 0
 PRECISION_MIXED = 1
+PLANS_COMPILED = 0
+PLANS_RUNTIME = 1
 
 c_double_p = C.POINTER(C.c_double)
 c_u8_p = C.POINTER(C.c_uint8)
@@ -124,6 +126,10 @@ _SIGS = [
     ("qsm_ctx_destroy", C.c_int, [C.c_void_p]),
     ("qsm_ctx_set_precision", C.c_int, [C.c_void_p, C.c_int]),
     ("qsm_ctx_get_precision", C.c_int, [C.c_void_p]),
+    ("qsm_ctx_set_plan_mode", C.c_int, [C.c_void_p, C.c_int]),
+    ("qsm_ctx_get_plan_mode", C.c_int, [C.c_void_p]),
+    ("qsm_ctx_set_krylov_precision", C.c_int, [C.c_void_p, C.c_int]),
+    ("qsm_ctx_get_krylov_precision", C.c_int, [C.c_void_p]),
     ("qsm_ctx_release_workspace", C.c_int, [C.c_void_p]),
     ("qsm_last_error", C.c_char_p, [C.c_void_p]),
     ("qsm_ctx_kernel_launches", C.c_uint64, [C.c_void_p]),
@@ -155,6 +161,8 @@ _SIGS = [
                                     PROGRESS_FN, C.c_void_p, C.POINTER(C.c_size_t)]),
     ("qsm_tv_admm_batch_device", C.c_int, [C.c_void_p, C.POINTER(QsmVolume), C.c_size_t, C.POINTER(QsmTvParams),
                                            PROGRESS_FN, C.c_void_p, C.POINTER(C.c_size_t)]),
+    ("qsm_batch_partition", C.c_int, [C.POINTER(QsmGrid), C.POINTER(C.c_size_t), C.c_size_t, C.c_size_t,
+                                      C.POINTER(C.c_uint32), C.POINTER(C.c_double)]),
     ("qsm_tkd_batch_device", C.c_int, [C.c_void_p, C.POINTER(QsmVolume), C.c_size_t, C.POINTER(QsmTkdParams)]),
     ("qsm_apply_reference", C.c_int, [C.c_void_p, c_double_p, c_u8_p, C.c_size_t, C.c_int, c_double_p]),
     ("qsm_run_tgv", C.c_int, [C.c_void_p, C.POINTER(c_double_p), C.c_size_t, C.c_size_t, c_u8_p,

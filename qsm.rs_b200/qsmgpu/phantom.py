@@ -6,6 +6,9 @@ bundle) is not available, so every input here is generated from a seed.
 * ``tv_case_64``   — 64^3 at 1 mm, B0 = z: 12 random ellipsoids (semi-axes 3-12 voxels,
   chi ~ U[-0.1, 0.2] ppm) in a sphere mask of radius 28; local field =
   Re IFFT(D * FFT(chi)) + N(0, 0.01) ppm inside the mask.
+* ``brain_tv_case`` — 256 x 256 x 176 at 1 mm, B0 = z: 12 ellipsoids inside a
+  100 x 120 x 75-voxel ellipsoid brain mask; local field = dipole-convolved chi +
+  N(0, 0.01) ppm inside the mask (the TV-ADMM throughput case).
 * ``chain_case``   — 256 x 256 x 176 at 1 mm, 3 T, TE 20 ms: ellipsoid brain mask with
   semi-axes 100 x 120 x 75 voxels, ellipsoid chi phantom inside, background field from
   4 point dipoles outside the mask; wrapped phase = angle(exp(i * 2 pi * 42.58 * 3 *
@@ -116,6 +119,23 @@ def tv_case(n=(64, 64, 64), seed=0, n_ellipsoids=12, mask_radius=28.0, noise=0.0
 
 def tv_case_64(seed=0) -> TvCase:
     return tv_case((64, 64, 64), seed=seed)
+
+
+def brain_tv_case(seed=0, dims=(256, 256, 176)):
+    """(local_field, mask) of the TV-ADMM throughput case: 12 ellipsoids (semi-axes 3-12
+    voxels, chi ~ U[-0.1, 0.2] ppm) centred within +-60/72/45 voxels of the middle, an
+    ellipsoid brain mask with semi-axes 100 x 120 x 75 voxels, noise N(0, 0.01) ppm."""
+    nx, ny, nz = dims
+    rng = np.random.default_rng(seed)
+    shape = (nz, ny, nx)
+    mask = ellipsoid_mask(shape, (100.0, 120.0, 75.0))
+    chi = np.zeros(shape)
+    ctr = ((nx - 1) / 2, (ny - 1) / 2, (nz - 1) / 2)
+    box = [(ctr[0] - 60, ctr[0] + 60), (ctr[1] - 72, ctr[1] + 72), (ctr[2] - 45, ctr[2] + 45)]
+    add_ellipsoids(chi, rng, 12, box)
+    chi *= mask
+    f = forward_field(chi) + rng.normal(0.0, 0.01, size=shape) * mask
+    return np.ascontiguousarray(f), np.ascontiguousarray(mask)
 
 
 @dataclass

@@ -85,7 +85,9 @@ def test_grid_support_planner(lib):
     ok = lambda *d: lib.qsm_grid_supported(C.byref(_lib.QsmGrid(*d, 1.0, 1.0, 1.0)))
     assert ok(256, 256, 176) and ok(64, 64, 64) and ok(384, 384, 256) and ok(225, 135, 125)
     assert ok(1, 7, 13) and ok(2, 3, 11)
-    assert not ok(17, 8, 8) and not ok(8, 8, 19) and not ok(8, 8, 8192)
+    # prime factors above 13 take Bluestein plans up to 2048 (MNI 182x218x182: 218 = 2*109)
+    assert ok(17, 8, 8) and ok(8, 8, 19) and ok(182, 218, 182) and ok(2039, 23, 127) and ok(2048, 4096, 1)
+    assert not ok(2053, 8, 8) and not ok(8, 4097, 8) and not ok(8, 8, 8192) and not ok(8, 8, 4094)
 
 
 def test_null_context_rejected(lib):

@@ -287,7 +287,7 @@ def test_pipeline_dispatch_and_errors(ctx64):
 
 
 def test_invalid_arguments_are_errors_not_faults(ctx64):
-    grid = Grid.new(17, 8, 8)  # 17 has no plan
+    grid = Grid.new(2053, 4, 4)  # a prime above the Bluestein limit (2048) has no plan
     with pytest.raises(qsmgpu.QsmError) as e:
         inversion.tkd(np.zeros(grid.shape), np.ones(grid.shape, np.uint8), grid, ctx=ctx64)
     assert e.value.status == 3

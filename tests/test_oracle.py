@@ -372,6 +372,72 @@ def test_ilsqr_small():
     np.testing.assert_array_equal(chi, np.where(mask > 0, xlsqr - xsa, 0.0))
 
 
+def _ilsqr_phantom():
+    """24x20x18 ellipsoid-mask phantom at (1, 1.2, 0.9) mm with an oblique field."""
+    rng = np.random.default_rng(5)
+    nx, ny, nz = 24, 20, 18
+    grid = O.Grid.new(nx, ny, nz, 1.0, 1.2, 0.9)
+    bdir = (math.sin(0.35) * math.cos(0.8), math.sin(0.35) * math.sin(0.8), math.cos(0.35))
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    c = ((nx - 1) / 2, (ny - 1) / 2, (nz - 1) / 2)
+    mask = ((i - c[0]) / (0.4 * nx)) ** 2 + ((j - c[1]) / (0.4 * ny)) ** 2 + ((k - c[2]) / (0.4 * nz)) ** 2 < 1.0
+    chi = np.zeros(grid.shape)
+    for _ in range(6):
+        p = [rng.uniform(0.3, 0.7) * s for s in (nx, ny, nz)]
+        r = rng.uniform(1.5, 3.5)
+        chi[((i - p[0]) ** 2 + (j - p[1]) ** 2 + (k - p[2]) ** 2) < r * r] = rng.uniform(-0.1, 0.2)
+    chi *= mask
+    d = O.dipole_kernel(grid, bdir)
+    f = np.fft.ifftn(d * np.fft.fftn(chi)).real + rng.normal(0, 0.01, grid.shape) * mask
+    return f, mask.astype(np.uint8), grid, bdir
+
+
+def test_ilsqr_krylov_steps_amplify_rounding():
+    """Why mixed-precision iLSQR keeps its Krylov steps in FP64.  The reference's LSQR step
+    (src/inversion/ilsqr.rs:953-1030) stops at relres 0.01 or 50 iterations; on this phantom
+    it runs all 50 and its iterate is far (> 10%) from the converged least-squares
+    solution, so the result is the truncated Krylov iterate itself:
+      * relative noise of 1e-7 (float rounding) on every FFT output moves the outputs by
+        more than 1e-4, while the same noise on the input field alone moves them by ~1e-7:
+        the Krylov recurrences amplify per-operation rounding about a thousandfold;
+      * an outer iterative-refinement step (FP64 residual b - A x, truncated LSQR on it)
+        converges towards the least-squares solution and away from the reference's iterate.
+    """
+    f, mask, grid, bdir = _ilsqr_phantom()
+    ref = O.ilsqr(f, mask, grid, bdir, O.IlsqrParams())
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    # input perturbation: small response
+    noisy = f * (1 + 1e-7 * np.random.default_rng(1).standard_normal(f.shape))
+    r_in = O.ilsqr(noisy, mask, grid, bdir, O.IlsqrParams())
+    assert max(rel(a, b) for a, b in zip(r_in, ref)) < 1e-6
+    # per-FFT rounding-level noise: amplified by the Krylov steps
+    f0, i0 = O.fft3d, O.ifft3d
+    rng = np.random.default_rng(0)
+    noise = lambda a: a * (1 + 1e-7 * rng.standard_normal(a.shape))
+    try:
+        O.fft3d = lambda a: noise(f0(a))
+        O.ifft3d = lambda a: noise(i0(a))
+        r_fft = O.ilsqr(f, mask, grid, bdir, O.IlsqrParams())
+    finally:
+        O.fft3d, O.ifft3d = f0, i0
+    e = {n: rel(a, b) for n, a, b in zip(("chi", "xsa", "xfs", "xlsqr"), r_fft, ref)}
+    assert e["xlsqr"] > 1e-4 and e["xsa"] > 1e-4 and e["xfs"] < 1e-6, e
+    # truncated LSQR vs converged, and one refinement step
+    d = O.dipole_kernel(grid, bdir)
+    w = O.laplacian_weights_ilsqr(f, mask, grid)
+    b = (O.fft3d((w * f).astype(np.complex128)) * d).ravel()
+
+    def apply_a(x):
+        r = O.ifft3d(d * x.reshape(grid.shape)).real
+        return (O.fft3d((w * r).astype(np.complex128)) * d).ravel()
+
+    x_ref, iters = O.lsqr_complex(apply_a, apply_a, b, 0.01, 50, return_iters=True)
+    x_conv = O.lsqr_complex(apply_a, apply_a, b, 1e-12, 2000)
+    assert iters == 50 and rel(x_ref, x_conv) > 0.1
+    x_ref1 = x_ref + O.lsqr_complex(apply_a, apply_a, b - apply_a(x_ref), 0.01, 50)
+    assert rel(x_ref1, x_ref) > 0.1 and rel(x_ref1, x_conv) < rel(x_ref, x_conv)
+
+
 # ------------------------------------------------------------------------------ TGV --
 def test_tgv_erode_mask():
     """src/inversion/tgv.rs:1335-1347: 5^3 all-ones mask, one erosion keeps the centre."""
