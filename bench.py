@@ -32,12 +32,24 @@ import numpy as np  # noqa: E402
 DIMS = (256, 256, 176)
 ITERS = 250
 METRIC = "TV-ADMM volumes/s at 256x256x176 (250 iterations)"
-# DRAM bytes (read + write) per launch of the dominant kernels, from one ncu --set full
-# capture of this workload (profiles/tv_admm_256x256x176_kernels.md); ncu flushes the
-# caches before each replay, so these are cold-cache figures.
-NCU_TRAFFIC = {"tv_step": 434251520, "fft_z_fused": 75313408}
-NCU_TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/tv_admm_256x256x176_kernels.md"
 UNIT = "volumes/s"
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "tv_admm_256x256x176_dram.txt")
+
+
+def ncu_traffic():
+    """DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the TV-ADMM
+    kernels at this workload, from the committed summary of one ncu capture ("name bytes"
+    lines; ncu flushes the caches before each replay, so these are cold-cache figures)."""
+    out = {}
+    try:
+        with open(TRAFFIC_FILE) as fh:
+            for line in fh:
+                parts = line.split("#", 1)[0].split()
+                if len(parts) == 2:
+                    out[parts[0]] = int(parts[1])
+    except OSError:
+        pass
+    return out
 
 
 def parse():
@@ -50,64 +62,7 @@ def parse():
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-extras", action="store_true",
                     help="skip the full-chain and 32-volume batch measurements (reported beside the headline)")
-    ap.add_argument("--one-shot", type=int, default=0, metavar="ITERS",
-                    help="profiling aid: run one TV-ADMM solve of ITERS iterations (mixed) and exit")
-    ap.add_argument("--one-shot-precision", default="mixed", choices=["mixed", "f64"])
-    ap.add_argument("--one-shot-dims", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
-                    help="one-shot on a seeded N(0, 0.01) field of this grid (full mask) instead of the phantom")
-    ap.add_argument("--one-shot-tgv", type=int, nargs=4, default=None, metavar=("NX", "NY", "NZ", "ITERS"),
-                    help="profiling aid: one TGV solve (ellipsoid mask, seeded uniform wrapped phase, 0.6 mm) and exit")
     return ap.parse_args()
-
-
-def one_shot(args):
-    """Small, self-contained run for ncu captures: one full-size solve, no timing."""
-    import torch
-    import qsmgpu
-    from qsmgpu import Grid, inversion
-    dims = DIMS
-    if args.one_shot_dims:
-        dims = tuple(args.one_shot_dims)
-        n = dims[0] * dims[1] * dims[2]
-        f = np.random.default_rng(3).normal(0.0, 0.01, n)
-        mask = np.ones(n, np.uint8)
-    else:
-        f, mask = make_case(0)
-    dev = torch.device("cuda", 0)
-    d_f = torch.from_numpy(f.ravel()).to(dev)
-    d_m = torch.from_numpy(mask.ravel()).to(dev)
-    d_o = torch.empty(f.size, dtype=torch.float64, device=dev)
-    with qsmgpu.Context(0, args.one_shot_precision) as ctx:
-        inversion.tv_admm_device(ctx, d_f.data_ptr(), d_m.data_ptr(), Grid.new(*dims), (0.0, 0.0, 1.0),
-                                 inversion.TvParams(2e-4, 2e-2, 0.0, args.one_shot), d_o.data_ptr())
-    torch.cuda.synchronize()
-    print(f"one-shot ok: {args.one_shot} iterations, |chi|max={float(d_o.abs().max()):.4g}")
-
-
-def one_shot_tgv(args):
-    """Small, self-contained TGV run for ncu captures: ellipsoid mask (semi-axes 0.42/0.45/0.40
-    of the grid), phase uniform in [-3, 3] rad inside it, 0.6 mm voxels, tol 0."""
-    import torch
-    import qsmgpu
-    from qsmgpu import Grid, inversion
-    nx, ny, nz, iters = args.one_shot_tgv
-    dev = torch.device("cuda", 0)
-    z, y, x = torch.meshgrid(torch.arange(nz, device=dev, dtype=torch.float32),
-                             torch.arange(ny, device=dev, dtype=torch.float32),
-                             torch.arange(nx, device=dev, dtype=torch.float32), indexing="ij")
-    cx, cy, cz = (nx - 1) / 2, (ny - 1) / 2, (nz - 1) / 2
-    mask = (((x - cx) / (0.42 * nx)) ** 2 + ((y - cy) / (0.45 * ny)) ** 2 + ((z - cz) / (0.40 * nz)) ** 2) < 1
-    m8 = mask.reshape(-1).to(torch.uint8).contiguous()
-    g = torch.Generator(device=dev).manual_seed(1)
-    ph = ((torch.rand(nx * ny * nz, generator=g, device=dev, dtype=torch.float64) * 2 - 1) * 3.0 * m8.double())
-    ph = ph.contiguous()
-    out = torch.empty_like(ph)
-    with qsmgpu.Context(0, "mixed") as ctx:
-        inversion.tgv_qsm_device(ctx, ph.data_ptr(), m8.data_ptr(), Grid.new(nx, ny, nz, 0.6, 0.6, 0.6),
-                                 inversion.TgvParams(iterations=iters, tol=0.0, fieldstrength=3.0, te=0.020),
-                                 (0.0, 0.0, 1.0), out.data_ptr())
-    torch.cuda.synchronize()
-    print(f"one-shot tgv ok: {iters} iterations, |chi|max={float(out.abs().max()):.4g}")
 
 
 def make_case(seed):
@@ -196,7 +151,7 @@ def kernel_bytes_model(N, s):
         "tv_step": 10 * N * s,     # read x0, y_{i-1}, y_{i-2}, u(3); write u(3), div
         "fft_x_r2c": 2 * N * s,    # read div, write spectrum
         "fft_y_fwd": 2 * N * s,
-        "fft_z_fused": 2 * N * s,  # read + write spectrum (multiplier computed in-kernel)
+        "fft_z_fused": 2 * N * s + N * s // 2,  # read + write spectrum, read the real half-spectrum multiplier
         "fft_y_inv": 2 * N * s,
         "fft_x_c2r": 2 * N * s,    # read spectrum, write y_i
     }
@@ -250,6 +205,45 @@ def _fast_size(n):
         m += 1
 
 
+def _rel_l2(a, b):
+    a = np.asarray(a, np.float64).ravel()
+    b = np.asarray(b, np.float64).ravel()
+    return float(np.linalg.norm(a - b) / (np.linalg.norm(b) or 1.0))
+
+
+def _errs(a, b):
+    """rel-L2 and max-abs of a against the comparator b."""
+    return {"rel_l2": _rel_l2(a, b), "max_abs": float(np.abs(np.asarray(a, np.float64) - np.asarray(b, np.float64)).max())}
+
+
+def _profiled(ctx, fn):
+    """{kernel: (launches, total_ms)} of one call of fn with per-launch CUDA events."""
+    ctx.set_profiling(True)
+    ctx.profile_reset()
+    fn()
+    prof = ctx.profile()
+    ctx.set_profiling(False)
+    return prof
+
+
+def _dominant_roofline(prof, model, note):
+    """Roofline of the modelled kernel with the largest total time: algorithmic bytes
+    per launch (model) / average launch time, against the measured HBM peak."""
+    peak, kind = measured_peak()
+    cands = [k for k in model if k in prof]
+    if not cands:
+        return None
+    dom = max(cands, key=lambda k: prof[k][1])
+    cnt, tot = prof[dom]
+    avg_s = tot / max(cnt, 1) / 1e3
+    gbs = model[dom] / avg_s / 1e9
+    tot_all = sum(v[1] for v in prof.values()) or 1.0
+    return {"bound": "hbm", "kernel": dom, "launches": cnt, "avg_us": round(avg_s * 1e6, 2),
+            "alg_bytes": int(model[dom]), "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(gbs / peak, 3), "share": round(tot / tot_all, 3), "model": note,
+            "peak_source": kind}
+
+
 def _timed(stream, fn, reps=1):
     import torch
     e0 = torch.cuda.Event(enable_timing=True)
@@ -300,14 +294,22 @@ def bench_chain(local, dev):
         times = {"unwrap": _timed(s, st_unwrap), "vsharp": _timed(s, st_vsharp), "tv_admm": _timed(s, st_tv)}
         out[prec] = {"ms": {k: round(v, 3) for k, v in times.items()},
                      "arrays": (uw.cpu().numpy(), loc.cpu().numpy(), fm.cpu().numpy(), chi.cpu().numpy())}
+        if prec == "mixed":
+            # every V-SHARP FFT pass reads and writes one half spectrum (N*s bytes each way)
+            sz = 4
+            model = {k: 2 * N * sz for k in ("fft_x_r2c", "fft_y_fwd", "fft_z_fwd", "fft_z_inv", "fft_y_inv",
+                                              "fft_x_c2r", "fft_z_fused")}
+            out["roofline"] = _dominant_roofline(_profiled(ctx, st_vsharp), model,
+                                                 "FFT pass: read + write one float half spectrum, 2*N*4 B")
         ctx.close()
     a, b = out["mixed"]["arrays"], out["f64"]["arrays"]
-    rl = lambda x, y: float(np.linalg.norm(x - y) / (np.linalg.norm(y) or 1.0))
     return {"workload": "wrapped phase 256x256x176, 3 T, TE 20 ms -> laplacian_unwrap -> vsharp (12 radii) -> "
                         f"tv_admm x{ITERS}; synthetic brain-mask phantom with 4 background dipoles",
             "ms_mixed": out["mixed"]["ms"], "ms_f64": out["f64"]["ms"],
-            "rel_l2_mixed_vs_fp64": {"unwrap": rl(a[0], b[0]), "vsharp": rl(a[1], b[1]), "tv_admm": rl(a[3], b[3])},
-            "vsharp_mask_equal": bool(np.array_equal(a[2], b[2]))}
+            "errors_mixed_vs_fp64_gpu": {"unwrap": _errs(a[0], b[0]), "vsharp": _errs(a[1], b[1]),
+                                          "tv_admm": _errs(a[3], b[3])},
+            "vsharp_mask_equal": bool(np.array_equal(a[2], b[2])),
+            "vsharp_roofline_mixed": out.get("roofline")}
 
 
 def bench_batch(local, dev, n_vol=32, seed=7):
@@ -348,17 +350,129 @@ def bench_batch(local, dev, n_vol=32, seed=7):
     inversion.tv_admm_batch_device(ctx, cases, p)  # warm-up
     t_batch = _timed(s, lambda: inversion.tv_admm_batch_device(ctx, cases, p))
     one_by_one = lambda: [inversion.tv_admm_device(ctx, df, dm, g, b, p, do) for df, dm, do, g, b in cases]
+    # the batch's own results, before the one-call-per-volume run overwrites the outputs
+    res32 = [keep[3 * i + 2].cpu().numpy() for i in range(n_vol)]
     one_by_one()  # warm-up: grows the single-volume workspace to the largest volume
     t_seq = _timed(s, one_by_one)
     tk = inversion.TkdParams(0.19)
     inversion.tkd_batch_device(ctx, cases, tk)
     t_tkd = _timed(s, lambda: inversion.tkd_batch_device(ctx, cases, tk), reps=3)
+    tkd32 = [keep[3 * i + 2].cpu().numpy() for i in range(n_vol)]
     ctx.close()
+    # the same batch in FP64 (the plain comparator), batched
+    c64 = qsmgpu.Context(local, "f64")
+    s64 = torch.cuda.ExternalStream(c64.stream_handle(), device=dev)
+    inversion.tv_admm_batch_device(c64, cases, p)
+    t_b64 = _timed(s64, lambda: inversion.tv_admm_batch_device(c64, cases, p))
+    res64 = [keep[3 * i + 2].cpu().numpy() for i in range(n_vol)]
+    inversion.tkd_batch_device(c64, cases, tk)
+    t_tkd64 = _timed(s64, lambda: inversion.tkd_batch_device(c64, cases, tk), reps=3)
+    tkd64 = [keep[3 * i + 2].cpu().numpy() for i in range(n_vol)]
+    c64.close()
+    worst = lambda xs, ys: {"rel_l2_max_over_volumes": max(_rel_l2(x, y) for x, y in zip(xs, ys)),
+                            "max_abs": max(float(np.abs(x - y).max()) for x, y in zip(xs, ys))}
     return {"workload": f"{n_vol} volumes of uneven size (2^a 3^b 5^c in 96-224 x 96-224 x 64-160), B0 tilted "
-                        f"<= 25 deg, TV-ADMM x{ITERS} + TKD 0.19, mixed; {vox / 1e6:.1f} M voxels in total",
-            "tv_admm_batched": {"volumes_per_s": round(n_vol / (t_batch / 1e3), 3), "ms": round(t_batch, 2)},
-            "tv_admm_one_call_per_volume": {"volumes_per_s": round(n_vol / (t_seq / 1e3), 3), "ms": round(t_seq, 2)},
-            "tkd_batched": {"volumes_per_s": round(n_vol / (t_tkd / 1e3), 3), "ms": round(t_tkd, 3)}}
+                        f"<= 25 deg, TV-ADMM x{ITERS} + TKD 0.19; {vox / 1e6:.1f} M voxels in total",
+            "tv_admm_batched_mixed": {"volumes_per_s": round(n_vol / (t_batch / 1e3), 3), "ms": round(t_batch, 2)},
+            "tv_admm_batched_fp64": {"volumes_per_s": round(n_vol / (t_b64 / 1e3), 3), "ms": round(t_b64, 2)},
+            "tv_admm_one_call_per_volume_mixed": {"volumes_per_s": round(n_vol / (t_seq / 1e3), 3),
+                                                  "ms": round(t_seq, 2)},
+            "batched_mixed_over_batched_fp64": round(t_b64 / t_batch, 3),
+            "tv_admm_errors_mixed_vs_fp64_gpu": worst(res32, res64),
+            "tkd_batched_mixed": {"volumes_per_s": round(n_vol / (t_tkd / 1e3), 3), "ms": round(t_tkd, 3)},
+            "tkd_batched_fp64": {"volumes_per_s": round(n_vol / (t_tkd64 / 1e3), 3), "ms": round(t_tkd64, 3)},
+            "tkd_errors_mixed_vs_fp64_gpu": worst(tkd32, tkd64)}
+
+
+def bench_batch_brain(local, dev, n_vol=4):
+    """A batch of n_vol 256x256x176 volumes (the throughput phantom with seeds 0..n-1),
+    TV-ADMM x250: batched mixed precision against the plain FP64 form (one FP64 call per
+    volume)."""
+    import torch
+    import qsmgpu
+    from qsmgpu import Grid, inversion
+    grid = Grid.new(*DIMS)
+    keep, cases = [], []
+    for k in range(n_vol):
+        f, m = make_case(k)
+        df = torch.from_numpy(f.ravel()).to(dev)
+        dm = torch.from_numpy(m.ravel()).to(dev)
+        do = torch.empty_like(df)
+        keep += [df, dm, do]
+        cases.append((df.data_ptr(), dm.data_ptr(), do.data_ptr(), grid, (0.0, 0.0, 1.0)))
+    p = inversion.TvParams(2e-4, 2e-2, 0.0, ITERS)
+    ctx = qsmgpu.Context(local, "mixed")
+    s = torch.cuda.ExternalStream(ctx.stream_handle(), device=dev)
+    inversion.tv_admm_batch_device(ctx, cases, p)
+    t_b = _timed(s, lambda: inversion.tv_admm_batch_device(ctx, cases, p))
+    r32 = [keep[3 * i + 2].cpu().numpy() for i in range(n_vol)]
+    ctx.close()
+    c64 = qsmgpu.Context(local, "f64")
+    s64 = torch.cuda.ExternalStream(c64.stream_handle(), device=dev)
+    plain = lambda: [inversion.tv_admm_device(c64, df, dm, g, b, p, do) for df, dm, do, g, b in cases]
+    plain()
+    t_64 = _timed(s64, plain)
+    r64 = [keep[3 * i + 2].cpu().numpy() for i in range(n_vol)]
+    c64.close()
+    return {"workload": f"{n_vol} volumes of 256x256x176 (throughput phantom, seeds 0..{n_vol - 1}), tv_admm x{ITERS}",
+            "batched_mixed": {"volumes_per_s": round(n_vol / (t_b / 1e3), 3), "ms": round(t_b, 2)},
+            "plain_fp64": {"volumes_per_s": round(n_vol / (t_64 / 1e3), 3), "ms": round(t_64, 2)},
+            "batched_mixed_over_plain_fp64": round(t_64 / t_b, 3),
+            "errors_mixed_vs_fp64_gpu": {"rel_l2_max_over_volumes": max(_rel_l2(a, b) for a, b in zip(r32, r64)),
+                                         "max_abs": max(float(np.abs(a - b).max()) for a, b in zip(r32, r64))}}
+
+
+def bench_batch_sharded(local, dev, rank, world, dist, n_vol=32, seed=7):
+    """The 32-volume TV-ADMM batch (mixed) sharded over the ranks: every rank draws the
+    same batch description, keeps the volumes the longest-processing-time placement gives
+    it (qsm_batch_partition) and solves them as one batched call; no collective while
+    solving.  Time = max over ranks (device events); the results stay on their ranks."""
+    import torch
+    import qsmgpu
+    from qsmgpu import Grid, inversion, phantom, shard
+    rng = np.random.default_rng(seed)
+    desc = []
+    for _ in range(n_vol):
+        nx, ny = (_fast_size(int(rng.integers(96, 225))) for _ in range(2))
+        nz = _fast_size(int(rng.integers(64, 161)))
+        th, ph = np.radians(rng.uniform(0, 25)), rng.uniform(0, 2 * np.pi)
+        desc.append((Grid.new(nx, ny, nz), (float(np.sin(th) * np.cos(ph)), float(np.sin(th) * np.sin(ph)),
+                                            float(np.cos(th))), int(rng.integers(1 << 30))))
+    mine = shard.share([d[0] for d in desc], rank, world, [ITERS] * n_vol)
+    ctx = qsmgpu.Context(local, "mixed")
+    s = torch.cuda.ExternalStream(ctx.stream_handle(), device=dev)
+    keep, cases = [], []
+    for b in mine:
+        grid, bdir, vseed = desc[b]
+        nz, ny, nx = grid.shape
+        vr = np.random.default_rng(vseed)
+        mask = phantom.ellipsoid_mask(grid.shape, (0.4 * nx, 0.45 * ny, 0.4 * nz))
+        chi = np.zeros(grid.shape)
+        ctr = ((nx - 1) / 2, (ny - 1) / 2, (nz - 1) / 2)
+        phantom.add_ellipsoids(chi, vr, 8, [(c - 0.25 * n, c + 0.25 * n) for c, n in zip(ctr, (nx, ny, nz))],
+                               semi=(3.0, 10.0))
+        dchi = torch.from_numpy((chi * mask).ravel()).to(dev)
+        f = torch.empty_like(dchi)
+        inversion.dipole_forward_device(ctx, dchi.data_ptr(), grid, bdir, f.data_ptr())
+        f += torch.from_numpy(vr.normal(0.0, 0.01, size=chi.size) * mask.ravel()).to(dev)
+        dm = torch.from_numpy(mask.ravel()).to(dev)
+        do = torch.empty_like(f)
+        keep += [f, dm, do]
+        cases.append((f.data_ptr(), dm.data_ptr(), do.data_ptr(), grid, bdir))
+    p = inversion.TvParams(2e-4, 2e-2, 0.0, ITERS)
+    run = lambda: inversion.tv_admm_batch_device(ctx, cases, p) if cases else None
+    run()
+    dist.barrier()
+    torch.cuda.synchronize()
+    ms = _timed(s, run)
+    t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ctx.close()
+    ms = float(t.item())
+    return {"workload": f"{n_vol} uneven volumes (as batch_32_volumes), tv_admm x{ITERS} mixed, placed over {world} "
+                        "GPUs by longest-processing-time on N log N x iterations",
+            "volumes_per_s": round(n_vol / (ms / 1e3), 3), "ms_max_over_ranks": round(ms, 2),
+            "volumes_on_rank0": len(mine) if rank == 0 else None}
 
 
 def bench_adjoint(local, dev):
@@ -374,7 +488,9 @@ def bench_adjoint(local, dev):
     grid = Grid.new(*dims)
     out = {"workload": "unrolled tv_admm 160x192x160, K=50, checkpoint every 10, lambda 1e-3, rho 2e-2, mixed; "
                        "ellipsoid phantom"}
-    for prec in ("mixed", "f64"):
+    gchi64 = None
+    res = {}
+    for prec in ("f64", "mixed"):
         ctx = qsmgpu.Context(local, prec)
         s = torch.cuda.ExternalStream(ctx.stream_handle(), device=dev)
         f = torch.from_numpy(np.ascontiguousarray(case.local_field).ravel()).to(dev)
@@ -383,23 +499,32 @@ def bench_adjoint(local, dev):
         chi = torch.empty_like(f)
         gf = torch.empty_like(f)
         gchi = torch.empty_like(f)
+        glam = [0.0]
 
         def fwd():
             inversion.tv_admm_unrolled_vjp_device(ctx, f.data_ptr(), m.data_ptr(), grid, (0.0, 0.0, 1.0), 1e-3, 2e-2,
                                                   50, 10, 0, chi.data_ptr())
 
         def fwd_bwd():
-            inversion.tv_admm_unrolled_vjp_device(ctx, f.data_ptr(), m.data_ptr(), grid, (0.0, 0.0, 1.0), 1e-3, 2e-2,
-                                                  50, 10, gchi.data_ptr(), chi.data_ptr(), gf.data_ptr())
+            glam[0] = inversion.tv_admm_unrolled_vjp_device(ctx, f.data_ptr(), m.data_ptr(), grid, (0.0, 0.0, 1.0),
+                                                            1e-3, 2e-2, 50, 10, gchi.data_ptr(), chi.data_ptr(),
+                                                            gf.data_ptr())
 
         fwd()
-        gchi.copy_(2.0 * (chi - truth))
+        # dL/dchi_K of L = ||chi_K - chi_true||^2, taken from the FP64 forward pass for both
+        if gchi64 is None:
+            gchi64 = (2.0 * (chi - truth)).clone()
+        gchi.copy_(gchi64)
         fwd_bwd()
+        res[prec] = (chi.cpu().numpy(), gf.cpu().numpy(), float(glam[0]))
         t_f = _timed(s, fwd, reps=2)
         t_fb = _timed(s, fwd_bwd, reps=2)
         out[prec] = {"forward_ms": round(t_f, 2), "forward_plus_vjp_ms": round(t_fb, 2),
                      "vjp_over_forward": round((t_fb - t_f) / t_f, 3)}
         ctx.close()
+    a, b = res["mixed"], res["f64"]
+    out["errors_mixed_vs_fp64_gpu"] = {"chi_K": _errs(a[0], b[0]), "dL_dfield": _errs(a[1], b[1]),
+                                       "dL_dlambda_rel": abs(a[2] - b[2]) / (abs(b[2]) or 1.0)}
     return out
 
 
@@ -463,16 +588,39 @@ def bench_multi_echo(local, dev, seed=5):
     fit_bytes = (2 * len(tes) * 8 + 1 + 3 * 8 + 1) * N
     ppm = (fit_f / w0).contiguous()
     ctx.close()
+    il = inversion.IlsqrParams()
+    il_out, il_ms = {}, {}
+    prof_il = None
+    for name, prec, kry in (("fp64", "f64", "f64"), ("mixed", "mixed", "f64"), ("mixed_float_krylov", "mixed", "mixed")):
+        c = qsmgpu.Context(local, prec)
+        c.krylov_precision = kry
+        sc = torch.cuda.ExternalStream(c.stream_handle(), device=dev)
+        o = [torch.empty_like(field) for _ in range(4)]
+
+        def run_ilsqr():
+            inversion.ilsqr_device(c, ppm.data_ptr(), m8.data_ptr(), grid, (0.0, 0.0, 1.0), il, o[0].data_ptr(),
+                                   o[1].data_ptr(), o[2].data_ptr(), o[3].data_ptr())
+
+        run_ilsqr()
+        il_ms[name] = round(_timed(sc, run_ilsqr), 2)
+        il_out[name] = [t.cpu().numpy() for t in o]
+        if name == "mixed":
+            prof_il = _profiled(c, run_ilsqr)
+        c.close()
+        del o
+    names = ("chi", "xsa", "xfs", "xlsqr")
+    il_err = {v: {k: _errs(a, b) for k, a, b in zip(names, il_out[v], il_out["fp64"])}
+              for v in ("mixed", "mixed_float_krylov")}
+    # the LSQR loop's passes run on full complex FP64 spectra (16 B per value) in the default mixed
+    # context: Z inverse with the dipole scale reads x and writes t, the fused X pass reads t and
+    # the weights and writes t, the Z forward epilogue reads t and the previous vector and writes
+    sd = 16
+    il_model = {"fft_z_inv": 2 * N * sd, "fft_y_inv": 2 * N * sd, "fft_y_fwd": 2 * N * sd,
+                "fft_x_lsqr": 2 * N * sd + N * 8, "fft_z_lsqr": 3 * N * sd}
+    il_roof = _dominant_roofline(prof_il, il_model, "LSQR passes on full complex FP64 spectra: read + write one "
+                                                    "spectrum (2*N*16 B), + weights (fused X), + previous vector (Z out)")
     cm = qsmgpu.Context(local, "mixed")
     sm = torch.cuda.ExternalStream(cm.stream_handle(), device=dev)
-    chi_out = torch.empty_like(field)
-    il = inversion.IlsqrParams()
-
-    def run_ilsqr():
-        inversion.ilsqr_device(cm, ppm.data_ptr(), m8.data_ptr(), grid, (0.0, 0.0, 1.0), il, chi_out.data_ptr())
-
-    run_ilsqr()
-    t_il = _timed(sm, run_ilsqr)
     wrapped = torch.remainder(phases[2] + np.pi, 2 * np.pi) - np.pi
     wrapped = (wrapped * m8.to(torch.float64)).contiguous()
     tg = inversion.TgvParams(iterations=1000, tol=0.0, fieldstrength=3.0, te=0.020)
@@ -483,12 +631,42 @@ def bench_multi_echo(local, dev, seed=5):
 
     run_tgv()
     t_tgv = _timed(sm, run_tgv)
+    tg_prof = inversion.TgvParams(iterations=20, tol=0.0, fieldstrength=3.0, te=0.020)
+    prof_tgv = _profiled(cm, lambda: inversion.tgv_qsm_device(cm, wrapped.data_ptr(), m8.data_ptr(), grid, tg_prof,
+                                                              (0.0, 0.0, 1.0), tgv_out.data_ptr()))
     cm.close()
+    # TGV works on the bounding box (padding 2) of mask0 = erode^(erosions+1)(mask), with
+    # mask_eroded = erode^erosions(mask) (6-neighbour erosion that also clears the faces)
+    mk = m8.reshape(nz, ny, nx).bool()
+    m_eroded = mk
+    for e in range(tg.erosions + 1):
+        if e == tg.erosions:
+            m_eroded = mk
+        pad = torch.nn.functional.pad(mk[None, None].to(torch.float32), (1, 1, 1, 1, 1, 1))[0, 0] > 0
+        mk = (pad[1:-1, 1:-1, 1:-1] & pad[:-2, 1:-1, 1:-1] & pad[2:, 1:-1, 1:-1] & pad[1:-1, :-2, 1:-1] &
+              pad[1:-1, 2:, 1:-1] & pad[1:-1, 1:-1, :-2] & pad[1:-1, 1:-1, 2:])
+    m0 = mk
+    idx = m0.nonzero()
+    lo = (idx.min(0).values - 2).clamp_min(0)
+    hi = torch.minimum(idx.max(0).values + 3, torch.tensor([nz, ny, nx], device=dev))
+    box = lambda a: a[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]]
+    V = int(box(m0).numel())
+    V0 = int(box(m0).sum())
+    Vm = int(box(m_eroded).sum())
+    # bytes per box voxel: dual reads both masks and chi; inside mask0 phi, lphi, eta (r+w), q (r+w);
+    # inside the eroded mask p (r+w) and w.  Primal reads both masks, phi, chi, w and writes phi, chi,
+    # w twice (iterate and extrapolation); inside mask0 eta and p; inside the eroded mask q.
+    tgv_model = {"tgv_dual": 6 * V + 64 * V0 + 36 * Vm, "tgv_primal": 62 * V + 16 * V0 + 24 * Vm}
+    tgv_roof = _dominant_roofline(prof_tgv, tgv_model, "compulsory bytes per box voxel by mask membership: "
+                                                       "dual 6 + 64 (mask0) + 36 (eroded mask), primal 62 + 16 + 24")
     return {"workload": "384x384x256 at 0.6 mm, 3 T, 4 echoes TE 4/12/20/28 ms, 40 cylinders chi 0.3-0.6 ppm; "
                         "synthetic phantom",
             "linear_fit_fp64": {"ms": round(t_fit, 3), "fit_kernel_alg_gb": round(fit_bytes / 1e9, 3),
                                 "note": "ms covers the fit kernel and the reliability percentile (radix select)"},
-            "ilsqr_mixed_ms": round(t_il, 2), "tgv_1000_iterations_ms": round(t_tgv, 2)}
+            "ilsqr_ms": il_ms, "ilsqr_errors_vs_fp64_gpu": il_err, "ilsqr_roofline_mixed": il_roof,
+            "tgv_1000_iterations_ms": round(t_tgv, 2),
+            "tgv_box": {"voxels": V, "mask0": V0, "eroded_mask": Vm}, "tgv_roofline": tgv_roof,
+            "tgv_note": "float32 as in the reference (src/inversion/tgv.rs); no FP64 comparator exists"}
 
 
 def run_reference(args):
@@ -528,12 +706,6 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
-        return
-    if args.one_shot_tgv:
-        one_shot_tgv(args)
-        return
-    if args.one_shot:
-        one_shot(args)
         return
 
     import torch
@@ -641,9 +813,11 @@ def main():
         v["share"] = round(v["total_ms"] / tot_all, 3)
     dom = max((n for n in kernels if n in model), key=lambda n: kernels[n]["total_ms"])
     iter_bytes = 20 * N * 4
+    traffic = ncu_traffic()
     roofline = {"bound": "hbm", "achieved": kernels[dom]["gbs"], "peak": peak, "unit": "GB/s",
-                "frac": round(kernels[dom]["gbs"] / peak, 3), "traffic": NCU_TRAFFIC.get(dom), "kernel": dom,
-                "traffic_source": NCU_TRAFFIC_SOURCE if dom in NCU_TRAFFIC else None,
+                "frac": round(kernels[dom]["gbs"] / peak, 3), "traffic": traffic.get(dom), "kernel": dom,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, one capture of this "
+                                  "workload" if dom in traffic else None,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
                 "fallback 6.65 TB/s",
                 "iteration_model_gbs": round(iter_bytes / (ms_step / ITERS / 1e3) / 1e9, 1),
@@ -675,9 +849,14 @@ def main():
                  "rel_l2_mixed_vs_fp64": err, "max_abs_mixed_vs_fp64": float(np.abs(chi_mixed - chi64).max())}
         ctx64.close()
 
+    if world > 1 and not args.skip_extras:
+        sharded = bench_batch_sharded(local, dev, rank, world, dist)
+        if rank == 0:
+            extra["batch_32_volumes_sharded"] = sharded
     if rank == 0 and world == 1 and not args.skip_extras:
         extra["chain_256x256x176"] = bench_chain(local, dev)
         extra["batch_32_volumes"] = bench_batch(local, dev)
+        extra["batch_4x256x256x176"] = bench_batch_brain(local, dev)
         extra["unrolled_adjoint_160x192x160"] = bench_adjoint(local, dev)
         extra["multi_echo_384x384x256"] = bench_multi_echo(local, dev)
 

@@ -103,6 +103,16 @@ QSM_API int qsm_ctx_get_plan_mode(const qsm_ctx* ctx);
  * 2e-3 relative L2 from the reference).  An FP64 context always runs double. */
 QSM_API qsm_status qsm_ctx_set_krylov_precision(qsm_ctx* ctx, int precision);
 QSM_API int qsm_ctx_get_krylov_precision(const qsm_ctx* ctx);
+/* Input check (no reference counterpart; off by default, as the reference lets NaN and
+ * infinities propagate into the result).  When on, every solver first scans its input
+ * volume and returns QSM_ERR_INVALID_ARGUMENT, naming the count, if a voxel is NaN or
+ * infinite. */
+QSM_API qsm_status qsm_ctx_set_input_check(qsm_ctx* ctx, int on);
+/* Fault injection for callers' error-path tests: after `after` more successful device
+ * allocations, the context's next allocation fails with QSM_ERR_ALLOC (the failure is
+ * simulated on the host; nothing reaches the GPU), then allocations succeed again.  A
+ * negative value cancels.  The context stays usable after the failed call. */
+QSM_API qsm_status qsm_ctx_inject_alloc_failure(qsm_ctx* ctx, long long after);
 /* 1 when every axis length of `grid` has a transform plan: lengths up to 4096 whose prime
  * factors are at most 13, and any length up to 2048 (a Bluestein transform). */
 QSM_API int qsm_grid_supported(const qsm_grid* grid);
@@ -268,6 +278,14 @@ QSM_API qsm_status qsm_ilsqr_device(qsm_ctx* ctx, const double* d_local_field, c
                                     const qsm_grid* grid, const double bdir[3], const qsm_ilsqr_params* params,
                                     qsm_progress_fn progress, void* user, double* d_out_chi, double* d_out_xsa,
                                     double* d_out_xfs, double* d_out_xlsqr);
+/* The operator of iLSQR's LSQR step — the apply_a closure of lsqr_step,
+ * src/inversion/ilsqr.rs:988-1010: y = D * FFT(w * Re(IFFT(D * x))), D the dipole kernel
+ * of (grid, bdir).  x and y are full complex spectra of nx*ny*nz values (interleaved re,
+ * im; Fortran order; 16-byte aligned device memory), w is real (nx*ny*nz values).  Runs
+ * the five passes of the solver's own loop, in float in a mixed context (whatever its
+ * Krylov precision) and in double otherwise. */
+QSM_API qsm_status qsm_ilsqr_lsqr_operator_device(qsm_ctx* ctx, const qsm_grid* grid, const double bdir[3],
+                                                  const double* d_weights, const double* d_x, double* d_y);
 /* inversion::tgv_qsm — src/inversion/tgv.rs:1045-1299: susceptibility (ppm) from WRAPPED
  * phase, parameters before the field direction as in the reference.  Progress is
  * (iter, iterations) for every iteration started, then (final_iter, iterations).  The

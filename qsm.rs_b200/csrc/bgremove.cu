@@ -545,6 +545,7 @@ void check_io(const void* a, const void* m, const void* o) {
 void unwrap_device(qsm_ctx* ctx, const double* ph, const uint8_t* m, const qsm_grid* grid, double* out) {
   GridDims d = check_grid(grid);
   check_io(ph, m, out);
+  check_volume_finite(ctx, ph, d.n, "phase");
   if (ctx->precision == QSM_PRECISION_MIXED) unwrap_impl<float>(ctx, d, ph, m, out);
   else unwrap_impl<double>(ctx, d, ph, m, out);
 }
@@ -552,6 +553,7 @@ void unwrap_device(qsm_ctx* ctx, const double* ph, const uint8_t* m, const qsm_g
 void smv_device(qsm_ctx* ctx, const double* f, const uint8_t* m, const GridDims& d, double radius, double* ol,
                 uint8_t* om) {
   check_finite(radius, "radius");
+  check_volume_finite(ctx, f, d.n, "field");
   if (ctx->precision == QSM_PRECISION_MIXED) smv_impl<float>(ctx, d, f, m, radius, ol, om);
   else smv_impl<double>(ctx, d, f, m, radius, ol, om);
 }
@@ -561,6 +563,7 @@ void ismv_device(qsm_ctx* ctx, const double* f, const uint8_t* m, const GridDims
   check_ptr(p, "params");
   check_finite(p->radius, "radius");
   if (std::isnan(p->tol)) throw QsmError(QSM_ERR_INVALID_ARGUMENT, "tol is NaN");
+  check_volume_finite(ctx, f, d.n, "field");
   if (ctx->precision == QSM_PRECISION_MIXED) ismv_impl<float>(ctx, d, f, m, *p, progress, user, ol, om);
   else ismv_impl<double>(ctx, d, f, m, *p, progress, user, ol, om);
 }
@@ -569,6 +572,7 @@ void sharp_device(qsm_ctx* ctx, const double* f, const uint8_t* m, const GridDim
                   double* ol, uint8_t* om) {
   check_finite(thr, "threshold");
   check_finite(radius, "radius");
+  check_volume_finite(ctx, f, d.n, "field");
   if (ctx->precision == QSM_PRECISION_MIXED) sharp_impl<float>(ctx, d, f, m, thr, radius, ol, om);
   else sharp_impl<double>(ctx, d, f, m, thr, radius, ol, om);
 }
@@ -579,6 +583,7 @@ void vsharp_device(qsm_ctx* ctx, const double* f, const uint8_t* m, const GridDi
   if (n_radii > 0) check_ptr(radii, "radii");
   std::vector<double> r(radii, radii + n_radii);
   for (double v : r) check_finite(v, "radius");
+  check_volume_finite(ctx, f, d.n, "field");
   const size_t N = (size_t)d.n;
   if (r.empty()) {  // src/bgremove/vsharp.rs:98-100
     QSM_CUDA(cudaMemsetAsync(ol, 0, N * sizeof(double), ctx->stream));

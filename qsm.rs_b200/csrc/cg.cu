@@ -353,6 +353,7 @@ void resharp_device(qsm_ctx* ctx, const double* field, const uint8_t* mask, cons
   check_ptr(out_mask, "out_mask");
   check_ptr(p, "params");
   check_finite(p->radius, "radius");
+  check_volume_finite(ctx, field, d.n, "field");
   check_finite(p->tik_reg, "tik_reg");
   if (std::isnan(p->tol)) throw QsmError(QSM_ERR_INVALID_ARGUMENT, "tol is NaN");
   if (ctx->precision == QSM_PRECISION_MIXED)

@@ -8,6 +8,43 @@
 
 namespace qsm {
 
+cudaError_t ctx_malloc(qsm_ctx* ctx, void** p, size_t bytes) {
+  if (ctx->alloc_fail_after == 0) {
+    ctx->alloc_fail_after = -1;  // one injected failure, then allocations succeed again
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  if (ctx->alloc_fail_after > 0) ctx->alloc_fail_after--;
+  return cudaMalloc(p, bytes);
+}
+
+namespace {
+__global__ void k_count_nonfinite(long long n, const double* __restrict__ a, unsigned long long* count) {
+  unsigned long long c = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    c += isfinite(a[i]) ? 0ull : 1ull;
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
+}
+}  // namespace
+
+void check_volume_finite(qsm_ctx* ctx, const double* d, long long n, const char* name) {
+  if (!ctx->check_inputs || n <= 0) return;
+  unsigned long long* cnt = ws<unsigned long long>(ctx, "check.count", 1);
+  QSM_CUDA(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), ctx->stream));
+  long long blocks = (n + 255) / 256;
+  if (blocks > 148LL * 8) blocks = 148LL * 8;
+  LaunchScope ls(ctx, "check_finite");
+  k_count_nonfinite<<<(unsigned)blocks, 256, 0, ctx->stream>>>(n, d, cnt);
+  ls.done();
+  unsigned long long h = 0;
+  d2h(ctx, &h, cnt, sizeof(h));
+  sync(ctx);
+  if (h != 0)
+    throw QsmError(QSM_ERR_INVALID_ARGUMENT, std::string(name) + " has " + std::to_string(h) +
+                                                 " non-finite voxel(s) (NaN or infinity)");
+}
+
 void* ws_get(qsm_ctx* ctx, const std::string& name, size_t bytes) {
   if (bytes == 0) bytes = 16;
   DevBuf& b = ctx->ws[name];
@@ -22,7 +59,7 @@ void* ws_get(qsm_ctx* ctx, const std::string& name, size_t bytes) {
       b.bytes = 0;
     }
     void* p = nullptr;
-    cudaError_t e = cudaMalloc(&p, bytes);
+    cudaError_t e = ctx_malloc(ctx, &p, bytes);
     if (e != cudaSuccess) {
       (void)cudaGetLastError();
       throw QsmError(QSM_ERR_ALLOC, "device allocation of " + std::to_string(bytes) + " bytes for '" + name +
@@ -104,7 +141,7 @@ const void* twiddle_table(qsm_ctx* ctx, const FftPlan1D& pl, bool dbl) {
   if (it != ctx->twiddles.end()) return it->second;
   const std::vector<unsigned char> host = transform_table(pl, dbl);
   void* d = nullptr;
-  cudaError_t e = cudaMalloc(&d, host.size());
+  cudaError_t e = ctx_malloc(ctx, &d, host.size());
   if (e != cudaSuccess) {
     (void)cudaGetLastError();
     throw QsmError(QSM_ERR_ALLOC, "twiddle table allocation failed");
@@ -118,7 +155,7 @@ const void* upload_table(qsm_ctx* ctx, const std::string& key, const void* host,
   auto it = ctx->tables.find(key);
   if (it != ctx->tables.end()) return it->second;
   void* d = nullptr;
-  cudaError_t e = cudaMalloc(&d, bytes ? bytes : 16);
+  cudaError_t e = ctx_malloc(ctx, &d, bytes ? bytes : 16);
   if (e != cudaSuccess) {
     (void)cudaGetLastError();
     throw QsmError(QSM_ERR_ALLOC, "table allocation failed");
@@ -333,6 +370,18 @@ qsm_status qsm_ctx_set_krylov_precision(qsm_ctx* ctx, int precision) {
 }
 
 int qsm_ctx_get_krylov_precision(const qsm_ctx* ctx) { return ctx ? ctx->krylov_precision : -1; }
+
+qsm_status qsm_ctx_set_input_check(qsm_ctx* ctx, int on) {
+  if (ctx == nullptr) return QSM_ERR_INVALID_ARGUMENT;
+  ctx->check_inputs = on != 0;
+  return QSM_OK;
+}
+
+qsm_status qsm_ctx_inject_alloc_failure(qsm_ctx* ctx, long long after) {
+  if (ctx == nullptr) return QSM_ERR_INVALID_ARGUMENT;
+  ctx->alloc_fail_after = after < 0 ? -1 : after;
+  return QSM_OK;
+}
 
 qsm_status qsm_ctx_release_workspace(qsm_ctx* ctx) {
   if (ctx == nullptr) return QSM_ERR_INVALID_ARGUMENT;

@@ -340,55 +340,6 @@ __device__ __forceinline__ void run_stages(const FftPlan1D& pl, int t, bool acti
   }
 }
 
-// Bluestein (chirp-z) transform of one pencil of length n through a cyclic convolution
-// of length m >= 2n - 1 (Bluestein 1970; Rabiner, Schafer and Rader 1969).  With
-// q_j = exp(DIR i pi j^2 / n), jk = (j^2 + k^2 - (k - j)^2) / 2 gives
-//   X_k = q_k * sum_j (x_j q_j) conj(q_{k-j}),
-// a convolution of a_j = x_j q_j (zero-padded to m) with the conjugate chirp.  The table
-// holds c_j = exp(-i pi j^2 / n) (so q = c forward, conj(c) inverse) and K = DFT_m of the
-// conjugate chirp wrapped cyclically, divided by m.  That sequence is even, so K is even
-// and the inverse direction's kernel spectrum is conj(K).  The pencil's slot holds m
-// elements; the length-m transforms run in place with the plan's stages and twiddles.
-template <int DIR, typename C, class SA, bool SRC_G, bool DST_G>
-__device__ __forceinline__ void bluestein_pencil(const FftPlan1D& pl, int t, bool active, C* sp, const SA& sa,
-                                                 const C* tw, const C* gsrc, C* gdst, long long base,
-                                                 long long stride) {
-  const int n = pl.n, m = pl.m, T = pl.T;
-  const C* chirp = static_cast<const C*>(pl.ext);
-  const C* kspec = chirp + n;
-  if (active) {
-    for (int j = t; j < m; j += T) {
-      C a = mk<C>(decltype(a.x)(0), decltype(a.x)(0));
-      if (j < n) {
-        C x;
-        if constexpr (SRC_G) x = gsrc[base + j * stride];
-        else x = sp[sa(j)];
-        const C c = chirp[j];
-        a = (DIR < 0) ? cmul(x, c) : cmulc(x, c);
-      }
-      sp[sa(j)] = a;
-    }
-  }
-  __syncthreads();
-  auto fetch = [&](int e) -> C { return sp[sa(e)]; };
-  auto emit_k = [&](int e, C v) {
-    const C k = kspec[e];
-    sp[sa(e)] = (DIR < 0) ? cmul(v, k) : cmulc(v, k);
-  };
-  run_stages<-1>(pl, t, active, sp, sa, tw, fetch, emit_k);
-  auto emit_out = [&](int e, C v) {
-    if (e < n) {
-      const C c = chirp[e];
-      const C y = (DIR < 0) ? cmul(v, c) : cmulc(v, c);
-      if constexpr (DST_G) gdst[base + e * stride] = y;
-      else sp[sa(e)] = y;
-    }
-  };
-  // the last stage writes each output element once, after every thread has read its
-  // inputs (the stage's first barrier), so the in-place emit is safe
-  run_stages<+1>(pl, t, active, sp, sa, tw, fetch, emit_out);
-}
-
 // Full 1D transform of one pencil. DIR = -1 forward (exp(-2 pi i nk/n)), +1 inverse
 // (unnormalised).  tw points at the forward table W_m^k, k in [0, m) (m = n except for
 // Bluestein plans).
@@ -397,14 +348,13 @@ __device__ __forceinline__ void bluestein_pencil(const FftPlan1D& pl, int t, boo
 // shared-memory slot (sp[sa(e)]), and written likewise (DST_G).  Solver-specific
 // work (loaders, multipliers, stores) runs in coalesced loops around this call, so
 // the engine is compiled once per I/O shape instead of once per solver operator.
-template <int DIR, typename C, class SA, bool SRC_G, bool DST_G>
-__device__ __noinline__ void fft_pencil(const FftPlan1D* plp, int t, bool active, C* sp, SA sa, const C* tw,
-                                        const C* gsrc, C* gdst, long long base, long long stride) {
+// Direct transform (m = n), or the length-m stages of a Bluestein plan in place.  BL
+// only separates the instances the Bluestein kernels call from the direct kernels' own:
+// a function shared by both gets the smaller register budget and spills.
+template <int DIR, typename C, class SA, bool SRC_G, bool DST_G, bool BL = false>
+__device__ __noinline__ void fft_pencil_direct(const FftPlan1D* plp, int t, bool active, C* sp, SA sa, const C* tw,
+                                               const C* gsrc, C* gdst, long long base, long long stride) {
   const FftPlan1D& pl = *plp;
-  if (pl.m != pl.n) {
-    bluestein_pencil<DIR, C, SA, SRC_G, DST_G>(pl, t, active, sp, sa, tw, gsrc, gdst, base, stride);
-    return;
-  }
   auto fetch = [&](int e) -> C {
     if constexpr (SRC_G) return gsrc[base + e * stride];
     else return sp[sa(e)];
@@ -426,6 +376,63 @@ __device__ __noinline__ void fft_pencil(const FftPlan1D* plp, int t, bool active
 #undef QSM_TRY_FIXED
   }
   run_stages<DIR>(pl, t, active, sp, sa, tw, fetch, emit);
+}
+
+// Bluestein (chirp-z) transform of one pencil of length n through a cyclic convolution
+// of length m >= 2n - 1 (Bluestein 1970; Rabiner, Schafer and Rader 1969).  With
+// q_j = exp(DIR i pi j^2 / n), jk = (j^2 + k^2 - (k - j)^2) / 2 gives
+//   X_k = q_k * sum_j (x_j q_j) conj(q_{k-j}),
+// a convolution of a_j = x_j q_j (zero-padded to m) with the conjugate chirp.  The table
+// holds c_j = exp(-i pi j^2 / n) (so q = c forward, conj(c) inverse) and K = DFT_m of the
+// conjugate chirp wrapped cyclically, divided by m.  That sequence is even, so K is even
+// and the inverse direction's kernel spectrum is conj(K).  The pencil's slot holds m
+// elements; the two length-m transforms are the plan's own stages, run in place by the
+// direct engine, with the pointwise steps inline in the kernel.  BL selects this path at
+// compile time: every runtime pass kernel is instantiated separately for Bluestein plans,
+// because any second call path next to the direct engine in the same kernel (inline or
+// out of line) shrinks the engine's register budget and makes it spill.
+template <int DIR, typename C, class SA, bool SRC_G, bool DST_G, bool BL>
+__device__ __forceinline__ void fft_pencil(const FftPlan1D* plp, int t, bool active, C* sp, SA sa, const C* tw,
+                                           const C* gsrc, C* gdst, long long base, long long stride) {
+  if constexpr (!BL) {
+    fft_pencil_direct<DIR, C, SA, SRC_G, DST_G>(plp, t, active, sp, sa, tw, gsrc, gdst, base, stride);
+    return;
+  }
+  const int n = plp->n, m = plp->m, T = plp->T;
+  const C* chirp = static_cast<const C*>(plp->ext);
+  const C* kspec = chirp + n;
+  if (active) {
+    for (int j = t; j < m; j += T) {
+      C a = mk<C>(decltype(a.x)(0), decltype(a.x)(0));
+      if (j < n) {
+        C x;
+        if constexpr (SRC_G) x = gsrc[base + j * stride];
+        else x = sp[sa(j)];
+        const C c = chirp[j];
+        a = (DIR < 0) ? cmul(x, c) : cmulc(x, c);
+      }
+      sp[sa(j)] = a;
+    }
+  }
+  __syncthreads();
+  fft_pencil_direct<-1, C, SA, false, false, true>(plp, t, active, sp, sa, tw, nullptr, nullptr, 0, 0);
+  if (active) {
+    for (int j = t; j < m; j += T) {
+      const C k = kspec[j];
+      sp[sa(j)] = (DIR < 0) ? cmul(sp[sa(j)], k) : cmulc(sp[sa(j)], k);
+    }
+  }
+  __syncthreads();
+  fft_pencil_direct<+1, C, SA, false, false, true>(plp, t, active, sp, sa, tw, nullptr, nullptr, 0, 0);
+  if (active) {
+    for (int j = t; j < n; j += T) {
+      const C c = chirp[j];
+      const C y = (DIR < 0) ? cmul(sp[sa(j)], c) : cmulc(sp[sa(j)], c);
+      if constexpr (DST_G) gdst[base + j * stride] = y;
+      else sp[sa(j)] = y;
+    }
+  }
+  __syncthreads();
 }
 
 }  // namespace qsm

@@ -709,14 +709,23 @@ void run_iterations(qsm_ctx* ctx, size_t iters, const int* d_done, One one) {
 
 }  // namespace
 
-template <typename T>
+// T: arithmetic of the Krylov steps (LSQR, step 1; LSMR, step 3) and of their vectors;
+// TD: arithmetic of the direct step 2 (fastQSM filtering, TKD, the fit).  An FP64 context
+// runs both in double; a mixed context runs step 2 in float and the Krylov steps in
+// double unless its Krylov precision is set to mixed: the reference stops LSQR after 50
+// iterations short of its tolerance, so its result is the truncated Krylov iterate, and
+// float rounding in the operator is amplified about a thousandfold there.
+template <typename T, typename TD>
 void ilsqr_impl(qsm_ctx* ctx, const GridDims& d, const double* f, const uint8_t* mask, const double bdir[3],
                 const qsm_ilsqr_params& p, qsm_progress_fn progress, void* user, double* chi, double* xsa_out,
                 double* xfs_out, double* xlsqr_out) {
   using C = cplx_t<T>;
+  using CD = cplx_t<TD>;
   const long long N = d.n;
   const char* pre = sizeof(T) == 4 ? "il32." : "il64.";
   auto nm = [&](const char* s) { return std::string(pre) + s; };
+  const char* pre_d = sizeof(TD) == 4 ? "il32." : "il64.";
+  auto nmd = [&](const char* s) { return std::string(pre_d) + s; };
   auto report = [&](size_t k) {
     if (progress) progress(user, k, 4);
   };
@@ -807,17 +816,21 @@ void ilsqr_impl(qsm_ctx* ctx, const GridDims& d, const double* f, const uint8_t*
 
   // ------------------------------------------------------------- step 2 --
   report(2);
-  C* Fb = vb;  // FFT(f)
-  C* hs = ub;  // SMV kernel spectrum
-  run_x_full<T, -1, 0>(ctx, ff, LoadRealProduct<double, T>{f, nullptr, d.nx}, MidId<T>{},
-                       StoreSpecRow<T>{Fb, ff.g.pitch}, nullptr, "fft_x_c2c");
-  run_yz<T, -1, 1>(ctx, ff, Fb, Fb, OpId<T>{}, nullptr);
-  run_yz<T, -1, 2>(ctx, ff, Fb, Fb, OpId<T>{}, nullptr);
-  run_x_full<T, -1, 0>(ctx, ff, LoadSphereC<T>{sphere_img(d, 3.0)}, MidId<T>{}, StoreSpecRow<T>{hs, ff.g.pitch},
+  // step 2 runs in TD; with TD == T its buffers are step 1's (same names, same sizes)
+  Fft3<TD> ffd = make_fft3_full<TD>(ctx, d);
+  const TD invnd = (TD)(1.0 / (double)N);
+  CD* Fb = ws<CD>(ctx, nmd("v"), (size_t)NF);  // FFT(f)
+  CD* hs = ws<CD>(ctx, nmd("u"), (size_t)NF);  // SMV kernel spectrum
+  CD* td = ws<CD>(ctx, nmd("t"), (size_t)NF);
+  run_x_full<TD, -1, 0>(ctx, ffd, LoadRealProduct<double, TD>{f, nullptr, d.nx}, MidId<TD>{},
+                       StoreSpecRow<TD>{Fb, ffd.g.pitch}, nullptr, "fft_x_c2c");
+  run_yz<TD, -1, 1>(ctx, ffd, Fb, Fb, OpId<TD>{}, nullptr);
+  run_yz<TD, -1, 2>(ctx, ffd, Fb, Fb, OpId<TD>{}, nullptr);
+  run_x_full<TD, -1, 0>(ctx, ffd, LoadSphereC<TD>{sphere_img(d, 3.0)}, MidId<TD>{}, StoreSpecRow<TD>{hs, ffd.g.pitch},
                        nullptr, "fft_x_c2c");
-  run_yz<T, -1, 1>(ctx, ff, hs, hs, OpId<T>{}, nullptr);
-  run_yz<T, -1, 2>(ctx, ff, hs, hs, OpId<T>{}, nullptr);
-  FsFilter<T> filt{K, hs, 0.001, 0.0, 0.0};
+  run_yz<TD, -1, 1>(ctx, ffd, hs, hs, OpId<TD>{}, nullptr);
+  run_yz<TD, -1, 2>(ctx, ffd, hs, hs, OpId<TD>{}, nullptr);
+  FsFilter<TD> filt{K, hs, 0.001, 0.0, 0.0};
   {
     LaunchScope ls(ctx, "ilsqr_dipole_pow");
     k_dipole_pow<<<grid1d(N), 256, 0, ctx->stream>>>(K, d.nx, d.ny, d.nz, 0.001, dwork);
@@ -826,26 +839,26 @@ void ilsqr_impl(qsm_ctx* ctx, const GridDims& d, const double* f, const uint8_t*
     filt.lo = th[0];
     filt.range = th[1] - th[0];
   }
-  T* xfs_raw = ws<T>(ctx, nm("xfs_raw"), (size_t)N);
-  T* xtkd = ws<T>(ctx, nm("xtkd"), (size_t)N);
-  T* xfs = ws<T>(ctx, nm("xfs"), (size_t)N);
-  run_yz<T, +1, 2>(ctx, ff, Fb, t, OpFsFirst<T>{filt}, nullptr);
-  run_yz<T, +1, 1>(ctx, ff, t, t, OpId<T>{}, nullptr);
-  run_x_full<T, +1, -1>(ctx, ff, LoadSpecRow<T>{t, ff.g.pitch}, MidMaskRe<T>{mask, d.nx, invn},
-                        StoreSpecRow<T>{t, ff.g.pitch}, nullptr, "fft_x_fastqsm");
-  run_yz<T, -1, 1>(ctx, ff, t, t, OpId<T>{}, nullptr);
-  run_z_fused<T>(ctx, ff, t, t, OpFsMid<T>{filt}, nullptr);
-  run_yz<T, +1, 1>(ctx, ff, t, t, OpId<T>{}, nullptr);
-  run_x_full<T, +1, 0>(ctx, ff, LoadSpecRow<T>{t, ff.g.pitch}, MidId<T>{}, StoreMaskRe<T, T>{xfs_raw, mask, d.nx, invn},
+  TD* xfs_raw = ws<TD>(ctx, nmd("xfs_raw"), (size_t)N);
+  TD* xtkd = ws<TD>(ctx, nmd("xtkd"), (size_t)N);
+  TD* xfs = ws<TD>(ctx, nmd("xfs"), (size_t)N);
+  run_yz<TD, +1, 2>(ctx, ffd, Fb, td, OpFsFirst<TD>{filt}, nullptr);
+  run_yz<TD, +1, 1>(ctx, ffd, td, td, OpId<TD>{}, nullptr);
+  run_x_full<TD, +1, -1>(ctx, ffd, LoadSpecRow<TD>{td, ffd.g.pitch}, MidMaskRe<TD>{mask, d.nx, invnd},
+                        StoreSpecRow<TD>{td, ffd.g.pitch}, nullptr, "fft_x_fastqsm");
+  run_yz<TD, -1, 1>(ctx, ffd, td, td, OpId<TD>{}, nullptr);
+  run_z_fused<TD>(ctx, ffd, td, td, OpFsMid<TD>{filt}, nullptr);
+  run_yz<TD, +1, 1>(ctx, ffd, td, td, OpId<TD>{}, nullptr);
+  run_x_full<TD, +1, 0>(ctx, ffd, LoadSpecRow<TD>{td, ffd.g.pitch}, MidId<TD>{}, StoreMaskRe<TD, TD>{xfs_raw, mask, d.nx, invnd},
                        nullptr, "fft_x_c2c");
-  run_yz<T, +1, 2>(ctx, ff, Fb, t, OpTkdInv<T>{K, 1.0 / 8.0}, nullptr);
-  run_yz<T, +1, 1>(ctx, ff, t, t, OpId<T>{}, nullptr);
-  run_x_full<T, +1, 0>(ctx, ff, LoadSpecRow<T>{t, ff.g.pitch}, MidId<T>{}, StoreMaskRe<T, T>{xtkd, mask, d.nx, invn},
+  run_yz<TD, +1, 2>(ctx, ffd, Fb, td, OpTkdInv<TD>{K, 1.0 / 8.0}, nullptr);
+  run_yz<TD, +1, 1>(ctx, ffd, td, td, OpId<TD>{}, nullptr);
+  run_x_full<TD, +1, 0>(ctx, ffd, LoadSpecRow<TD>{td, ffd.g.pitch}, MidId<TD>{}, StoreMaskRe<TD, TD>{xtkd, mask, d.nx, invnd},
                        nullptr, "fft_x_c2c");
   {
-    double* sums = ws<double>(ctx, nm("sums"), 4);
+    double* sums = ws<double>(ctx, nmd("sums"), 4);
     LaunchScope ls(ctx, "fastqsm_sums");
-    k_fs_sums<T><<<grid1d(N), 256, 0, ctx->stream>>>(N, xfs_raw, xtkd, partials, counter, sums);
+    k_fs_sums<TD><<<grid1d(N), 256, 0, ctx->stream>>>(N, xfs_raw, xtkd, partials, counter, sums);
     ls.done();
     double s[4];
     d2h(ctx, s, sums, sizeof(s));
@@ -858,7 +871,7 @@ void ilsqr_impl(qsm_ctx* ctx, const GridDims& d, const double* f, const uint8_t*
       b = (s[2] * s[1] - s[0] * s[3]) / det;
     }
     LaunchScope ls2(ctx, "fastqsm_final");
-    k_fs_final<T><<<grid1d(N), 256, 0, ctx->stream>>>(N, xfs_raw, mask, a, b, xfs, xfs_out);
+    k_fs_final<TD><<<grid1d(N), 256, 0, ctx->stream>>>(N, xfs_raw, mask, a, b, xfs, xfs_out);
     ls2.done();
   }
 
@@ -867,7 +880,7 @@ void ilsqr_impl(qsm_ctx* ctx, const GridDims& d, const double* f, const uint8_t*
   T* wg = ws<T>(ctx, nm("wgrad"), (size_t)(3 * N));
   {
     LaunchScope ls(ctx, "ilsqr_fgrad_masked");
-    k_fgrad_masked<T><<<grid1d(N), 256, 0, ctx->stream>>>(xfs, mask, d.nx, d.ny, d.nz, 1.0 / d.vsx, 1.0 / d.vsy,
+    k_fgrad_masked<TD><<<grid1d(N), 256, 0, ctx->stream>>>(xfs, mask, d.nx, d.ny, d.nz, 1.0 / d.vsx, 1.0 / d.vsy,
                                                           1.0 / d.vsz, dwork);
     ls.done();
     const std::vector<double> tx = percentiles(ctx, dwork, mask, N, count, {50.0, 70.0});
@@ -950,6 +963,87 @@ void ilsqr_impl(qsm_ctx* ctx, const GridDims& d, const double* f, const uint8_t*
   report(4);
 }
 
+// ---------------------------------------------------- the LSQR operator alone ----
+// Contiguous complex double rows (nx values) <-> full-spectrum rows (pitch values).
+template <typename T>
+__global__ void k_rows_to_pitch(long long nrows, int nx, int pitch, const double2* __restrict__ in,
+                                cplx_t<T>* __restrict__ out) {
+  const long long total = nrows * pitch;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long row = i / pitch;
+    const int e = (int)(i - row * pitch);
+    cplx_t<T> v = mk<cplx_t<T>>(T(0), T(0));
+    if (e < nx) {
+      const double2 a = in[row * nx + e];
+      v = mk<cplx_t<T>>((T)a.x, (T)a.y);
+    }
+    out[i] = v;
+  }
+}
+template <typename T>
+__global__ void k_pitch_to_rows(long long nrows, int nx, int pitch, const cplx_t<T>* __restrict__ in,
+                                double2* __restrict__ out) {
+  const long long total = nrows * nx;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long row = i / nx;
+    const cplx_t<T> v = in[row * pitch + (i - row * nx)];
+    out[i] = make_double2((double)v.x, (double)v.y);
+  }
+}
+template <typename T>
+__global__ void k_cast_real(long long n, const double* __restrict__ in, T* __restrict__ out) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = (T)in[i];
+}
+
+// y = D * FFT(w * Re(IFFT(D * x))): one application of lsqr_step's operator
+// (src/inversion/ilsqr.rs:988-1010) with the five passes of the solver's own loop.
+template <typename T>
+void lsqr_operator_impl(qsm_ctx* ctx, const GridDims& d, const double bdir[3], const double* w, const double2* x,
+                        double2* y) {
+  using C = cplx_t<T>;
+  const std::string pre = sizeof(T) == 4 ? "ilop32." : "ilop64.";
+  Fft3<T> ff = make_fft3_full<T>(ctx, d);
+  KSpace K = make_kspace(ctx, d, bdir);
+  const long long N = d.n, NF = ff.g.hsize(), nrows = (long long)d.ny * d.nz;
+  C* xin = ws<C>(ctx, pre + "x", (size_t)NF);
+  C* t = ws<C>(ctx, pre + "t", (size_t)NF);
+  C* yo = ws<C>(ctx, pre + "y", (size_t)NF);
+  T* wl = ws<T>(ctx, pre + "w", (size_t)N);
+  LsqrState* st = ws<LsqrState>(ctx, pre + "state", 1);
+  double* partials = ws<double>(ctx, pre + "partials", (size_t)kMaxPersistentBlocks * 4);
+  unsigned* counter = ws<unsigned>(ctx, pre + "counter", 1);
+  LsqrState init{};
+  init.su = 1.0;
+  init.sv = 1.0;
+  h2d(ctx, st, &init, sizeof(init));
+  QSM_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned), ctx->stream));
+  {
+    LaunchScope ls(ctx, "ilsqr_op_pack");
+    k_rows_to_pitch<T><<<grid1d(NF), 256, 0, ctx->stream>>>(nrows, d.nx, ff.g.pitch, x, xin);
+    ls.done();
+    LaunchScope ls2(ctx, "ilsqr_op_weights");
+    k_cast_real<T><<<grid1d(N), 256, 0, ctx->stream>>>(N, w, wl);
+    ls2.done();
+  }
+  const T invn = (T)(1.0 / (double)N);
+  run_yz<T, +1, 2>(ctx, ff, xin, t, OpScaleD<T>{K, &st->su}, nullptr);
+  run_yz<T, +1, 1>(ctx, ff, t, t, OpId<T>{}, nullptr);
+  run_x_full<T, +1, -1, true>(ctx, ff, LoadSpecRow<T>{t, ff.g.pitch}, MidWeightRe<T>{wl, d.nx, invn},
+                              StoreSpecRow<T>{t, ff.g.pitch}, nullptr, "fft_x_lsqr");
+  run_yz<T, -1, 1>(ctx, ff, t, t, OpId<T>{}, nullptr);
+  run_yz_acc<T, -1, 2, true>(ctx, ff, t, yo, OpLsqrOut<T>{K, nullptr, st, 2}, partials, counter, nullptr,
+                             "fft_z_lsqr");
+  {
+    LaunchScope ls(ctx, "ilsqr_op_unpack");
+    k_pitch_to_rows<T><<<grid1d(nrows * d.nx), 256, 0, ctx->stream>>>(nrows, d.nx, ff.g.pitch, yo, y);
+    ls.done();
+  }
+  sync(ctx);
+}
+
 void ilsqr_device(qsm_ctx* ctx, const double* f, const uint8_t* m, const qsm_grid* grid, const double bdir[3],
                   const qsm_ilsqr_params* p, qsm_progress_fn progress, void* user, double* chi, double* xsa,
                   double* xfs, double* xlsqr) {
@@ -960,11 +1054,16 @@ void ilsqr_device(qsm_ctx* ctx, const double* f, const uint8_t* m, const qsm_gri
   check_ptr(p, "params");
   check_bdir(bdir);
   if (std::isnan(p->tol)) throw QsmError(QSM_ERR_INVALID_ARGUMENT, "tol is NaN");
+  check_volume_finite(ctx, f, d.n, "local_field");
   if (d.nx < 2 || d.ny < 2 || d.nz < 2)
     throw QsmError(QSM_ERR_UNSUPPORTED_SIZE, "iLSQR needs every axis length >= 2 (one-sided stencils)");
   if (d.n >= (1LL << 32)) throw QsmError(QSM_ERR_UNSUPPORTED_SIZE, "iLSQR volumes hold fewer than 2^32 voxels");
-  if (ctx->precision == QSM_PRECISION_MIXED) ilsqr_impl<float>(ctx, d, f, m, bdir, *p, progress, user, chi, xsa, xfs, xlsqr);
-  else ilsqr_impl<double>(ctx, d, f, m, bdir, *p, progress, user, chi, xsa, xfs, xlsqr);
+  if (ctx->precision != QSM_PRECISION_MIXED)
+    ilsqr_impl<double, double>(ctx, d, f, m, bdir, *p, progress, user, chi, xsa, xfs, xlsqr);
+  else if (ctx->krylov_precision == QSM_PRECISION_MIXED)
+    ilsqr_impl<float, float>(ctx, d, f, m, bdir, *p, progress, user, chi, xsa, xfs, xlsqr);
+  else
+    ilsqr_impl<double, float>(ctx, d, f, m, bdir, *p, progress, user, chi, xsa, xfs, xlsqr);
 }
 
 }  // namespace qsm
@@ -985,6 +1084,23 @@ qsm_status qsm_ilsqr_device(qsm_ctx* ctx, const double* d_local_field, const uin
   return guarded(ctx, [&] {
     ilsqr_device(ctx, d_local_field, d_mask, grid, bdir, params, progress, user, d_out_chi, d_out_xsa, d_out_xfs,
                  d_out_xlsqr);
+  });
+}
+
+qsm_status qsm_ilsqr_lsqr_operator_device(qsm_ctx* ctx, const qsm_grid* grid, const double bdir[3],
+                                          const double* d_weights, const double* d_x, double* d_y) {
+  return guarded(ctx, [&] {
+    GridDims d = check_grid(grid);
+    check_bdir(bdir);
+    check_ptr(d_weights, "weights");
+    check_ptr(d_x, "x");
+    check_ptr(d_y, "y");
+    if ((reinterpret_cast<uintptr_t>(d_x) | reinterpret_cast<uintptr_t>(d_y)) % 16 != 0)
+      throw QsmError(QSM_ERR_INVALID_ARGUMENT, "complex vectors must be 16-byte aligned");
+    const double2* x = reinterpret_cast<const double2*>(d_x);
+    double2* y = reinterpret_cast<double2*>(d_y);
+    if (ctx->precision == QSM_PRECISION_MIXED) lsqr_operator_impl<float>(ctx, d, bdir, d_weights, x, y);
+    else lsqr_operator_impl<double>(ctx, d, bdir, d_weights, x, y);
   });
 }
 

@@ -58,6 +58,8 @@ struct qsm_ctx {
   int precision = QSM_PRECISION_F64;
   int plan_mode = QSM_PLANS_COMPILED;  // qsm_ctx_set_plan_mode
   int krylov_precision = QSM_PRECISION_F64;  // qsm_ctx_set_krylov_precision (mixed contexts)
+  bool check_inputs = false;  // qsm_ctx_set_input_check
+  long long alloc_fail_after = -1;  // qsm_ctx_inject_alloc_failure: allocations left before one fails
   cudaStream_t stream = nullptr;
   std::string err;
   std::map<std::string, qsm::DevBuf> ws;
@@ -107,6 +109,12 @@ struct GridDims {
 GridDims check_grid(const qsm_grid* g);
 void check_ptr(const void* p, const char* name);
 void check_finite(double v, const char* name);
+// With the context's input check on (qsm_ctx_set_input_check), reject a device volume
+// holding a NaN or an infinity (QSM_ERR_INVALID_ARGUMENT); otherwise do nothing.
+void check_volume_finite(qsm_ctx* ctx, const double* d, long long n, const char* name);
+// Device allocation for the context: cudaMalloc, or the failure requested by
+// qsm_ctx_inject_alloc_failure.
+cudaError_t ctx_malloc(qsm_ctx* ctx, void** p, size_t bytes);
 
 // Host <-> device staging used by the host-pointer entry points.
 // Copies through two pinned staging buffers (kStageBytes each): the host copy of one

@@ -51,6 +51,7 @@ void tkd_device(qsm_ctx* ctx, const double* f, const uint8_t* m, const qsm_grid*
   check_ptr(p, "params");
   check_bdir(bdir);
   check_finite(p->threshold, "threshold");
+  check_volume_finite(ctx, f, d.n, "local_field");
   KSpace K = make_kspace(ctx, d, bdir);
   closed_form(ctx, d, f, m, OpTkd<float>{K, p->threshold, tsvd}, OpTkd<double>{K, p->threshold, tsvd}, out);
 }
@@ -65,6 +66,7 @@ void tikhonov_device(qsm_ctx* ctx, const double* f, const uint8_t* m, const qsm_
   check_bdir(bdir);
   check_finite(p->lambda, "lambda");
   if (p->reg < 0 || p->reg > 2) throw QsmError(QSM_ERR_INVALID_ARGUMENT, "unknown regularization");
+  check_volume_finite(ctx, f, d.n, "local_field");
   KSpace K = make_kspace(ctx, d, bdir);
   closed_form(ctx, d, f, m, OpTikhonov<float>{K, p->lambda, p->reg}, OpTikhonov<double>{K, p->lambda, p->reg}, out);
 }

@@ -156,7 +156,7 @@ void run_x_r2c(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* spec, const Load& ld, 
   const int Tt = x_block_t(f.px.T);
   const int P = x_pencils_per_block<T>(f.px.T);
   const size_t smem = (size_t)(f.px.m + P * x_rowlen<T>(f.px.m)) * sizeof(C);
-  auto kern = k_x_r2c<T, Load>;
+  auto kern = f.px.m != f.px.n ? k_x_r2c<T, Load, true> : k_x_r2c<T, Load, false>;
   ensure_smem(kern, smem);
   LaunchScope ls(ctx, "fft_x_r2c");
   kern<<<(unsigned)x_blocks(f), dim3(Tt, P), smem, ctx->stream>>>(f.g, f.px, f.twx, spec, ld, done);
@@ -170,7 +170,7 @@ void run_x_c2r(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* spec, const Stor
   const int Tt = x_block_t(f.px.T);
   const int P = x_pencils_per_block<T>(f.px.T);
   const size_t smem = (size_t)(f.px.m + P * x_rowlen<T>(f.px.m)) * sizeof(C);
-  auto kern = k_x_c2r<T, Store>;
+  auto kern = f.px.m != f.px.n ? k_x_c2r<T, Store, true> : k_x_c2r<T, Store, false>;
   ensure_smem(kern, smem);
   LaunchScope ls(ctx, "fft_x_c2r");
   kern<<<(unsigned)x_blocks(f), dim3(Tt, P), smem, ctx->stream>>>(f.g, f.px, f.twx, spec, st, done);
@@ -223,7 +223,8 @@ void run_x_full(qsm_ctx* ctx, const Fft3<T>& f, const Load& ld, const Mid& mid, 
   const int Tt = x_block_t(f.px.T);
   const int P = x_pencils_per_block<T>(f.px.T);
   const size_t smem = (size_t)(f.px.m + P * x_rowlen<T>(f.px.m)) * sizeof(C);
-  auto kern = k_x_full<T, D1, D2, Load, Mid, Store>;
+  auto kern = f.px.m != f.px.n ? k_x_full<T, D1, D2, Load, Mid, Store, true>
+                                : k_x_full<T, D1, D2, Load, Mid, Store, false>;
   ensure_smem(kern, smem);
   const long long blocks = ((long long)f.g.nrows() + P - 1) / P;
   LaunchScope ls(ctx, name);
@@ -387,7 +388,7 @@ void run_yz(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst
   }
   const FftPlan1D& pl = (AXIS == 1) ? f.py : f.pz;
   const cplx_t<T>* tw = (AXIS == 1) ? f.twy : f.twz;
-  auto kern = k_pass_yz<T, DIR, AXIS, Op>;
+  auto kern = pl.m != pl.n ? k_pass_yz<T, DIR, AXIS, Op, true> : k_pass_yz<T, DIR, AXIS, Op, false>;
   const int P = yz_tile_width<T>(kern, pl.m, pl.T);
   const size_t smem = yz_smem<T>(pl.m, P);
   const TileWalk w = tile_walk(f, AXIS, P);
@@ -407,7 +408,7 @@ void run_yz_acc(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>*
   }
   const FftPlan1D& pl = (AXIS == 1) ? f.py : f.pz;
   const cplx_t<T>* tw = (AXIS == 1) ? f.twy : f.twz;
-  auto kern = k_pass_yz_acc<T, DIR, AXIS, Op>;
+  auto kern = pl.m != pl.n ? k_pass_yz_acc<T, DIR, AXIS, Op, true> : k_pass_yz_acc<T, DIR, AXIS, Op, false>;
   const int P = yz_tile_width<T>(kern, pl.m, pl.T);
   const size_t smem = yz_smem<T>(pl.m, P);
   const TileWalk w = tile_walk(f, AXIS, P);
@@ -425,7 +426,7 @@ template <typename T> inline size_t zm_smem(int n, int m, int P) {
 
 // Tile width of the multiplier-array Z pass, 0 when no width fits (very long axes).
 template <typename T> int zm_tile_width(int n, int m, int Tn) {
-  auto kern = k_z_fused_m<T>;
+  auto kern = m != n ? k_z_fused_m<T, true> : k_z_fused_m<T, false>;
   for (int p = yz_cols<T>(); p >= 16 / (int)sizeof(T); p /= 2) {
     if (p * Tn > 1024 || zm_smem<T>(n, m, p) > 227u * 1024u) continue;
     ensure_smem(kern, zm_smem<T>(n, m, p));
@@ -468,7 +469,7 @@ void run_z_fused_m(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<
 #undef QSM_TRY_ZM
     }
   }
-  auto kern = k_z_fused_m<T>;
+  auto kern = pl.m != pl.n ? k_z_fused_m<T, true> : k_z_fused_m<T, false>;
   const int P = zm_tile_width<T>(pl.n, pl.m, pl.T);
   if (P == 0) throw QsmError(QSM_ERR_UNSUPPORTED_SIZE, "z axis does not fit one multiplier tile");
   const size_t smem = zm_smem<T>(pl.n, pl.m, P);
@@ -483,7 +484,7 @@ template <typename T, class Op>
 void run_z_fused(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst, const Op& op,
                  const int* done) {
   const FftPlan1D& pl = f.pz;
-  auto kern = k_z_fused<T, Op>;
+  auto kern = pl.m != pl.n ? k_z_fused<T, Op, true> : k_z_fused<T, Op, false>;
   const int P = yz_tile_width<T>(kern, pl.m, pl.T);
   const size_t smem = yz_smem<T>(pl.m, P);
   const TileWalk w = tile_walk(f, 2, P);

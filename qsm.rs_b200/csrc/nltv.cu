@@ -185,6 +185,7 @@ void nltv_device(qsm_ctx* ctx, const double* f, const uint8_t* m, const qsm_grid
   check_ptr(out, "out");
   check_ptr(p, "params");
   check_bdir(bdir);
+  check_volume_finite(ctx, f, d.n, "local_field");
   check_finite(p->lambda, "lambda");
   check_finite(p->mu, "mu");
   if (std::isnan(p->tol)) throw QsmError(QSM_ERR_INVALID_ARGUMENT, "tol is NaN");

@@ -67,7 +67,7 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
 // A thread holds at most kFftEmax elements of a row (T >= n/16), so the loader's
 // global reads are issued as one unrolled batch before any is consumed.
 // ---------------------------------------------------------------------------
-template <typename T, class Load>
+template <typename T, class Load, bool BL>
 __global__ void k_x_r2c(Geom g, const __grid_constant__ FftPlan1D pl, const cplx_t<T>* __restrict__ twg,
                         cplx_t<T>* __restrict__ spec, Load ld, const int* __restrict__ done) {
   using C = cplx_t<T>;
@@ -108,7 +108,7 @@ __global__ void k_x_r2c(Geom g, const __grid_constant__ FftPlan1D pl, const cplx
     }
   }
   __syncthreads();
-  fft_pencil<-1, C, SAPadded<PadG<T>::G>, false, false>(&pl, t, active, sp, sa, tw, nullptr, nullptr, 0, 0);
+  fft_pencil<-1, C, SAPadded<PadG<T>::G>, false, false, BL>(&pl, t, active, sp, sa, tw, nullptr, nullptr, 0, 0);
   if (active) {
     const T half = T(0.5);
     for (int k = t; k < g.nxh; k += pl.T) {
@@ -130,7 +130,7 @@ __global__ void k_x_r2c(Geom g, const __grid_constant__ FftPlan1D pl, const cplx
 //   Mid  : C operator()(C v, int row, int e)
 //   Store: void operator()(int row, int e, C v); void finish()
 // ---------------------------------------------------------------------------
-template <typename T, int D1, int D2, class Load, class Mid, class Store>
+template <typename T, int D1, int D2, class Load, class Mid, class Store, bool BL>
 __global__ void k_x_full(Geom g, const __grid_constant__ FftPlan1D pl, const cplx_t<T>* __restrict__ twg, Load ld,
                          Mid mid, Store st0, const int* __restrict__ done) {
   using C = cplx_t<T>;
@@ -163,11 +163,11 @@ __global__ void k_x_full(Geom g, const __grid_constant__ FftPlan1D pl, const cpl
     }
   }
   __syncthreads();
-  if constexpr (D1 != 0) fft_pencil<D1, C, SAPadded<PadG<T>::G>, false, false>(&pl, t, active, sp, sa, tw, nullptr, nullptr, 0, 0);
+  if constexpr (D1 != 0) fft_pencil<D1, C, SAPadded<PadG<T>::G>, false, false, BL>(&pl, t, active, sp, sa, tw, nullptr, nullptr, 0, 0);
   if (active)
     for (int e = t; e < n; e += pl.T) sp[sa(e)] = mid(sp[sa(e)], (int)row, e);
   __syncthreads();
-  if constexpr (D2 != 0) fft_pencil<D2, C, SAPadded<PadG<T>::G>, false, false>(&pl, t, active, sp, sa, tw, nullptr, nullptr, 0, 0);
+  if constexpr (D2 != 0) fft_pencil<D2, C, SAPadded<PadG<T>::G>, false, false, BL>(&pl, t, active, sp, sa, tw, nullptr, nullptr, 0, 0);
   Store st = st0;
   {
     C v[kFftEmax];
@@ -227,7 +227,7 @@ __global__ void k_x_full_fx(Geom g, const cplx_t<T>* __restrict__ twg, Load ld, 
 // ---------------------------------------------------------------------------
 constexpr int kXHalfMax = 9;
 
-template <typename T, class Store>
+template <typename T, class Store, bool BL>
 __global__ void k_x_c2r(Geom g, const __grid_constant__ FftPlan1D pl, const cplx_t<T>* __restrict__ twg,
                         const cplx_t<T>* __restrict__ spec, Store st0, const int* __restrict__ done) {
   using C = cplx_t<T>;
@@ -277,7 +277,7 @@ __global__ void k_x_c2r(Geom g, const __grid_constant__ FftPlan1D pl, const cplx
     }
   }
   __syncthreads();
-  fft_pencil<+1, C, SAPadded<PadG<T>::G>, false, false>(&pl, t, active, sp, sa, tw, nullptr, nullptr, 0, 0);
+  fft_pencil<+1, C, SAPadded<PadG<T>::G>, false, false, BL>(&pl, t, active, sp, sa, tw, nullptr, nullptr, 0, 0);
   Store st = st0;
   {
     C v[kFftEmax];
@@ -427,7 +427,7 @@ template <typename T> struct YzRegCap { static constexpr int value = sizeof(T) =
 // spill (float: ~0.1 KB, double: ~1.5 KB per thread), so they get a larger one.
 template <typename T> struct ZRegCap { static constexpr int value = sizeof(T) == 4 ? 128 : 168; };
 
-template <typename T, int DIR, int AXIS, class Op>
+template <typename T, int DIR, int AXIS, class Op, bool BL>
 __global__ void __maxnreg__(YzRegCap<T>::value)
     k_pass_yz(Geom g, const __grid_constant__ FftPlan1D pl, TileWalk w, const cplx_t<T>* __restrict__ twg,
                           const cplx_t<T>* src, cplx_t<T>* dst, Op op, const int* __restrict__ done) {
@@ -462,7 +462,7 @@ __global__ void __maxnreg__(YzRegCap<T>::value)
     const long long base = col + (long long)outer * w.ostride;
     C* sp = cur + px;
     if constexpr (IsPlainOp<Op>::value) {
-      fft_pencil<DIR, C, SAStrided, false, true>(&pl, t, active, sp, sa, tw, nullptr, dst, base, w.estride);
+      fft_pencil<DIR, C, SAStrided, false, true, BL>(&pl, t, active, sp, sa, tw, nullptr, dst, base, w.estride);
     } else {
       if (active) {
         for (int e = t; e < n; e += pl.T) {
@@ -471,7 +471,7 @@ __global__ void __maxnreg__(YzRegCap<T>::value)
         }
       }
       __syncthreads();
-      fft_pencil<DIR, C, SAStrided, false, false>(&pl, t, active, sp, sa, tw, nullptr, nullptr, 0, 0);
+      fft_pencil<DIR, C, SAStrided, false, false, BL>(&pl, t, active, sp, sa, tw, nullptr, nullptr, 0, 0);
       if (active) {
         for (int e = t; e < n; e += pl.T) {
           const long long idx = base + e * w.estride;
@@ -557,7 +557,7 @@ __device__ __forceinline__ bool grid_sum_last(double (&a)[K], double* __restrict
 // Y/Z pass whose post hook also accumulates one FP64 value per element
 // (post(v, ix, iy, iz, idx, acc) returns the value to store).  The block that
 // finishes last reduces the sums and runs op.last(total) on its thread 0.
-template <typename T, int DIR, int AXIS, class Op>
+template <typename T, int DIR, int AXIS, class Op, bool BL>
 __global__ void __maxnreg__(YzRegCap<T>::value)
     k_pass_yz_acc(Geom g, const __grid_constant__ FftPlan1D pl, TileWalk w, const cplx_t<T>* __restrict__ twg,
                   const cplx_t<T>* src, cplx_t<T>* dst, Op op, double* __restrict__ partials, unsigned* counter,
@@ -600,7 +600,7 @@ __global__ void __maxnreg__(YzRegCap<T>::value)
       }
     }
     __syncthreads();
-    fft_pencil<DIR, C, SAStrided, false, false>(&pl, t, active, sp, sa, tw, nullptr, nullptr, 0, 0);
+    fft_pencil<DIR, C, SAStrided, false, false, BL>(&pl, t, active, sp, sa, tw, nullptr, nullptr, 0, 0);
     if (active) {
       for (int e = t; e < n; e += pl.T) {
         const long long idx = base + e * w.estride;
@@ -653,7 +653,7 @@ __device__ __forceinline__ void issue_mtile(const T* __restrict__ src, T* buf, c
 // Z forward -> multiply by a precomputed real multiplier -> Z inverse.  The
 // multiplier (spectrum layout, real) is staged with the spectrum tile, so the
 // pointwise step is one shared-memory read per element.  Needs P*sizeof(T) >= 16.
-template <typename T>
+template <typename T, bool BL>
 __global__ void __maxnreg__(ZRegCap<T>::value) k_z_fused_m(Geom g, const __grid_constant__ FftPlan1D pl, TileWalk w,
                             const cplx_t<T>* __restrict__ twg, const cplx_t<T>* src, cplx_t<T>* dst,
                             const T* __restrict__ mult, const int* __restrict__ done) {
@@ -697,12 +697,12 @@ __global__ void __maxnreg__(ZRegCap<T>::value) k_z_fused_m(Geom g, const __grid_
     const bool active = col < g.nxh;
     const long long base = col + (long long)iy * w.ostride;
     C* sp = cur + px;
-    fft_pencil<-1, C, SAStrided, false, false>(&pl, t, active, sp, sa, tw, nullptr, nullptr, 0, 0);
+    fft_pencil<-1, C, SAStrided, false, false, BL>(&pl, t, active, sp, sa, tw, nullptr, nullptr, 0, 0);
     if (active) {
       for (int e = t; e < n; e += pl.T) sp[sa(e)] = cscale(sp[sa(e)], mcur[e * P + px]);
     }
     __syncthreads();
-    fft_pencil<+1, C, SAStrided, false, true>(&pl, t, active, sp, sa, tw, nullptr, dst, base, w.estride);
+    fft_pencil<+1, C, SAStrided, false, true, BL>(&pl, t, active, sp, sa, tw, nullptr, dst, base, w.estride);
   }
   cp_async_wait<0>();
 }
@@ -854,7 +854,7 @@ __global__ void __launch_bounds__(P* FP::T, zm_min_blocks<P * FP::T>())
 }
 
 // Z forward -> Op::mid pointwise -> Z inverse, tiled like k_pass_yz (outer = y).
-template <typename T, class Op>
+template <typename T, class Op, bool BL>
 __global__ void __maxnreg__(ZRegCap<T>::value)
     k_z_fused(Geom g, const __grid_constant__ FftPlan1D pl, TileWalk w, const cplx_t<T>* __restrict__ twg,
                           const cplx_t<T>* src, cplx_t<T>* dst, Op op, const int* __restrict__ done) {
@@ -888,13 +888,13 @@ __global__ void __maxnreg__(ZRegCap<T>::value)
     const bool active = col < g.nxh;
     const long long base = col + (long long)iy * w.ostride;
     C* sp = cur + px;
-    fft_pencil<-1, C, SAStrided, false, false>(&pl, t, active, sp, sa, tw, nullptr, nullptr, 0, 0);
+    fft_pencil<-1, C, SAStrided, false, false, BL>(&pl, t, active, sp, sa, tw, nullptr, nullptr, 0, 0);
     if (active) {
 #pragma unroll 1
       for (int e = t; e < n; e += pl.T) sp[sa(e)] = op.mid(sp[sa(e)], col, iy, e, base + e * w.estride);
     }
     __syncthreads();
-    fft_pencil<+1, C, SAStrided, false, true>(&pl, t, active, sp, sa, tw, nullptr, dst, base, w.estride);
+    fft_pencil<+1, C, SAStrided, false, true, BL>(&pl, t, active, sp, sa, tw, nullptr, dst, base, w.estride);
   }
   cp_async_wait<0>();
 }

@@ -162,6 +162,7 @@ void rts_device(qsm_ctx* ctx, const double* f, const uint8_t* m, const qsm_grid*
   check_ptr(out, "out");
   check_ptr(p, "params");
   check_bdir(bdir);
+  check_volume_finite(ctx, f, d.n, "local_field");
   check_finite(p->delta, "delta");
   check_finite(p->mu, "mu");
   check_finite(p->rho, "rho");

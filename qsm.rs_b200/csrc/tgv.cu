@@ -605,6 +605,7 @@ void tgv_device(qsm_ctx* ctx, const double* phase, const uint8_t* mask, const qs
   for (double v : {(double)p->alpha0, (double)p->alpha1, (double)p->step_size, (double)p->fieldstrength, (double)p->te})
     check_finite(v, "TGV parameter");
   if (std::isnan(p->tol)) throw QsmError(QSM_ERR_INVALID_ARGUMENT, "tol is NaN");
+  check_volume_finite(ctx, phase, d.n, "phase");
   const long long N = d.n;
   // erosions: mask_eroded = erode^erosions(mask), mask0 = erode(mask_eroded)
   uint8_t* ea = ws<uint8_t>(ctx, "tgv.er_a", (size_t)N);

@@ -232,6 +232,7 @@ void tv_unrolled_device(qsm_ctx* ctx, const double* f, const uint8_t* mask, cons
   check_bdir(bdir);
   check_finite(lambda, "lambda");
   check_finite(rho, "rho");
+  check_volume_finite(ctx, f, d.n, "local_field");
   if (K == 0) throw QsmError(QSM_ERR_INVALID_ARGUMENT, "iterations must be >= 1");
   if (C == 0) throw QsmError(QSM_ERR_INVALID_ARGUMENT, "checkpoint_every must be >= 1");
   if (d.n >= (1LL << 32)) throw QsmError(QSM_ERR_UNSUPPORTED_SIZE, "volumes hold fewer than 2^32 voxels");

@@ -185,6 +185,7 @@ void tv_batch_device(qsm_ctx* ctx, const qsm_volume* vols, size_t n, const qsm_t
     check_ptr(vols[b].out_chi, "out_chi");
     check_bdir(vols[b].bdir);
   }
+  for (size_t b = 0; b < n; ++b) check_volume_finite(ctx, vols[b].local_field, check_grid(&vols[b].grid).n, "local_field");
   if (ctx->precision == QSM_PRECISION_MIXED) tv_admm_batch_impl<float>(ctx, vols, n, *p, progress, user, out_iters);
   else tv_admm_batch_impl<double>(ctx, vols, n, *p, progress, user, out_iters);
   sync(ctx);
@@ -198,6 +199,7 @@ void tv_device(qsm_ctx* ctx, const double* f, const uint8_t* m, const qsm_grid* 
   check_ptr(out, "out");
   check_ptr(p, "params");
   check_bdir(bdir);
+  check_volume_finite(ctx, f, d.n, "local_field");
   check_finite(p->lambda, "lambda");
   check_finite(p->rho, "rho");
   if (std::isnan(p->tol)) throw QsmError(QSM_ERR_INVALID_ARGUMENT, "tol is NaN");

@@ -1,0 +1,81 @@
+#!/usr/bin/env python
+"""One solve of a named workload, untimed, for an ncu capture of its kernels.
+
+    python qsm.rs_b200/profile_case.py tv --iters 4 [--precision mixed|f64] [--dims NX NY NZ]
+    python qsm.rs_b200/profile_case.py tgv --dims 256 256 192 --iters 4
+
+tv : TV-ADMM (src/inversion/tv.rs:63-97) on the 256x256x176 ellipsoid brain phantom, or,
+     with --dims, on a seeded N(0, 0.01) field with a full mask;
+tgv: TGV (src/inversion/tgv.rs:1045-1299) on an ellipsoid mask (semi-axes 0.42/0.45/0.40
+     of the grid) with uniform wrapped phase in [-3, 3] rad, 0.6 mm voxels, tol 0.
+Both run on cuda:0 and exit; nothing is timed.
+"""
+import argparse
+import os
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+import numpy as np  # noqa: E402
+
+
+def run_tv(a):
+    import torch
+    import qsmgpu
+    from qsmgpu import Grid, inversion, phantom
+    if a.dims:
+        dims = tuple(a.dims)
+        n = dims[0] * dims[1] * dims[2]
+        f = np.random.default_rng(3).normal(0.0, 0.01, n)
+        mask = np.ones(n, np.uint8)
+    else:
+        dims = (256, 256, 176)
+        f, mask = phantom.brain_tv_case(0, dims)
+    dev = torch.device("cuda", 0)
+    d_f = torch.from_numpy(np.ascontiguousarray(f).ravel()).to(dev)
+    d_m = torch.from_numpy(np.ascontiguousarray(mask).ravel()).to(dev)
+    d_o = torch.empty(d_f.numel(), dtype=torch.float64, device=dev)
+    with qsmgpu.Context(0, a.precision) as ctx:
+        inversion.tv_admm_device(ctx, d_f.data_ptr(), d_m.data_ptr(), Grid.new(*dims), (0.0, 0.0, 1.0),
+                                 inversion.TvParams(2e-4, 2e-2, 0.0, a.iters), d_o.data_ptr())
+    torch.cuda.synchronize()
+    print(f"tv ok: {dims} x{a.iters}, |chi|max={float(d_o.abs().max()):.4g}")
+
+
+def run_tgv(a):
+    import torch
+    import qsmgpu
+    from qsmgpu import Grid, inversion
+    nx, ny, nz = a.dims or (256, 256, 192)
+    dev = torch.device("cuda", 0)
+    z, y, x = torch.meshgrid(torch.arange(nz, device=dev, dtype=torch.float32),
+                             torch.arange(ny, device=dev, dtype=torch.float32),
+                             torch.arange(nx, device=dev, dtype=torch.float32), indexing="ij")
+    cx, cy, cz = (nx - 1) / 2, (ny - 1) / 2, (nz - 1) / 2
+    mask = (((x - cx) / (0.42 * nx)) ** 2 + ((y - cy) / (0.45 * ny)) ** 2 + ((z - cz) / (0.40 * nz)) ** 2) < 1
+    m8 = mask.reshape(-1).to(torch.uint8).contiguous()
+    g = torch.Generator(device=dev).manual_seed(1)
+    ph = ((torch.rand(nx * ny * nz, generator=g, device=dev, dtype=torch.float64) * 2 - 1) * 3.0 * m8.double())
+    ph = ph.contiguous()
+    out = torch.empty_like(ph)
+    with qsmgpu.Context(0, "mixed") as ctx:
+        inversion.tgv_qsm_device(ctx, ph.data_ptr(), m8.data_ptr(), Grid.new(nx, ny, nz, 0.6, 0.6, 0.6),
+                                 inversion.TgvParams(iterations=a.iters, tol=0.0, fieldstrength=3.0, te=0.020),
+                                 (0.0, 0.0, 1.0), out.data_ptr())
+    torch.cuda.synchronize()
+    print(f"tgv ok: {(nx, ny, nz)} x{a.iters}, |chi|max={float(out.abs().max()):.4g}")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("case", choices=["tv", "tgv"])
+    ap.add_argument("--iters", type=int, default=4)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "f64"])
+    ap.add_argument("--dims", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"))
+    a = ap.parse_args()
+    run_tv(a) if a.case == "tv" else run_tgv(a)
+
+
+if __name__ == "__main__":
+    main()

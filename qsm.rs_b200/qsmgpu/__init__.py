@@ -154,6 +154,15 @@ class Context:
     def krylov_precision(self, p: str):
         _check(self, self._lib.qsm_ctx_set_krylov_precision(self._h, _prec_code(p)))
 
+    def set_input_check(self, on: bool):
+        """Reject input volumes holding NaN or infinity (off by default, as in the reference)."""
+        _check(self, self._lib.qsm_ctx_set_input_check(self._h, 1 if on else 0))
+
+    def inject_alloc_failure(self, after: int):
+        """Make the context's device allocation after `after` more successful ones fail
+        with QSM_ERR_ALLOC (simulated on the host); negative cancels."""
+        _check(self, self._lib.qsm_ctx_inject_alloc_failure(self._h, int(after)))
+
     def last_error(self) -> str:
         s = self._lib.qsm_last_error(self._h)
         return s.decode() if s else ""

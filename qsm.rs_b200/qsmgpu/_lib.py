@@ -130,6 +130,8 @@ _SIGS = [
     ("qsm_ctx_get_plan_mode", C.c_int, [C.c_void_p]),
     ("qsm_ctx_set_krylov_precision", C.c_int, [C.c_void_p, C.c_int]),
     ("qsm_ctx_get_krylov_precision", C.c_int, [C.c_void_p]),
+    ("qsm_ctx_set_input_check", C.c_int, [C.c_void_p, C.c_int]),
+    ("qsm_ctx_inject_alloc_failure", C.c_int, [C.c_void_p, C.c_longlong]),
     ("qsm_ctx_release_workspace", C.c_int, [C.c_void_p]),
     ("qsm_last_error", C.c_char_p, [C.c_void_p]),
     ("qsm_ctx_kernel_launches", C.c_uint64, [C.c_void_p]),
@@ -195,6 +197,8 @@ _SIGS = [
     ("qsm_ilsqr_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(QsmGrid), c_double_p,
                                    C.POINTER(QsmIlsqrParams), PROGRESS_FN, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p]),
+    ("qsm_ilsqr_lsqr_operator_device", C.c_int, [C.c_void_p, C.POINTER(QsmGrid), c_double_p, C.c_void_p,
+                                                 C.c_void_p, C.c_void_p]),
     ("qsm_tkd_params_default", None, [C.POINTER(QsmTkdParams)]),
     ("qsm_tikhonov_params_default", None, [C.POINTER(QsmTikhonovParams)]),
     ("qsm_sharp_params_default", None, [C.POINTER(QsmSharpParams)]),

@@ -222,6 +222,15 @@ def ilsqr_device(ctx: Context, d_local_field: int, d_mask: int, grid: Grid, bdir
     _check(ctx, st)
 
 
+def ilsqr_lsqr_operator_device(ctx: Context, grid: Grid, bdir, d_weights: int, d_x: int, d_y: int):
+    """One application of iLSQR's LSQR operator y = D * FFT(w * Re IFFT(D * x))
+    (src/inversion/ilsqr.rs:988-1010) on device complex128 vectors of nx*ny*nz values."""
+    b, _keep = _bdir(bdir)
+    g = grid._c()
+    _check(ctx, ctx._lib.qsm_ilsqr_lsqr_operator_device(ctx.handle, C.byref(g), b, C.c_void_p(d_weights),
+                                                         C.c_void_p(d_x), C.c_void_p(d_y)))
+
+
 def prctile_device(ctx: Context, d_vals: int, d_mask: int, n: int, percents):
     """prctile (src/inversion/ilsqr.rs:937-946) of device values where mask != 0 (all when
     d_mask is 0), one result per percent."""

@@ -2,7 +2,11 @@
 
 All four outputs (chi, xsa, xfs, xlsqr) are compared.  Tolerances (relative L2 over the
 volume): FP64 context 1e-9 (two Krylov solvers amplify transform rounding); mixed context
-2e-3 (float vectors and transforms with FP64 norms and recurrences).
+1e-4 with its default FP64 Krylov steps (the direct fastQSM step in float); 2e-3 with the
+Krylov steps in float too (float vectors and transforms with FP64 norms and recurrences:
+the reference's truncated LSQR amplifies float rounding about a thousandfold, see
+tests/test_oracle.py::test_ilsqr_krylov_steps_amplify_rounding).  The LSQR operator alone
+(src/inversion/ilsqr.rs:988-1010) is checked at every compile-time x length.
 """
 import math
 
@@ -109,12 +113,94 @@ def test_ilsqr_default_params_f64(ctx64, dims, vs, bdir):
     check_all(got, ref, max(1e-9, 100.0 * sens))
 
 
-def test_ilsqr_mixed(ctx32):
-    grid = Grid.new(24, 20, 18, 1.0, 1.2, 0.9)
+@pytest.mark.parametrize("dims,vs", [((24, 20, 18), (1.0, 1.2, 0.9)), ((32, 32, 24), (1.0, 1.0, 1.0))])
+def test_ilsqr_mixed(ctx32, dims, vs):
+    grid = Grid.new(*dims, *vs)
     f, mask = phantom_case(grid, OBLIQUE, seed=5)
-    got = inversion.ilsqr(f, mask, grid, OBLIQUE, inversion.IlsqrParams(), ctx=ctx32)
     ref = O.ilsqr(f, mask, og(grid), OBLIQUE, O.IlsqrParams())
-    check_all(got, ref, 2e-3)
+    assert ctx32.krylov_precision == "f64"
+    got = inversion.ilsqr(f, mask, grid, OBLIQUE, inversion.IlsqrParams(), ctx=ctx32)
+    errs = check_all(got, ref, 1e-4)
+    print("\nmixed, FP64 Krylov:", {k: f"{v:.1e}" for k, v in errs.items()})
+    ctx32.krylov_precision = "mixed"
+    try:
+        got = inversion.ilsqr(f, mask, grid, OBLIQUE, inversion.IlsqrParams(), ctx=ctx32)
+    finally:
+        ctx32.krylov_precision = "f64"
+    errs = check_all(got, ref, 2e-3)
+    print("mixed, float Krylov:", {k: f"{v:.1e}" for k, v in errs.items()})
+
+
+def _oracle_lsqr_operator(grid, bdir, w, x):
+    """apply_a of lsqr_step (src/inversion/ilsqr.rs:988-1010), as the oracle writes it."""
+    d = O.dipole_kernel(og(grid), bdir)
+    r = O.ifft3d(d * x).real
+    return O.fft3d((w * r).astype(np.complex128)) * d
+
+
+def _lsqr_operator(ctx, grid, bdir, w, x):
+    import torch
+    dw = torch.from_numpy(np.ascontiguousarray(w).ravel()).cuda()
+    dx = torch.from_numpy(np.ascontiguousarray(x).ravel()).cuda()
+    dy = torch.empty_like(dx)
+    inversion.ilsqr_lsqr_operator_device(ctx, grid, bdir, dw.data_ptr(), dx.data_ptr(), dy.data_ptr())
+    return dy.cpu().numpy().reshape(grid.shape)
+
+
+def _operator_case(grid, seed):
+    rng = np.random.default_rng(seed)
+    w = rng.uniform(0.0, 1.0, grid.shape)
+    x = rng.standard_normal(grid.shape) + 1j * rng.standard_normal(grid.shape)
+    return w, x
+
+
+@pytest.mark.parametrize("dims", [(8, 6, 10), (24, 20, 18), (15, 9, 25), (17, 12, 10)])
+def test_lsqr_operator_f64(ctx64, dims):
+    grid = Grid.new(*dims, 1.0, 1.2, 0.9)
+    w, x = _operator_case(grid, sum(dims))
+    got = _lsqr_operator(ctx64, grid, OBLIQUE, w, x)
+    assert rel(got.view(np.float64), _oracle_lsqr_operator(grid, OBLIQUE, w, x).view(np.float64)) < 1e-12
+
+
+XFULL = [64, 96, 128, 160, 176, 192, 256, 384, 200, 90]
+
+
+@pytest.mark.parametrize("nx", XFULL)
+def test_lsqr_operator_mixed_compile_time_x(ctx32, nx):
+    """The float X pass over full rows (inverse FFT, weight, forward FFT) takes the
+    compile-time kernel at the base lengths and the runtime engine elsewhere (200, 90):
+    both against the oracle, and compile-time against runtime."""
+    grid = Grid.new(nx, 24, 20)
+    w, x = _operator_case(grid, nx)
+    want = _oracle_lsqr_operator(grid, OBLIQUE, w, x).view(np.float64)
+    got = _lsqr_operator(ctx32, grid, OBLIQUE, w, x)
+    assert rel(got.view(np.float64), want) < 2e-6, rel(got.view(np.float64), want)
+    ctx32.plan_mode = "runtime"
+    try:
+        rt = _lsqr_operator(ctx32, grid, OBLIQUE, w, x)
+    finally:
+        ctx32.plan_mode = "compiled"
+    assert rel(got.view(np.float64), rt.view(np.float64)) < 1e-6
+
+
+def test_ilsqr_mixed_vs_f64_384x384x256(ctx32, ctx64):
+    """Configuration 5's grid: the mixed context (float fastQSM step, FP64 Krylov steps)
+    against the FP64 context."""
+    import torch
+    from qsmgpu import phantom
+    case = phantom.tv_case((384, 384, 256), seed=2, n_ellipsoids=16, mask_radius=110.0,
+                           voxel_size=(0.6, 0.6, 0.6))
+    grid = Grid.new(384, 384, 256, 0.6, 0.6, 0.6)
+    df = torch.from_numpy(np.ascontiguousarray(case.local_field).ravel()).cuda()
+    dm = torch.from_numpy(np.ascontiguousarray(case.mask).ravel()).cuda()
+    outs = {}
+    for name, ctx in (("mixed", ctx32), ("f64", ctx64)):
+        o = [torch.empty_like(df) for _ in range(4)]
+        inversion.ilsqr_device(ctx, df.data_ptr(), dm.data_ptr(), grid, (0.0, 0.0, 1.0), inversion.IlsqrParams(),
+                               o[0].data_ptr(), o[1].data_ptr(), o[2].data_ptr(), o[3].data_ptr())
+        outs[name] = [t.cpu().numpy() for t in o]
+    errs = check_all(outs["mixed"], outs["f64"], 1e-4)
+    print("\n384x384x256 mixed vs f64:", {k: f"{v:.1e}" for k, v in errs.items()})
 
 
 def test_ilsqr_pipeline_dispatch(ctx64):
