@@ -108,6 +108,25 @@ QSM_API int qsm_ctx_get_krylov_precision(const qsm_ctx* ctx);
  * volume and returns QSM_ERR_INVALID_ARGUMENT, naming the count, if a voxel is NaN or
  * infinite. */
 QSM_API qsm_status qsm_ctx_set_input_check(qsm_ctx* ctx, int on);
+/* Autotuner of the compile-time Y/Z pass launch shapes (no reference counterpart; on by
+ * default).  The first TV-ADMM-family solve of a grid on a context times each candidate
+ * shape of its Y and fused Z passes once, on the solve's own buffers before they hold
+ * data, and keeps the fastest per (pass, grid, precision) for the context's lifetime.
+ * Candidates differ in grid form (resident blocks walking the tiles, or one block per
+ * tile) and in how a narrow remainder of columns is tiled; all compute the same values,
+ * so results do not depend on the choice.  Off: the resident-block shape always.
+ * qsm_ctx_autotune_entry reports entry i (0 <= i < qsm_ctx_autotune_count): its key,
+ * the chosen candidate, and up to `cap` (candidate, microseconds per launch) pairs;
+ * *count receives the number of candidates timed. */
+QSM_API qsm_status qsm_ctx_set_autotune(qsm_ctx* ctx, int on);
+/* Test hook: launch every tunable pass in candidate shape `shape` (0..63: bit 0 edge
+ * tiles where the grid has a narrow column remainder, bit 1 one block per tile, bits 2-5
+ * resident blocks per SM of the persistent grid, 0 = as many as fit), or -1 to return to
+ * the autotuner's choice. */
+QSM_API qsm_status qsm_ctx_force_launch_shape(qsm_ctx* ctx, int shape);
+QSM_API size_t qsm_ctx_autotune_count(const qsm_ctx* ctx);
+QSM_API qsm_status qsm_ctx_autotune_entry(const qsm_ctx* ctx, size_t i, char* key, size_t key_cap, int* choice,
+                                          int* candidates, float* us, size_t cap, size_t* count);
 /* Fault injection for callers' error-path tests: after `after` more successful device
  * allocations, the context's next allocation fails with QSM_ERR_ALLOC (the failure is
  * simulated on the host; nothing reaches the GPU), then allocations succeed again.  A

@@ -72,6 +72,58 @@ void* ws_get(qsm_ctx* ctx, const std::string& name, size_t bytes) {
   return b.p;
 }
 
+bool stream_capturing(qsm_ctx* ctx) {
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  QSM_CUDA(cudaStreamIsCapturing(ctx->stream, &st));
+  return st != cudaStreamCaptureStatusNone;
+}
+
+void autotune_pick(qsm_ctx* ctx, const std::string& key, const std::vector<int>& cands,
+                   const std::function<void(int)>& launch) {
+  if (cands.empty()) return;
+  TuneRec rec;
+  if (cands.size() == 1) {
+    rec.choice = cands[0];
+    ctx->tuned[key] = rec;
+    return;
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  QSM_CUDA(cudaEventCreate(&e0));
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    throw QsmError(QSM_ERR_CUDA, "autotuner: event creation failed");
+  }
+  std::vector<float> best(cands.size(), 3.0e38f);
+  try {
+    for (int c : cands) launch(c);  // warm-up (raises shared-memory limits, loads the code)
+    QSM_CUDA(cudaGetLastError());
+    constexpr int kRounds = 3, kReps = 5;
+    for (int r = 0; r < kRounds; ++r) {
+      for (size_t i = 0; i < cands.size(); ++i) {
+        QSM_CUDA(cudaEventRecord(e0, ctx->stream));
+        for (int k = 0; k < kReps; ++k) launch(cands[i]);
+        QSM_CUDA(cudaEventRecord(e1, ctx->stream));
+        QSM_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        QSM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        best[i] = std::min(best[i], 1000.f * ms / kReps);
+      }
+    }
+  } catch (...) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  size_t k = 0;
+  for (size_t i = 1; i < cands.size(); ++i)
+    if (best[i] < best[k]) k = i;
+  rec.choice = cands[k];
+  for (size_t i = 0; i < cands.size(); ++i) rec.us.emplace_back(cands[i], best[i]);
+  ctx->tuned[key] = rec;
+}
+
 void ws_release(qsm_ctx* ctx) {
   cudaStreamSynchronize(ctx->stream);
   for (auto& kv : ctx->ws)
@@ -374,6 +426,44 @@ int qsm_ctx_get_krylov_precision(const qsm_ctx* ctx) { return ctx ? ctx->krylov_
 qsm_status qsm_ctx_set_input_check(qsm_ctx* ctx, int on) {
   if (ctx == nullptr) return QSM_ERR_INVALID_ARGUMENT;
   ctx->check_inputs = on != 0;
+  return QSM_OK;
+}
+
+qsm_status qsm_ctx_set_autotune(qsm_ctx* ctx, int on) {
+  if (ctx == nullptr) return QSM_ERR_INVALID_ARGUMENT;
+  ctx->autotune = on != 0;
+  return QSM_OK;
+}
+
+qsm_status qsm_ctx_force_launch_shape(qsm_ctx* ctx, int shape) {
+  if (ctx == nullptr) return QSM_ERR_INVALID_ARGUMENT;
+  if (shape < -1 || shape > kTuneMaxShape) {
+    ctx->err = "launch shape must be -1 (none) or 0.." + std::to_string(kTuneMaxShape);
+    return QSM_ERR_INVALID_ARGUMENT;
+  }
+  ctx->forced_shape = shape;
+  return QSM_OK;
+}
+
+size_t qsm_ctx_autotune_count(const qsm_ctx* ctx) { return ctx ? ctx->tuned.size() : 0; }
+
+qsm_status qsm_ctx_autotune_entry(const qsm_ctx* ctx, size_t i, char* key, size_t key_cap, int* choice,
+                                  int* candidates, float* us, size_t cap, size_t* count) {
+  if (ctx == nullptr || i >= ctx->tuned.size()) return QSM_ERR_INVALID_ARGUMENT;
+  auto it = ctx->tuned.begin();
+  std::advance(it, (long)i);
+  if (key != nullptr && key_cap > 0) {
+    const size_t n = std::min(key_cap - 1, it->first.size());
+    std::memcpy(key, it->first.data(), n);
+    key[n] = '\0';
+  }
+  if (choice) *choice = it->second.choice;
+  const size_t n = it->second.us.size();
+  if (count) *count = n;
+  for (size_t k = 0; k < n && k < cap; ++k) {
+    if (candidates) candidates[k] = it->second.us[k].first;
+    if (us) us[k] = it->second.us[k].second;
+  }
   return QSM_OK;
 }
 

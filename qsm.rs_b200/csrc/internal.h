@@ -5,6 +5,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <functional>
 #include <map>
 #include <stdexcept>
 #include <string>
@@ -46,6 +47,15 @@ struct ProfRec {
   cudaEvent_t start, stop;
 };
 
+// Largest launch-shape number of the autotuned passes (launch.cuh).
+constexpr int kTuneMaxShape = 63;
+
+// One autotuned launch shape: the chosen candidate and each candidate's best time.
+struct TuneRec {
+  int choice = 0;
+  std::vector<std::pair<int, float>> us;  // (candidate, microseconds per launch)
+};
+
 struct ProfStat {
   uint64_t launches = 0;
   double total_ms = 0.0;
@@ -59,6 +69,9 @@ struct qsm_ctx {
   int plan_mode = QSM_PLANS_COMPILED;  // qsm_ctx_set_plan_mode
   int krylov_precision = QSM_PRECISION_F64;  // qsm_ctx_set_krylov_precision (mixed contexts)
   bool check_inputs = false;  // qsm_ctx_set_input_check
+  bool autotune = true;  // qsm_ctx_set_autotune
+  int forced_shape = -1;  // qsm_ctx_force_launch_shape (-1: none)
+  std::map<std::string, qsm::TuneRec> tuned;  // launch shapes chosen by the autotuner
   long long alloc_fail_after = -1;  // qsm_ctx_inject_alloc_failure: allocations left before one fails
   cudaStream_t stream = nullptr;
   std::string err;

@@ -248,19 +248,36 @@ template <class K> unsigned persistent_grid(qsm_ctx* ctx, K kernel, int threads,
   return (unsigned)g;
 }
 
-template <typename T> TileWalk tile_walk(const Fft3<T>& f, int axis, int P) {
+// Tile walk of a Y (axis 1) or Z (axis 2) pass with P-column tiles.  edge: walk a
+// narrow column remainder (at most P/4 columns) as edge tiles (TileWalk); only the
+// compile-time kernels read edge tiles.
+template <typename T> TileWalk tile_walk(const Fft3<T>& f, int axis, int P, bool edge = false) {
   TileWalk w;
   w.ntx = (f.g.nxh + P - 1) / P;
+  w.nouter = axis == 1 ? f.g.nz : f.g.ny;
   if (axis == 1) {  // Y: outer = z
-    w.ntiles = w.ntx * f.g.nz;
     w.ostride = (long long)f.g.pitch * f.g.ny;
     w.estride = f.g.pitch;
   } else {  // Z: outer = y
-    w.ntiles = w.ntx * f.g.ny;
     w.ostride = f.g.pitch;
     w.estride = (long long)f.g.pitch * f.g.ny;
   }
+  const int rem = f.g.nxh % P;
+  w.nedge = 0;
+  w.col_edge = f.g.nxh;
+  if (edge && rem > 0 && 4 * rem <= P) {
+    w.ntx = f.g.nxh / P;
+    w.nedge = rem;
+    w.col_edge = w.ntx * P;
+  }
+  w.nmain = w.ntx * w.nouter;
+  w.ntiles = w.nmain + w.nedge * ((w.nouter + P - 1) / P);
   return w;
+}
+// True when tile_walk(..., edge = true) has edge tiles.
+template <typename T> bool has_edge_tiles(const Fft3<T>& f, int P) {
+  const int rem = f.g.nxh % P;
+  return rem > 0 && 4 * rem <= P;
 }
 
 // shared memory of the direct-fetch kernels: twiddles + one tile (the stage exchange)
@@ -296,7 +313,58 @@ template <typename T, class K> int yz_tile_width(K kernel, int n, int Tn) {
 // one of them.
 constexpr int kFxCols = 16;
 constexpr int kZmCols = 8;  // columns per tile of the fused Z pass
-template <class K> bool fx_launch_ok(qsm_ctx* ctx, K kern, int threads, size_t smem, unsigned* grid, long long work) {
+
+// ----------------------------------------------------------------- autotuner --
+// Launch shapes of the compile-time Y/Z passes, as fields of a candidate number:
+//   kTuneEdge         edge tiles for a narrow column remainder (TileWalk)
+//   kTuneBlockPerTile one block per tile, scheduled by the hardware, instead of a
+//                     persistent grid of resident blocks walking the tiles
+//   bits 2..5         persistent grid: resident blocks per SM (0 = as many as fit)
+// Every shape runs the same arithmetic on every column, so results do not depend on the
+// choice.  The choice is made per context by timing each candidate once on scratch
+// buffers (autotune_pick) and cached under a key naming the pass and its geometry;
+// launches whose key is not cached use shape 0, the persistent grid without edge tiles.
+constexpr int kTuneEdge = 1, kTuneBlockPerTile = 2, kTuneBpsmShift = 2;  // kTuneMaxShape: internal.h
+inline int tune_bpsm(int shape) { return (shape >> kTuneBpsmShift) & 15; }
+bool stream_capturing(qsm_ctx* ctx);
+// Time launch(c) for every candidate c on ctx->stream (after one warm-up launch each,
+// three rounds of five launches; the best round counts) and cache the fastest under key.
+void autotune_pick(qsm_ctx* ctx, const std::string& key, const std::vector<int>& cands,
+                   const std::function<void(int)>& launch);
+inline int tuned_shape(const qsm_ctx* ctx, const std::string& key) {
+  if (ctx->forced_shape >= 0) return ctx->forced_shape;
+  if (!ctx->autotune) return 0;
+  auto it = ctx->tuned.find(key);
+  return it == ctx->tuned.end() ? 0 : it->second.choice;
+}
+// Whether a tuning run for key should happen now (autotuner on, key not cached, stream
+// not capturing).
+inline bool autotune_due(qsm_ctx* ctx, const std::string& key) {
+  return ctx->autotune && ctx->forced_shape < 0 && ctx->tuned.find(key) == ctx->tuned.end() && !stream_capturing(ctx);
+}
+template <typename T> std::string yz_tune_key(const char* pass, const Fft3<T>& f, int axis, int dir) {
+  return std::string(pass) + (axis == 1 ? ":y" : ":z") + (dir < 0 ? "-" : "+") + ":" + std::to_string(f.g.nx) +
+         "x" + std::to_string(f.g.ny) + "x" + std::to_string(f.g.nz) + (sizeof(T) == 4 ? ":f32" : ":f64");
+}
+// Candidates: persistent grids of the occupancy limit and of one block per SM fewer,
+// and one block per tile, each with and without edge tiles where the grid has them.
+template <typename T, class K>
+std::vector<int> yz_candidates(const Fft3<T>& f, int P, K kern, int threads, size_t smem) {
+  int per_sm = 0;
+  QSM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
+  std::vector<int> base{0, kTuneBlockPerTile};
+  if (per_sm >= 2 && per_sm - 1 <= 15) base.push_back((per_sm - 1) << kTuneBpsmShift);
+  std::vector<int> c = base;
+  if (has_edge_tiles(f, P))
+    for (int b : base) c.push_back(b | kTuneEdge);
+  return c;
+}
+
+// Grid of a compile-time Y/Z pass over `work` tiles: resident blocks (persistent) or one
+// block per tile; false when the block does not fit on an SM.
+template <class K>
+bool fx_launch_ok(qsm_ctx* ctx, K kern, int threads, size_t smem, unsigned* grid, long long work,
+                  bool per_tile = false, int bpsm = 0) {
   if (smem > 227u * 1024u) return false;
   ensure_smem(kern, smem);
   int per_sm = 0;
@@ -305,9 +373,33 @@ template <class K> bool fx_launch_ok(qsm_ctx* ctx, K kern, int threads, size_t s
     return false;
   }
   if (per_sm < 1) return false;
-  long long g = (long long)per_sm * sm_count(ctx);
+  if (bpsm > 0 && bpsm < per_sm) per_sm = bpsm;
+  long long g = per_tile ? work : (long long)per_sm * sm_count(ctx);
   if (g > work) g = work;
   *grid = (unsigned)(g < 1 ? 1 : g);
+  return true;
+}
+
+// One compile-time Y/Z pass (k_pass_yz_dx, FP a FixedPlan) in launch shape `shape`.
+// scoped: count and (when profiling) time the launch under the pass's name.
+template <typename T, int DIR, int AXIS, class FP>
+bool launch_yz_fx(qsm_ctx* ctx, const Fft3<T>& f, int shape, const cplx_t<T>* src, cplx_t<T>* dst,
+                  const int* done, bool scoped) {
+  const cplx_t<T>* tw = (AXIS == 1) ? f.twy : f.twz;
+  auto kern = k_pass_yz_dx<T, DIR, FP, kFxCols>;
+  const size_t smem = dx_smem<T>(FP::n, kFxCols);
+  const TileWalk w = tile_walk(f, AXIS, kFxCols, (shape & kTuneEdge) != 0);
+  unsigned grid = 0;
+  if (!fx_launch_ok(ctx, kern, kFxCols * FP::T, smem, &grid, w.ntiles, (shape & kTuneBlockPerTile) != 0,
+                    tune_bpsm(shape)))
+    return false;
+  if (!scoped) {
+    kern<<<grid, dim3(kFxCols, FP::T), smem, ctx->stream>>>(f.g, w, tw, src, dst, done);
+    return true;
+  }
+  LaunchScope ls(ctx, AXIS == 1 ? (DIR < 0 ? "fft_y_fwd" : "fft_y_inv") : (DIR < 0 ? "fft_z_fwd" : "fft_z_inv"));
+  kern<<<grid, dim3(kFxCols, FP::T), smem, ctx->stream>>>(f.g, w, tw, src, dst, done);
+  ls.done();
   return true;
 }
 
@@ -318,19 +410,11 @@ bool run_yz_fixed(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T
     return false;
   } else {
     const FftPlan1D& pl = (AXIS == 1) ? f.py : f.pz;
-    const cplx_t<T>* tw = (AXIS == 1) ? f.twy : f.twz;
 #define QSM_TRY_YZ(N_, T_, R0_, R1_, R2_)                                                         \
     if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(pl) && kFxCols * T_ <= 1024) {                   \
       using FP = FixedPlan<N_, T_, R0_, R1_, R2_>;                                                \
-      auto kern = k_pass_yz_dx<T, DIR, FP, kFxCols>;                                              \
-      const size_t smem = dx_smem<T>(N_, kFxCols);                                                \
-      const TileWalk w = tile_walk(f, AXIS, kFxCols);                                             \
-      unsigned grid = 0;                                                                          \
-      if (!fx_launch_ok(ctx, kern, kFxCols * T_, smem, &grid, w.ntiles)) return false;            \
-      LaunchScope ls(ctx, AXIS == 1 ? (DIR < 0 ? "fft_y_fwd" : "fft_y_inv") : (DIR < 0 ? "fft_z_fwd" : "fft_z_inv")); \
-      kern<<<grid, dim3(kFxCols, T_), smem, ctx->stream>>>(f.g, w, tw, src, dst, done);          \
-      ls.done();                                                                                  \
-      return true;                                                                                \
+      const int shape = tuned_shape(ctx, yz_tune_key<T>("yz_fx", f, AXIS, DIR));                  \
+      return launch_yz_fx<T, DIR, AXIS, FP>(ctx, f, shape, src, dst, done, true);                 \
     }
     QSM_FIXED_PLANS(QSM_TRY_YZ)
     if constexpr (W) {
@@ -440,6 +524,87 @@ template <typename T> int zm_tile_width(int n, int m, int Tn) {
   return 0;
 }
 
+// One compile-time multiplier Z pass (k_z_fused_m_fx, FP a FixedPlan) in launch shape
+// `shape`; scoped as in launch_yz_fx.
+template <typename T, class FP>
+bool launch_zm_fx(qsm_ctx* ctx, const Fft3<T>& f, int shape, const cplx_t<T>* src, cplx_t<T>* dst, const T* mult,
+                  const int* done, bool scoped) {
+  auto kfx = k_z_fused_m_fx<T, FP, kZmCols>;
+  const size_t smem = zm_smem<T>(FP::n, FP::n, kZmCols);
+  const TileWalk w = tile_walk(f, 2, kZmCols, (shape & kTuneEdge) != 0);
+  unsigned grid = 0;
+  if (!fx_launch_ok(ctx, kfx, kZmCols * FP::T, smem, &grid, w.ntiles, (shape & kTuneBlockPerTile) != 0,
+                    tune_bpsm(shape)))
+    return false;
+  if (!scoped) {
+    kfx<<<grid, dim3(kZmCols, FP::T), smem, ctx->stream>>>(f.g, w, f.twz, src, dst, mult, done);
+    return true;
+  }
+  LaunchScope ls(ctx, "fft_z_fused");
+  kfx<<<grid, dim3(kZmCols, FP::T), smem, ctx->stream>>>(f.g, w, f.twz, src, dst, mult, done);
+  ls.done();
+  return true;
+}
+
+// Tune the launch shape of the compile-time Y/Z pass (DIR, AXIS) and of the multiplier
+// Z pass for grid f, running the candidates in place on `scratch` (a half spectrum of f
+// whose contents may be overwritten) and `mscratch` (a real half-spectrum array).  No-op
+// when the lengths have no compile-time pass, the shapes are cached, the autotuner is
+// off or the stream is capturing.
+template <typename T, int DIR, int AXIS, bool W>
+void tune_yz_fixed(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* scratch) {
+  if constexpr (std::is_same<T, float>::value) {
+    if (!compiled_plans(ctx)) return;
+    const std::string key = yz_tune_key<T>("yz_fx", f, AXIS, DIR);
+    if (!autotune_due(ctx, key)) return;
+    const FftPlan1D& pl = (AXIS == 1) ? f.py : f.pz;
+#define QSM_TUNE_YZ(N_, T_, R0_, R1_, R2_)                                                        \
+    if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(pl) && kFxCols * T_ <= 1024) {                   \
+      using FP = FixedPlan<N_, T_, R0_, R1_, R2_>;                                                \
+      auto kern = k_pass_yz_dx<T, DIR, FP, kFxCols>;                                              \
+      const size_t smem = dx_smem<T>(FP::n, kFxCols);                                             \
+      ensure_smem(kern, smem);                                                                    \
+      const auto cands = yz_candidates(f, kFxCols, kern, kFxCols * FP::T, smem);                  \
+      autotune_pick(ctx, key, cands, [&](int c) {                                                 \
+        launch_yz_fx<T, DIR, AXIS, FP>(ctx, f, c, scratch, scratch, nullptr, false);               \
+      });                                                                                         \
+      return;                                                                                     \
+    }
+    QSM_FIXED_PLANS(QSM_TUNE_YZ)
+    if constexpr (W) {
+      QSM_FIXED_PLANS_WIDE(QSM_TUNE_YZ)
+    }
+#undef QSM_TUNE_YZ
+  }
+}
+
+template <typename T, bool W>
+void tune_z_fused_m(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* scratch, T* mscratch) {
+  if constexpr (std::is_same<T, float>::value) {
+    if (!compiled_plans(ctx)) return;
+    const std::string key = yz_tune_key<T>("zm_fx", f, 2, -1);
+    if (!autotune_due(ctx, key)) return;
+    const FftPlan1D& pl = f.pz;
+#define QSM_TUNE_ZM(N_, T_, R0_, R1_, R2_)                                                        \
+    if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(pl) && kZmCols * T_ <= 1024) {                   \
+      using FP = FixedPlan<N_, T_, R0_, R1_, R2_>;                                                \
+      auto kfx = k_z_fused_m_fx<T, FP, kZmCols>;                                                  \
+      const size_t smem = zm_smem<T>(FP::n, FP::n, kZmCols);                                      \
+      ensure_smem(kfx, smem);                                                                     \
+      const auto cands = yz_candidates(f, kZmCols, kfx, kZmCols * FP::T, smem);                   \
+      autotune_pick(ctx, key, cands, [&](int c) {                                                 \
+        launch_zm_fx<T, FP>(ctx, f, c, scratch, scratch, mscratch, nullptr, false);                \
+      });                                                                                         \
+      return;                                                                                     \
+    }
+    QSM_FIXED_PLANS(QSM_TUNE_ZM)
+    if constexpr (W) {
+      QSM_FIXED_PLANS_WIDE(QSM_TUNE_ZM)
+    }
+#undef QSM_TUNE_ZM
+  }
+}
+
 // Z fused pass with a precomputed real multiplier array (spectrum layout); W adds
 // QSM_FIXED_PLANS_WIDE.
 template <typename T, bool W = false>
@@ -451,16 +616,8 @@ void run_z_fused_m(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<
 #define QSM_TRY_ZM(N_, T_, R0_, R1_, R2_)                                                         \
     if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(pl) && kZmCols * T_ <= 1024) {                   \
       using FP = FixedPlan<N_, T_, R0_, R1_, R2_>;                                                \
-      auto kfx = k_z_fused_m_fx<T, FP, kZmCols>;                                                  \
-      const size_t smem = zm_smem<T>(N_, N_, kZmCols);                                                \
-      const TileWalk w = tile_walk(f, 2, kZmCols);                                                \
-      unsigned grid = 0;                                                                          \
-      if (fx_launch_ok(ctx, kfx, kZmCols * T_, smem, &grid, w.ntiles)) {                          \
-        LaunchScope ls(ctx, "fft_z_fused");                                                       \
-        kfx<<<grid, dim3(kZmCols, T_), smem, ctx->stream>>>(f.g, w, f.twz, src, dst, mult, done); \
-        ls.done();                                                                                \
-        return;                                                                                   \
-      }                                                                                           \
+      const int shape = tuned_shape(ctx, yz_tune_key<T>("zm_fx", f, 2, -1));                      \
+      if (launch_zm_fx<T, FP>(ctx, f, shape, src, dst, mult, done, true)) return;                 \
     }
     QSM_FIXED_PLANS(QSM_TRY_ZM)
     if constexpr (W) {

@@ -311,12 +311,12 @@ __global__ void k_x_r2c_fx(Geom g, const cplx_t<T>* __restrict__ twg, cplx_t<T>*
                            const int* __restrict__ done) {
   using C = cplx_t<T>;
   constexpr int N = FP::n, TT = FP::T, NXH = N / 2 + 1;
-  if (done != nullptr && *done) return;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* tw = reinterpret_cast<C*>(smraw);
   C* sm = tw + N;
   const int tid = threadIdx.x + threadIdx.y * blockDim.x;
   for (int i = tid; i < N; i += blockDim.x * blockDim.y) tw[i] = twg[i];
+  if (done != nullptr && *done) return;
   const int t = threadIdx.x;
   const int p = threadIdx.y;
   const int nrows = g.nrows();
@@ -350,12 +350,12 @@ __global__ void k_x_c2r_fx(Geom g, const cplx_t<T>* __restrict__ twg, const cplx
                            const int* __restrict__ done) {
   using C = cplx_t<T>;
   constexpr int N = FP::n, TT = FP::T;
-  if (done != nullptr && *done) return;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* tw = reinterpret_cast<C*>(smraw);
   C* sm = tw + N;
   const int tid = threadIdx.x + threadIdx.y * blockDim.x;
   for (int i = tid; i < N; i += blockDim.x * blockDim.y) tw[i] = twg[i];
+  if (done != nullptr && *done) return;
   const int t = threadIdx.x;
   const int p = threadIdx.y;
   const int nrows = g.nrows();
@@ -395,10 +395,67 @@ __global__ void k_x_c2r_fx(Geom g, const cplx_t<T>* __restrict__ twg, const cplx
 // ---------------------------------------------------------------------------
 struct TileWalk {
   int ntx;        // column tiles along x'
-  int ntiles;     // ntx * nouter
+  int ntiles;     // tiles in all: nmain, plus the edge tiles
   long long ostride;  // global stride of the outer index
   long long estride;  // global stride along the transform axis
+  // Edge tiles (compile-time kernels only).  Main tiles are P consecutive columns at
+  // one outer index.  When the last nedge columns (from col_edge) would fill only a
+  // small part of a P-wide tile, as the one Nyquist column of an even length does
+  // (129 = 8 * 16 + 1), they are left out of the main tiles and walked as edge tiles
+  // instead: one of those columns at P consecutive outer indices, so no tile is mostly
+  // idle lanes.  Their loads are scattered (one element per row and lane), so the walk
+  // takes them first (tile indices below nfirst = ntiles - nmain) and the main tiles
+  // after them, rather than leaving the slowest tiles for the end.  nedge = 0: none.
+  int nmain;
+  int nouter;
+  int col_edge;
+  int nedge;
 };
+
+// Column and outer index of lane px in a tile (main or edge), and whether it is a
+// valid element column.
+__device__ __forceinline__ bool tile_pos(const Geom& g, const TileWalk& w, int tile, int px, int P, int& col,
+                                         int& outer) {
+  const int nfirst = w.ntiles - w.nmain;
+  if (tile >= nfirst) {
+    const int mt = tile - nfirst;
+    const int tx = mt % w.ntx;
+    outer = mt / w.ntx;
+    col = tx * P + px;
+    return col < g.nxh;
+  }
+  const int et = tile;
+  const int ob = (et / w.nedge) * P;
+  col = w.col_edge + (et - (et / w.nedge) * w.nedge);
+  outer = ob + px < w.nouter ? ob + px : w.nouter - 1;  // clamped: inactive lanes address a valid row
+  return ob + px < w.nouter;
+}
+
+// 4- or 8-byte global -> shared copies (edge tiles: one element per lane)
+template <int B> __device__ __forceinline__ void cp_async_small(void* smem, const void* gmem, bool pred) {
+  static_assert(B == 4 || B == 8 || B == 16, "cp.async copies 4, 8 or 16 bytes");
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int nbytes = pred ? B : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(s), "l"(gmem), "n"(B), "r"(nbytes)
+               : "memory");
+}
+
+// Stage an edge tile (element e of lane px at buf[e * P + px]) of complex (C) or real
+// (C = T) values.
+template <typename C>
+__device__ __forceinline__ void issue_edge_tile(const C* __restrict__ src, C* buf, const TileWalk& w, int tile,
+                                                int n, int P) {
+  const int et = tile;
+  const int ob = (et / w.nedge) * P;
+  const int col = w.col_edge + (et - (et / w.nedge) * w.nedge);
+  const int nth = blockDim.x * blockDim.y;
+  for (int c = threadIdx.x + threadIdx.y * blockDim.x; c < n * P; c += nth) {
+    const int e = c / P, px = c - e * P;
+    const bool ok = ob + px < w.nouter;
+    const C* gp = src + col + (long long)(ok ? ob + px : 0) * w.ostride + (long long)e * w.estride;
+    cp_async_small<(int)sizeof(C)>(buf + e * P + px, gp, ok);
+  }
+}
 
 template <typename C>
 __device__ __forceinline__ void issue_tile(const C* __restrict__ src, C* buf, const Geom& g, const TileWalk& w,
@@ -723,20 +780,19 @@ __global__ void __launch_bounds__(P* FP::T, (P * FP::T <= 256 ? 3 : 1))
                  const int* __restrict__ done) {
   using C = cplx_t<T>;
   constexpr int n = FP::n;
-  if (done != nullptr && *done) return;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* tw = reinterpret_cast<C*>(smraw);
   C* buf = tw + ((n + 7) & ~7);
   const int tid = threadIdx.x + threadIdx.y * P;
   for (int i = tid; i < n; i += P * FP::T) tw[i] = twg[i];
+  if (done != nullptr && *done) return;
   const int px = threadIdx.x;
   const int t = threadIdx.y;
   SAStridedC<P> sa;
   C* sp = buf + px;
   for (int tile = blockIdx.x; tile < w.ntiles; tile += gridDim.x) {
-    const int tx = tile % w.ntx, outer = tile / w.ntx;
-    const int col = tx * P + px;
-    const bool active = col < g.nxh;
+    int col, outer;
+    const bool active = tile_pos(g, w, tile, px, P, col, outer);
     const long long base = col + (long long)outer * w.ostride;
     auto fetch = [&](int e) -> C { return src[base + e * w.estride]; };
     auto emit = [&](int e, C v) { dst[base + e * w.estride] = v; };
@@ -807,7 +863,6 @@ __global__ void __launch_bounds__(P* FP::T, zm_min_blocks<P * FP::T>())
                    const T* __restrict__ mult, const int* __restrict__ done) {
   using C = cplx_t<T>;
   constexpr int n = FP::n;
-  if (done != nullptr && *done) return;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* tw = reinterpret_cast<C*>(smraw);
   C* buf0 = tw + ((n + 7) & ~7);
@@ -816,14 +871,21 @@ __global__ void __launch_bounds__(P* FP::T, zm_min_blocks<P * FP::T>())
   T* mb1 = mb0 + ((n * P + 3) & ~3);
   const int tid = threadIdx.x + threadIdx.y * P;
   for (int i = tid; i < n; i += P * FP::T) tw[i] = twg[i];
+  if (done != nullptr && *done) return;
   const int px = threadIdx.x;
   const int t = threadIdx.y;
   SAStridedC<P> sa;
+  auto issue = [&](int tl, C* b, T* mb) {
+    if (tl >= w.ntiles - w.nmain) {
+      issue_tile(src, b, g, w, tl - (w.ntiles - w.nmain), n, P);
+      issue_mtile(mult, mb, g, w, tl - (w.ntiles - w.nmain), n, P);
+    } else {
+      issue_edge_tile(src, b, w, tl, n, P);
+      issue_edge_tile(mult, mb, w, tl, n, P);
+    }
+  };
   int tile = blockIdx.x;
-  if (tile < w.ntiles) {
-    issue_tile(src, buf0, g, w, tile, n, P);
-    issue_mtile(mult, mb0, g, w, tile, n, P);
-  }
+  if (tile < w.ntiles) issue(tile, buf0, mb0);
   cp_async_commit();
   for (int it = 0; tile < w.ntiles; tile += gridDim.x, ++it) {
     C* cur = (it & 1) ? buf1 : buf0;
@@ -831,16 +893,12 @@ __global__ void __launch_bounds__(P* FP::T, zm_min_blocks<P * FP::T>())
     T* mcur = (it & 1) ? mb1 : mb0;
     T* mnxt = (it & 1) ? mb0 : mb1;
     const int next = tile + gridDim.x;
-    if (next < w.ntiles) {
-      issue_tile(src, nxt, g, w, next, n, P);
-      issue_mtile(mult, mnxt, g, w, next, n, P);
-    }
+    if (next < w.ntiles) issue(next, nxt, mnxt);
     cp_async_commit();
     cp_async_wait<1>();
     __syncthreads();
-    const int tx = tile % w.ntx, iy = tile / w.ntx;
-    const int col = tx * P + px;
-    const bool active = col < g.nxh;
+    int col, iy;
+    const bool active = tile_pos(g, w, tile, px, P, col, iy);
     const long long base = col + (long long)iy * w.ostride;
     C* sp = cur + px;
     auto fetch = [&](int e) -> C { return sp[sa(e)]; };

@@ -689,8 +689,16 @@ template <typename T> struct TvVol {
   double* out;
 };
 
+// Autotune the launch shapes of the iteration's Y and fused Z passes for this volume's
+// grid, on its spectrum and multiplier buffers before they hold data (instantiated once,
+// in tv_fft.cu).
+template <typename T> void tv_tune(qsm_ctx* ctx, const TvVol<T>& v);
+extern template void tv_tune<float>(qsm_ctx*, const TvVol<float>&);
+extern template void tv_tune<double>(qsm_ctx*, const TvVol<double>&);
+
 // Allocate one volume's buffers (workspace names prefixed by `pre`), launch shapes and
-// constants; `thr` is the shrink threshold.  Nothing is enqueued.
+// constants; `thr` is the shrink threshold.  The only work enqueued is the launch-shape
+// tuning of a grid the context has not seen (tv_tune), which overwrites the new buffers.
 template <typename T>
 void tv_alloc(qsm_ctx* ctx, TvVol<T>& v, const std::string& pre, const GridDims& d, const double bdir[3],
               double rho_mul, double thr, TvState* st, const uint8_t* d_mask, double* d_out) {
@@ -740,6 +748,7 @@ void tv_alloc(qsm_ctx* ctx, TvVol<T>& v, const std::string& pre, const GridDims&
   v.out = d_out;
   v.mult = ws<T>(ctx, pre + "mult", (size_t)v.f.g.hsize());
   v.use_mult = zm_tile_width<T>(d.nz, v.f.pz.m, v.f.pz.T) > 0;
+  tv_tune(ctx, v);
 }
 
 // Initial state on ctx->stream: y_0 = x0 (x_0 = 0), u = 0, iteration counter 1.
@@ -810,6 +819,12 @@ template <typename T> void tv_fft(qsm_ctx* ctx, const TvVol<T>& v, int q) {
 }
 extern template void tv_fft<float>(qsm_ctx*, const TvVol<float>&, int);
 extern template void tv_fft<double>(qsm_ctx*, const TvVol<double>&, int);
+
+template <typename T> void tv_tune(qsm_ctx* ctx, const TvVol<T>& v) {
+  tune_yz_fixed<T, -1, 1, true>(ctx, v.f, v.spec);
+  tune_yz_fixed<T, +1, 1, true>(ctx, v.f, v.spec);
+  if (v.use_mult) tune_z_fused_m<T, true>(ctx, v.f, v.spec, v.mult);
+}
 
 template <typename T> void tv_iter(qsm_ctx* ctx, const TvVol<T>& v, int q) {
   tv_step_launch(ctx, v, q, 0);

@@ -154,6 +154,32 @@ class Context:
     def krylov_precision(self, p: str):
         _check(self, self._lib.qsm_ctx_set_krylov_precision(self._h, _prec_code(p)))
 
+    def set_autotune(self, on: bool):
+        """Autotuner of the compile-time Y/Z pass launch shapes (on by default); results
+        do not depend on it."""
+        _check(self, self._lib.qsm_ctx_set_autotune(self._h, 1 if on else 0))
+
+    def force_launch_shape(self, shape: int):
+        """Test hook: run every tunable pass in candidate shape 0..3, or -1 for the
+        autotuner's choice."""
+        _check(self, self._lib.qsm_ctx_force_launch_shape(self._h, int(shape)))
+
+    def autotune_entries(self) -> dict:
+        """Launch shapes the autotuner chose: {key: {"choice": c, "us": {candidate: us}}}."""
+        out = {}
+        for i in range(int(self._lib.qsm_ctx_autotune_count(self._h))):
+            key = C.create_string_buffer(256)
+            choice = C.c_int(0)
+            cands = (C.c_int * 16)()
+            us = (C.c_float * 16)()
+            count = C.c_size_t(0)
+            _check(self, self._lib.qsm_ctx_autotune_entry(self._h, i, key, 256, C.byref(choice), cands, us, 16,
+                                                          C.byref(count)))
+            n = min(int(count.value), 16)
+            out[key.value.decode()] = {"choice": int(choice.value),
+                                       "us": {int(cands[k]): round(float(us[k]), 2) for k in range(n)}}
+        return out
+
     def set_input_check(self, on: bool):
         """Reject input volumes holding NaN or infinity (off by default, as in the reference)."""
         _check(self, self._lib.qsm_ctx_set_input_check(self._h, 1 if on else 0))

@@ -131,6 +131,12 @@ _SIGS = [
     ("qsm_ctx_set_krylov_precision", C.c_int, [C.c_void_p, C.c_int]),
     ("qsm_ctx_get_krylov_precision", C.c_int, [C.c_void_p]),
     ("qsm_ctx_set_input_check", C.c_int, [C.c_void_p, C.c_int]),
+    ("qsm_ctx_set_autotune", C.c_int, [C.c_void_p, C.c_int]),
+    ("qsm_ctx_force_launch_shape", C.c_int, [C.c_void_p, C.c_int]),
+    ("qsm_ctx_autotune_count", C.c_size_t, [C.c_void_p]),
+    ("qsm_ctx_autotune_entry", C.c_int, [C.c_void_p, C.c_size_t, C.c_char_p, C.c_size_t, C.POINTER(C.c_int),
+                                         C.POINTER(C.c_int), C.POINTER(C.c_float), C.c_size_t,
+                                         C.POINTER(C.c_size_t)]),
     ("qsm_ctx_inject_alloc_failure", C.c_int, [C.c_void_p, C.c_longlong]),
     ("qsm_ctx_release_workspace", C.c_int, [C.c_void_p]),
     ("qsm_last_error", C.c_char_p, [C.c_void_p]),
