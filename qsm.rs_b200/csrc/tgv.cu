@@ -408,37 +408,65 @@ __device__ __forceinline__ bool interior(int i, int j, int k, const Box& b) {
 // `zchunk` planes of one (i, j) column: no index division, and the y/z neighbours of a
 // voxel are the tile's own recent loads (L1) rather than another block's (L2).
 constexpr int kTgvBX = 32, kTgvBY = 8;
+// Resident blocks per SM the primal kernel is compiled for (its register budget).
+constexpr int kTgvPrimalBlocks = 6;
 
 // Dual update (tgv.rs:1157-1213).  q selects the buffers holding phi_, chi_, w_.
+// Every array is accessed through a restrict-qualified pointer (no two alias, and no
+// voxel reads what another voxel writes in the same launch), so the compiler issues a
+// plane's loads together instead of ordering them behind the stores of the update; the
+// two masks of the next plane are fetched while the current plane computes, so a plane's
+// data loads wait on no mask load.  The arithmetic is that of the reference, in its order.
 __global__ void __launch_bounds__(kTgvBX* kTgvBY) k_tgv_dual(Box b, TgvArrays A, TgvScalars c, TgvConst K, int q,
                                                              int zchunk, const TgvFlag* flag) {
   if (flag->done) return;
   const long long sxy = (long long)b.bx * b.by;
-  const float* phb = A.phi[q];
-  const float* chb = A.chi[q];
-  const float* wbx = A.w[q][0];
-  const float* wby = A.w[q][1];
-  const float* wbz = A.w[q][2];
+  const float* __restrict__ phb = A.phi[q];
+  const float* __restrict__ chb = A.chi[q];
+  const float* __restrict__ wbx = A.w[q][0];
+  const float* __restrict__ wby = A.w[q][1];
+  const float* __restrict__ wbz = A.w[q][2];
+  const uint8_t* __restrict__ m0 = A.m0;
+  const uint8_t* __restrict__ me = A.me;
+  const float* __restrict__ lphi = A.lphi;
+  float* __restrict__ eta = A.eta;
+  float* __restrict__ p0 = A.p[0];
+  float* __restrict__ p1 = A.p[1];
+  float* __restrict__ p2 = A.p[2];
+  float* __restrict__ q0 = A.q[0];
+  float* __restrict__ q1 = A.q[1];
+  float* __restrict__ q2 = A.q[2];
+  float* __restrict__ q3 = A.q[3];
+  float* __restrict__ q4 = A.q[4];
+  float* __restrict__ q5 = A.q[5];
   const int i = blockIdx.x * kTgvBX + threadIdx.x, j = blockIdx.y * kTgvBY + threadIdx.y;
   if (i >= b.bx || j >= b.by) return;
+  const int kbeg = blockIdx.z * zchunk;
   const int kend = min(b.bz, (int)(blockIdx.z + 1) * zchunk);
-  for (int k = blockIdx.z * zchunk; k < kend; ++k) {
-    const long long s = (long long)k * sxy + (long long)j * b.bx + i;
-    const bool in0 = A.m0[s] != 0, inm = A.me[s] != 0;
+  if (kbeg >= kend) return;
+  long long s = (long long)kbeg * sxy + (long long)j * b.bx + i;
+  uint8_t nm0 = m0[s], nme = me[s];
+  for (int k = kbeg; k < kend; ++k, s += sxy) {
+    const bool in0 = nm0 != 0, inm = nme != 0;
+    if (k + 1 < kend) {
+      nm0 = m0[s + sxy];
+      nme = me[s + sxy];
+    }
+    if (!(in0 || inm)) continue;
     const float cb = chb[s];
     if (in0) {
       const float t1 = lap_neumann([&](long long t) { return phb[t]; }, s, i, j, k, b, sxy, c);
       const float t2 = interior(i, j, k, b) ? stencil27([&](long long t) { return chb[t]; }, s, b.bx, sxy, K) : 0.0f;
-      A.eta[s] += c.sigma * (-t1 + t2 - A.lphi[s]);
+      eta[s] += c.sigma * (-t1 + t2 - lphi[s]);
     }
-    if (in0 || inm) {
+    {
       const float gx = i + 1 < b.bx ? (chb[s + 1] - cb) * c.hx : 0.0f;
       const float gy = j + 1 < b.by ? (chb[s + b.bx] - cb) * c.hy : 0.0f;
       const float gz = k + 1 < b.bz ? (chb[s + sxy] - cb) * c.hz : 0.0f;
       const float s0 = in0 ? c.sstep : 0.0f, s1 = inm ? c.sstep : 0.0f;
-      float px = A.p[0][s] + (s0 * gx - s1 * wbx[s]);
-      float py = A.p[1][s] + (s0 * gy - s1 * wby[s]);
-      float pz = A.p[2][s] + (s0 * gz - s1 * wbz[s]);
+      float px = p0[s] + (s0 * gx - s1 * wbx[s]);
+      float py = p1[s] + (s0 * gy - s1 * wby[s]);
+      float pz = p2[s] + (s0 * gz - s1 * wbz[s]);
       const float nrm = sqrtf(px * px + py * py + pz * pz);
       if (nrm > c.alpha1) {
         const float sc = c.alpha1 / nrm;
@@ -446,9 +474,9 @@ __global__ void __launch_bounds__(kTgvBX* kTgvBY) k_tgv_dual(Box b, TgvArrays A,
         py *= sc;
         pz *= sc;
       }
-      A.p[0][s] = px;
-      A.p[1][s] = py;
-      A.p[2][s] = pz;
+      p0[s] = px;
+      p1[s] = py;
+      p2[s] = pz;
     }
     if (in0) {
       // symgrad (src/utils/gradient.rs:300-372), zero on the far faces
@@ -469,8 +497,8 @@ __global__ void __launch_bounds__(kTgvBX* kTgvBY) k_tgv_dual(Box b, TgvArrays A,
         sxz += ((wbx[s + sxy] - wx0) * c.hz) * 0.5f;
         syz += ((wby[s + sxy] - wy0) * c.hz) * 0.5f;
       }
-      float qq[6] = {A.q[0][s] + c.sstep * sxx, A.q[1][s] + c.sstep * sxy_, A.q[2][s] + c.sstep * sxz,
-                     A.q[3][s] + c.sstep * syy, A.q[4][s] + c.sstep * syz, A.q[5][s] + c.sstep * szz};
+      float qq[6] = {q0[s] + c.sstep * sxx, q1[s] + c.sstep * sxy_, q2[s] + c.sstep * sxz,
+                     q3[s] + c.sstep * syy, q4[s] + c.sstep * syz, q5[s] + c.sstep * szz};
       const float fro = sqrtf(qq[0] * qq[0] + qq[3] * qq[3] + qq[5] * qq[5] +
                               2.0f * (qq[1] * qq[1] + qq[2] * qq[2] + qq[4] * qq[4]));
       if (fro > c.alpha0) {
@@ -478,74 +506,96 @@ __global__ void __launch_bounds__(kTgvBX* kTgvBY) k_tgv_dual(Box b, TgvArrays A,
 #pragma unroll
         for (int t = 0; t < 6; ++t) qq[t] *= sc;
       }
-#pragma unroll
-      for (int t = 0; t < 6; ++t) A.q[t][s] = qq[t];
+      q0[s] = qq[0];
+      q1[s] = qq[1];
+      q2[s] = qq[2];
+      q3[s] = qq[3];
+      q4[s] = qq[4];
+      q5[s] = qq[5];
     }
   }
 }
 
-// Primal update and extrapolation (tgv.rs:1215-1271).  Compiled for six blocks per SM
-// (<= 42 registers): more columns in flight hide its dependent loads better than the
-// unbounded 43-register form (555 vs 712 us per launch at a 23 M-voxel box).  Buffers [1-q] hold the current
+// Primal update and extrapolation (tgv.rs:1215-1271).  Buffers [1-q] hold the current
 // iterate x (read), [q] the extrapolation consumed by the dual step (overwritten with
-// x_new); [1-q] then receives 2 x_new - x.
-__global__ void __launch_bounds__(kTgvBX* kTgvBY, 6) k_tgv_primal(Box b, TgvArrays A, TgvScalars c, TgvConst K, int q,
-                                                               int zchunk, const TgvFlag* flag) {
+// x_new); [1-q] then receives 2 x_new - x.  Restrict-qualified pointers and the next
+// plane's masks fetched ahead, as in k_tgv_dual.
+__global__ void __launch_bounds__(kTgvBX* kTgvBY, kTgvPrimalBlocks) k_tgv_primal(Box b, TgvArrays A, TgvScalars c,
+                                                                              TgvConst K, int q, int zchunk,
+                                                                              const TgvFlag* flag) {
   if (flag->done) return;
   const long long sxy = (long long)b.bx * b.by;
+  const uint8_t* __restrict__ m0 = A.m0;
+  const uint8_t* __restrict__ me = A.me;
+  const float* __restrict__ etab = A.eta;
+  const float* __restrict__ p0 = A.p[0];
+  const float* __restrict__ p1 = A.p[1];
+  const float* __restrict__ p2 = A.p[2];
+  const float* __restrict__ qb[6] = {A.q[0], A.q[1], A.q[2], A.q[3], A.q[4], A.q[5]};
+  const float* __restrict__ phr = A.phi[1 - q];
+  float* __restrict__ phw = A.phi[q];
+  float* __restrict__ phx = A.phi[1 - q];
+  const float* __restrict__ chr = A.chi[1 - q];
+  float* __restrict__ chw = A.chi[q];
+  float* __restrict__ chx = A.chi[1 - q];
   // eta and q are only ever updated inside mask0 (k_tgv_dual) and start at zero, so
   // m0*eta = eta and m0*q = q
-  auto eta_m = [&](long long t) { return A.eta[t]; };
-  auto mq = [&](int comp, long long t) { return A.q[comp][t]; };
+  auto eta_m = [&](long long t) { return etab[t]; };
+  auto mq = [&](int comp, long long t) { return qb[comp][t]; };
   const int i = blockIdx.x * kTgvBX + threadIdx.x, j = blockIdx.y * kTgvBY + threadIdx.y;
   if (i >= b.bx || j >= b.by) return;
+  const int kbeg = blockIdx.z * zchunk;
   const int kend = min(b.bz, (int)(blockIdx.z + 1) * zchunk);
-  for (int k = blockIdx.z * zchunk; k < kend; ++k) {
-    const long long s = (long long)k * sxy + (long long)j * b.bx + i;
-    const bool in0 = A.m0[s] != 0, inm = A.me[s] != 0;
+  if (kbeg >= kend) return;
+  long long s = (long long)kbeg * sxy + (long long)j * b.bx + i;
+  uint8_t nm0 = m0[s], nme = me[s];
+  for (int k = kbeg; k < kend; ++k, s += sxy) {
+    const bool in0 = nm0 != 0, inm = nme != 0;
+    if (k + 1 < kend) {
+      nm0 = m0[s + sxy];
+      nme = me[s + sxy];
+    }
     // phi
     const float lap = in0 ? lap_neumann(eta_m, s, i, j, k, b, sxy, c) : 0.0f;
-    const float phi_old = A.phi[1 - q][s];
+    const float phi_old = phr[s];
     const float phi_new = (phi_old + c.tau * lap) / (1.0f + (inm ? c.tau : 0.0f));
     // chi: bdiv_masked (src/utils/gradient.rs:497-565) minus the stencil of m0*eta
     float t1 = 0.0f;
     if (in0) {
-      const float gxt = 1.0f * A.p[0][s] * c.hx - (i > 0 ? (A.m0[s - 1] ? 1.0f : 0.0f) * A.p[0][s - 1] * c.hx : 0.0f);
-      const float gyt =
-          1.0f * A.p[1][s] * c.hy - (j > 0 ? (A.m0[s - b.bx] ? 1.0f : 0.0f) * A.p[1][s - b.bx] * c.hy : 0.0f);
-      const float gzt = 1.0f * A.p[2][s] * c.hz - (k > 0 ? (A.m0[s - sxy] ? 1.0f : 0.0f) * A.p[2][s - sxy] * c.hz : 0.0f);
+      const float gxt = 1.0f * p0[s] * c.hx - (i > 0 ? (m0[s - 1] ? 1.0f : 0.0f) * p0[s - 1] * c.hx : 0.0f);
+      const float gyt = 1.0f * p1[s] * c.hy - (j > 0 ? (m0[s - b.bx] ? 1.0f : 0.0f) * p1[s - b.bx] * c.hy : 0.0f);
+      const float gzt = 1.0f * p2[s] * c.hz - (k > 0 ? (m0[s - sxy] ? 1.0f : 0.0f) * p2[s - sxy] * c.hz : 0.0f);
       t1 = gxt + gyt + gzt;
     }
     const float t2 = (in0 && interior(i, j, k, b)) ? stencil27(eta_m, s, b.bx, sxy, K) : 0.0f;
-    const float chi_old = A.chi[1 - q][s];
+    const float chi_old = chr[s];
     const float chi_new = chi_old + c.tstep * (t1 - t2);
     // w: symdiv of m0*q (src/utils/gradient.rs:380-432), zero on the near faces
-    float wn[3];
+    float wn[3], wo[3];
 #pragma unroll
-    for (int comp = 0; comp < 3; ++comp) wn[comp] = A.w[1 - q][comp][s];
+    for (int comp = 0; comp < 3; ++comp) wo[comp] = wn[comp] = A.w[1 - q][comp][s];
     if (inm) {
       auto bw = [&](int cq, int axis) {
         if (axis == 0) return i > 0 ? mq(cq, s - 1) : 0.0f;
         if (axis == 1) return j > 0 ? mq(cq, s - b.bx) : 0.0f;
         return k > 0 ? mq(cq, s - sxy) : 0.0f;
       };
-      const float q0 = mq(0, s), q1 = mq(1, s), q2 = mq(2, s), q3 = mq(3, s), q4 = mq(4, s), q5 = mq(5, s);
-      const float dqx = (q0 - bw(0, 0)) * c.hx + (q1 - bw(1, 1)) * c.hy + (q2 - bw(2, 2)) * c.hz;
-      const float dqy = (q1 - bw(1, 0)) * c.hx + (q3 - bw(3, 1)) * c.hy + (q4 - bw(4, 2)) * c.hz;
-      const float dqz = (q2 - bw(2, 0)) * c.hx + (q4 - bw(4, 1)) * c.hy + (q5 - bw(5, 2)) * c.hz;
-      wn[0] += c.tstep * (A.p[0][s] + dqx);
-      wn[1] += c.tstep * (A.p[1][s] + dqy);
-      wn[2] += c.tstep * (A.p[2][s] + dqz);
+      const float qa = mq(0, s), qb1 = mq(1, s), qc = mq(2, s), qd = mq(3, s), qe = mq(4, s), qf = mq(5, s);
+      const float dqx = (qa - bw(0, 0)) * c.hx + (qb1 - bw(1, 1)) * c.hy + (qc - bw(2, 2)) * c.hz;
+      const float dqy = (qb1 - bw(1, 0)) * c.hx + (qd - bw(3, 1)) * c.hy + (qe - bw(4, 2)) * c.hz;
+      const float dqz = (qc - bw(2, 0)) * c.hx + (qe - bw(4, 1)) * c.hy + (qf - bw(5, 2)) * c.hz;
+      wn[0] += c.tstep * (p0[s] + dqx);
+      wn[1] += c.tstep * (p1[s] + dqy);
+      wn[2] += c.tstep * (p2[s] + dqz);
     }
-    A.phi[q][s] = phi_new;
-    A.phi[1 - q][s] = 2.0f * phi_new - phi_old;
-    A.chi[q][s] = chi_new;
-    A.chi[1 - q][s] = 2.0f * chi_new - chi_old;
+    phw[s] = phi_new;
+    phx[s] = 2.0f * phi_new - phi_old;
+    chw[s] = chi_new;
+    chx[s] = 2.0f * chi_new - chi_old;
 #pragma unroll
     for (int comp = 0; comp < 3; ++comp) {
-      const float wo = A.w[1 - q][comp][s];
       A.w[q][comp][s] = wn[comp];
-      A.w[1 - q][comp][s] = 2.0f * wn[comp] - wo;
+      A.w[1 - q][comp][s] = 2.0f * wn[comp] - wo[comp];
     }
   }
 }
