@@ -192,13 +192,14 @@ template <typename T> struct MidId {
 };
 
 // X pass over full complex rows: load -> FFT(D1) -> mid -> FFT(D2) -> store.
-// W: a hot loop's pass; with both transforms in float it takes the compile-time kernel
-// (k_x_full_fx) for the lengths of QSM_FIXED_PLANS.
+// W: a hot loop's pass; with both transforms it takes the compile-time kernel
+// (k_x_full_fx) for the lengths of QSM_FIXED_PLANS (FP64 384: 96 registers against the
+// runtime engine's 130, two blocks per SM instead of one).
 template <typename T, int D1, int D2, bool W = false, class Load, class Mid, class Store>
 void run_x_full(qsm_ctx* ctx, const Fft3<T>& f, const Load& ld, const Mid& mid, const Store& st, const int* done,
                 const char* name) {
   using C = cplx_t<T>;
-  if constexpr (W && D1 != 0 && D2 != 0 && std::is_same<T, float>::value) {
+  if constexpr (W && D1 != 0 && D2 != 0) {
     if (compiled_plans(ctx)) {
 #define QSM_TRY_XF(N_, T_, R0_, R1_, R2_)                                                          \
     if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(f.px)) {                                         \
@@ -308,10 +309,9 @@ template <typename T, class K> int yz_tile_width(K kernel, int n, int Tn) {
   throw QsmError(QSM_ERR_UNSUPPORTED_SIZE, "axis of length " + std::to_string(n) + " does not fit one tile");
 }
 
-// Compile-time Y/Z kernels (float, 16-column tiles) for the axis lengths of
-// QSM_FIXED_PLANS (and QSM_FIXED_PLANS_WIDE when W); returns false when the plan is not
-// one of them.
-constexpr int kFxCols = 16;
+// Columns per tile of the compile-time Y/Z passes: 128-byte tile rows (16 float or 8
+// double complex values).
+template <typename T> constexpr int fx_cols() { return sizeof(T) == 4 ? 16 : 8; }
 constexpr int kZmCols = 8;  // columns per tile of the fused Z pass
 
 // ----------------------------------------------------------------- autotuner --
@@ -386,32 +386,33 @@ template <typename T, int DIR, int AXIS, class FP>
 bool launch_yz_fx(qsm_ctx* ctx, const Fft3<T>& f, int shape, const cplx_t<T>* src, cplx_t<T>* dst,
                   const int* done, bool scoped) {
   const cplx_t<T>* tw = (AXIS == 1) ? f.twy : f.twz;
-  auto kern = k_pass_yz_dx<T, DIR, FP, kFxCols>;
-  const size_t smem = dx_smem<T>(FP::n, kFxCols);
-  const TileWalk w = tile_walk(f, AXIS, kFxCols, (shape & kTuneEdge) != 0);
+  auto kern = k_pass_yz_dx<T, DIR, FP, fx_cols<T>()>;
+  const size_t smem = dx_smem<T>(FP::n, fx_cols<T>());
+  const TileWalk w = tile_walk(f, AXIS, fx_cols<T>(), (shape & kTuneEdge) != 0);
   unsigned grid = 0;
-  if (!fx_launch_ok(ctx, kern, kFxCols * FP::T, smem, &grid, w.ntiles, (shape & kTuneBlockPerTile) != 0,
+  if (!fx_launch_ok(ctx, kern, fx_cols<T>() * FP::T, smem, &grid, w.ntiles, (shape & kTuneBlockPerTile) != 0,
                     tune_bpsm(shape)))
     return false;
   if (!scoped) {
-    kern<<<grid, dim3(kFxCols, FP::T), smem, ctx->stream>>>(f.g, w, tw, src, dst, done);
+    kern<<<grid, dim3(fx_cols<T>(), FP::T), smem, ctx->stream>>>(f.g, w, tw, src, dst, done);
     return true;
   }
   LaunchScope ls(ctx, AXIS == 1 ? (DIR < 0 ? "fft_y_fwd" : "fft_y_inv") : (DIR < 0 ? "fft_z_fwd" : "fft_z_inv"));
-  kern<<<grid, dim3(kFxCols, FP::T), smem, ctx->stream>>>(f.g, w, tw, src, dst, done);
+  kern<<<grid, dim3(fx_cols<T>(), FP::T), smem, ctx->stream>>>(f.g, w, tw, src, dst, done);
   ls.done();
   return true;
 }
 
+// Compile-time Y/Z kernels (fx_cols<T>() columns per tile) for the axis lengths of
+// QSM_FIXED_PLANS (and QSM_FIXED_PLANS_WIDE when W); returns false when the plan is not
+// one of them.
 template <typename T, int DIR, int AXIS, bool W>
 bool run_yz_fixed(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst, const int* done) {
   if (!compiled_plans(ctx)) return false;
-  if constexpr (!std::is_same<T, float>::value) {
-    return false;
-  } else {
+  {
     const FftPlan1D& pl = (AXIS == 1) ? f.py : f.pz;
 #define QSM_TRY_YZ(N_, T_, R0_, R1_, R2_)                                                         \
-    if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(pl) && kFxCols * T_ <= 1024) {                   \
+    if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(pl) && fx_cols<T>() * T_ <= 1024) {                   \
       using FP = FixedPlan<N_, T_, R0_, R1_, R2_>;                                                \
       const int shape = tuned_shape(ctx, yz_tune_key<T>("yz_fx", f, AXIS, DIR));                  \
       return launch_yz_fx<T, DIR, AXIS, FP>(ctx, f, shape, src, dst, done, true);                 \
@@ -427,28 +428,26 @@ bool run_yz_fixed(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T
 
 constexpr int kMaxPersistentBlocks = 4096;
 
-// Compile-time Y/Z pass that carries an operator (k_pass_yz_dx_op), float, lengths of
+// Compile-time Y/Z pass that carries an operator (k_pass_yz_dx_op), lengths of
 // QSM_FIXED_PLANS; ACC as in run_yz_acc.  Returns false when the plan is not one of them.
 template <typename T, int DIR, int AXIS, bool ACC, class Op>
 bool run_yz_op_fixed(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T>* dst, const Op& op,
                      double* partials, unsigned* counter, const int* done, const char* name) {
   if (!compiled_plans(ctx)) return false;
-  if constexpr (!std::is_same<T, float>::value) {
-    return false;
-  } else {
+  {
     const FftPlan1D& pl = (AXIS == 1) ? f.py : f.pz;
     const cplx_t<T>* tw = (AXIS == 1) ? f.twy : f.twz;
 #define QSM_TRY_YZO(N_, T_, R0_, R1_, R2_)                                                         \
-    if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(pl) && kFxCols * T_ <= 1024) {                   \
+    if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(pl) && fx_cols<T>() * T_ <= 1024) {                   \
       using FP = FixedPlan<N_, T_, R0_, R1_, R2_>;                                                \
-      auto kern = k_pass_yz_dx_op<T, DIR, AXIS, FP, kFxCols, Op, ACC>;                            \
-      const size_t smem = dx_smem<T>(N_, kFxCols);                                                \
-      const TileWalk w = tile_walk(f, AXIS, kFxCols);                                             \
+      auto kern = k_pass_yz_dx_op<T, DIR, AXIS, FP, fx_cols<T>(), Op, ACC>;                            \
+      const size_t smem = dx_smem<T>(N_, fx_cols<T>());                                                \
+      const TileWalk w = tile_walk(f, AXIS, fx_cols<T>());                                             \
       unsigned grid = 0;                                                                          \
-      if (!fx_launch_ok(ctx, kern, kFxCols * T_, smem, &grid, w.ntiles)) return false;            \
+      if (!fx_launch_ok(ctx, kern, fx_cols<T>() * T_, smem, &grid, w.ntiles)) return false;            \
       if (ACC && grid > (unsigned)kMaxPersistentBlocks) return false;                             \
       LaunchScope ls(ctx, name);                                                                  \
-      kern<<<grid, dim3(kFxCols, T_), smem, ctx->stream>>>(f.g, w, tw, src, dst, op, partials, counter, done); \
+      kern<<<grid, dim3(fx_cols<T>(), T_), smem, ctx->stream>>>(f.g, w, tw, src, dst, op, partials, counter, done); \
       ls.done();                                                                                  \
       return true;                                                                                \
     }
@@ -553,18 +552,18 @@ bool launch_zm_fx(qsm_ctx* ctx, const Fft3<T>& f, int shape, const cplx_t<T>* sr
 // off or the stream is capturing.
 template <typename T, int DIR, int AXIS, bool W>
 void tune_yz_fixed(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* scratch) {
-  if constexpr (std::is_same<T, float>::value) {
+  {
     if (!compiled_plans(ctx)) return;
     const std::string key = yz_tune_key<T>("yz_fx", f, AXIS, DIR);
     if (!autotune_due(ctx, key)) return;
     const FftPlan1D& pl = (AXIS == 1) ? f.py : f.pz;
 #define QSM_TUNE_YZ(N_, T_, R0_, R1_, R2_)                                                        \
-    if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(pl) && kFxCols * T_ <= 1024) {                   \
+    if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(pl) && fx_cols<T>() * T_ <= 1024) {                   \
       using FP = FixedPlan<N_, T_, R0_, R1_, R2_>;                                                \
-      auto kern = k_pass_yz_dx<T, DIR, FP, kFxCols>;                                              \
-      const size_t smem = dx_smem<T>(FP::n, kFxCols);                                             \
+      auto kern = k_pass_yz_dx<T, DIR, FP, fx_cols<T>()>;                                              \
+      const size_t smem = dx_smem<T>(FP::n, fx_cols<T>());                                             \
       ensure_smem(kern, smem);                                                                    \
-      const auto cands = yz_candidates(f, kFxCols, kern, kFxCols * FP::T, smem);                  \
+      const auto cands = yz_candidates(f, fx_cols<T>(), kern, fx_cols<T>() * FP::T, smem);                  \
       autotune_pick(ctx, key, cands, [&](int c) {                                                 \
         launch_yz_fx<T, DIR, AXIS, FP>(ctx, f, c, scratch, scratch, nullptr, false);               \
       });                                                                                         \

@@ -677,6 +677,15 @@ __global__ void __maxnreg__(YzRegCap<T>::value)
 // bounds, j mod Ns, twiddle strides and shared-memory addressing fold into constants.
 // Plain copies (k_pass_yz_dx) and the multiplier Z pass (k_z_fused_m_fx).
 // ------------------------------------------------------------------------------
+// Resident blocks per SM the compile-time Y/Z passes are compiled for: three blocks of
+// up to 256 threads in float; in double (twice the registers per value) three blocks of
+// up to 128 threads and two of up to 256, so the long plans (384: 208 threads) do not
+// spill.
+template <typename T, int THREADS> constexpr int yz_dx_min_blocks() {
+  if constexpr (sizeof(T) == 4) return THREADS <= 256 ? 3 : 1;
+  else return THREADS <= 128 ? 3 : (THREADS <= 256 ? 2 : 1);
+}
+
 template <int P> struct SAStridedC {
   __device__ __forceinline__ int operator()(int e) const { return e * P; }
 };
@@ -775,7 +784,7 @@ __global__ void __maxnreg__(ZRegCap<T>::value) k_z_fused_m(Geom g, const __grid_
 // staging: at two blocks per SM the direct loads left its latency exposed.  One tile
 // buffer (the stage exchange) per block; blocks walk tiles with stride gridDim.x.
 template <typename T, int DIR, class FP, int P>
-__global__ void __launch_bounds__(P* FP::T, (P * FP::T <= 256 ? 3 : 1))
+__global__ void __launch_bounds__(P* FP::T, yz_dx_min_blocks<T, P * FP::T>())
     k_pass_yz_dx(Geom g, TileWalk w, const cplx_t<T>* __restrict__ twg, const cplx_t<T>* src, cplx_t<T>* dst,
                  const int* __restrict__ done) {
   using C = cplx_t<T>;
@@ -809,7 +818,7 @@ __global__ void __launch_bounds__(P* FP::T, (P * FP::T <= 256 ? 3 : 1))
 // that sum follows the fixed plan's last stage, so the total is deterministic for a
 // given launch shape.
 template <typename T, int DIR, int AXIS, class FP, int P, class Op, bool ACC>
-__global__ void __launch_bounds__(P* FP::T, (P * FP::T <= 256 ? 3 : 1))
+__global__ void __launch_bounds__(P* FP::T, yz_dx_min_blocks<T, P * FP::T>())
     k_pass_yz_dx_op(Geom g, TileWalk w, const cplx_t<T>* __restrict__ twg, const cplx_t<T>* src, cplx_t<T>* dst,
                     Op op, double* __restrict__ partials, unsigned* counter, const int* __restrict__ done) {
   using C = cplx_t<T>;
