@@ -413,10 +413,10 @@ constexpr int kTgvPrimalBlocks = 6;
 
 // Dual update (tgv.rs:1157-1213).  q selects the buffers holding phi_, chi_, w_.
 // Every array is accessed through a restrict-qualified pointer (no two alias, and no
-// voxel reads what another voxel writes in the same launch), so the compiler issues a
-// plane's loads together instead of ordering them behind the stores of the update; the
-// two masks of the next plane are fetched while the current plane computes, so a plane's
-// data loads wait on no mask load.  The arithmetic is that of the reference, in its order.
+// voxel reads what another voxel writes in the same launch); the two masks of the next
+// plane are fetched while the current plane computes, and every value a plane needs is
+// loaded into registers before its update, so a plane waits on one round of loads.  The
+// arithmetic is that of the reference, in its order.
 __global__ void __launch_bounds__(kTgvBX* kTgvBY) k_tgv_dual(Box b, TgvArrays A, TgvScalars c, TgvConst K, int q,
                                                              int zchunk, const TgvFlag* flag) {
   if (flag->done) return;
@@ -453,20 +453,90 @@ __global__ void __launch_bounds__(kTgvBX* kTgvBY) k_tgv_dual(Box b, TgvArrays A,
       nme = me[s + sxy];
     }
     if (!(in0 || inm)) continue;
-    const float cb = chb[s];
+    // Every load of the plane first, into registers, then the update in the reference's
+    // order.  Neighbour offsets are clamped to the box, which gives exactly the values the
+    // Neumann Laplacian substitutes at its faces (the centre), and loads that the
+    // zero-on-the-far-face differences and the interior-only stencil never use.
+    const long long dxm = i > 0 ? -1 : 0, dxp = i + 1 < b.bx ? 1 : 0;
+    const long long dym = j > 0 ? -(long long)b.bx : 0, dyp = j + 1 < b.by ? (long long)b.bx : 0;
+    const long long dzm = k > 0 ? -sxy : 0, dzp = k + 1 < b.bz ? sxy : 0;
+    const long long ox[3] = {dxm, 0, dxp}, oy[3] = {dym, 0, dyp}, oz[3] = {dzm, 0, dzp};
+    float ch[27];  // chi_ at (i + di - 1, j + dj - 1, k + dk - 1): ch[(dk * 3 + dj) * 3 + di]
+    float ph[7];   // phi_: centre, x-, x+, y-, y+, z-, z+
+    float wc[3], wx[3], wy[3], wz[3];  // w_ at the voxel and its x+1, y+1, z+1 neighbours
+    float lph = 0.0f, et = 0.0f, pc[3], qc[6];
+#pragma unroll
+    for (int dk = 0; dk < 3; ++dk)
+#pragma unroll
+      for (int dj = 0; dj < 3; ++dj)
+#pragma unroll
+        for (int di = 0; di < 3; ++di) ch[(dk * 3 + dj) * 3 + di] = 0.0f;
     if (in0) {
-      const float t1 = lap_neumann([&](long long t) { return phb[t]; }, s, i, j, k, b, sxy, c);
-      const float t2 = interior(i, j, k, b) ? stencil27([&](long long t) { return chb[t]; }, s, b.bx, sxy, K) : 0.0f;
-      eta[s] += c.sigma * (-t1 + t2 - lphi[s]);
+#pragma unroll
+      for (int dk = 0; dk < 3; ++dk)
+#pragma unroll
+        for (int dj = 0; dj < 3; ++dj)
+#pragma unroll
+          for (int di = 0; di < 3; ++di) ch[(dk * 3 + dj) * 3 + di] = chb[s + ox[di] + oy[dj] + oz[dk]];
+      ph[0] = phb[s];
+      ph[1] = phb[s + dxm];
+      ph[2] = phb[s + dxp];
+      ph[3] = phb[s + dym];
+      ph[4] = phb[s + dyp];
+      ph[5] = phb[s + dzm];
+      ph[6] = phb[s + dzp];
+      lph = lphi[s];
+      et = eta[s];
+#pragma unroll
+      for (int t = 0; t < 6; ++t) qc[t] = A.q[t][s];
+      wx[0] = wbx[s + dxp];
+      wx[1] = wby[s + dxp];
+      wx[2] = wbz[s + dxp];
+      wy[0] = wbx[s + dyp];
+      wy[1] = wby[s + dyp];
+      wy[2] = wbz[s + dyp];
+      wz[0] = wbx[s + dzp];
+      wz[1] = wby[s + dzp];
+      wz[2] = wbz[s + dzp];
+    } else {
+      ch[13] = chb[s];
+      ch[14] = chb[s + dxp];
+      ch[16] = chb[s + dyp];
+      ch[22] = chb[s + dzp];
+    }
+    wc[0] = wbx[s];
+    wc[1] = wby[s];
+    wc[2] = wbz[s];
+    pc[0] = p0[s];
+    pc[1] = p1[s];
+    pc[2] = p2[s];
+    const float cb = ch[13];
+    if (in0) {
+      const float a0 = ph[0];
+      const float t1 = c.hx2 * (ph[1] - 2.0f * a0 + ph[2]) + c.hy2 * (ph[3] - 2.0f * a0 + ph[4]) +
+                       c.hz2 * (ph[5] - 2.0f * a0 + ph[6]);
+      float t2 = 0.0f;
+      if (interior(i, j, k, b)) {
+        float sum = 0.0f;
+#pragma unroll
+        for (int dk = 0; dk < 3; ++dk)
+#pragma unroll
+          for (int dj = 0; dj < 3; ++dj)
+#pragma unroll
+            for (int di = 0; di < 3; ++di) sum += K.st[(di * 3 + dj) * 3 + dk] * ch[(dk * 3 + dj) * 3 + di];
+        t2 = sum;
+      }
+      et += c.sigma * (-t1 + t2 - lph);
+      eta[s] = et;
     }
     {
-      const float gx = i + 1 < b.bx ? (chb[s + 1] - cb) * c.hx : 0.0f;
-      const float gy = j + 1 < b.by ? (chb[s + b.bx] - cb) * c.hy : 0.0f;
-      const float gz = k + 1 < b.bz ? (chb[s + sxy] - cb) * c.hz : 0.0f;
+      const float gx = i + 1 < b.bx ? (ch[14] - cb) * c.hx : 0.0f;
+      const float gy = j + 1 < b.by ? (ch[16] - cb) * c.hy : 0.0f;
+      const float gz = k + 1 < b.bz ? (ch[22] - cb) * c.hz : 0.0f;
       const float s0 = in0 ? c.sstep : 0.0f, s1 = inm ? c.sstep : 0.0f;
-      float px = p0[s] + (s0 * gx - s1 * wbx[s]);
-      float py = p1[s] + (s0 * gy - s1 * wby[s]);
-      float pz = p2[s] + (s0 * gz - s1 * wbz[s]);
+      float px = pc[0] + (s0 * gx - s1 * wc[0]);
+      float py = pc[1] + (s0 * gy - s1 * wc[1]);
+      float pz = pc[2] + (s0 * gz - s1 * wc[2]);
       const float nrm = sqrtf(px * px + py * py + pz * pz);
       if (nrm > c.alpha1) {
         const float sc = c.alpha1 / nrm;
@@ -480,25 +550,25 @@ __global__ void __launch_bounds__(kTgvBX* kTgvBY) k_tgv_dual(Box b, TgvArrays A,
     }
     if (in0) {
       // symgrad (src/utils/gradient.rs:300-372), zero on the far faces
-      const float wx0 = wbx[s], wy0 = wby[s], wz0 = wbz[s];
+      const float wx0 = wc[0], wy0 = wc[1], wz0 = wc[2];
       float sxx = 0.0f, sxy_ = 0.0f, sxz = 0.0f, syy = 0.0f, syz = 0.0f, szz = 0.0f;
       if (i + 1 < b.bx) {
-        sxx = (wbx[s + 1] - wx0) * c.hx;
-        sxy_ = ((wby[s + 1] - wy0) * c.hx) * 0.5f;
-        sxz = ((wbz[s + 1] - wz0) * c.hx) * 0.5f;
+        sxx = (wx[0] - wx0) * c.hx;
+        sxy_ = ((wx[1] - wy0) * c.hx) * 0.5f;
+        sxz = ((wx[2] - wz0) * c.hx) * 0.5f;
       }
       if (j + 1 < b.by) {
-        syy = (wby[s + b.bx] - wy0) * c.hy;
-        sxy_ += ((wbx[s + b.bx] - wx0) * c.hy) * 0.5f;
-        syz = ((wbz[s + b.bx] - wz0) * c.hy) * 0.5f;
+        syy = (wy[1] - wy0) * c.hy;
+        sxy_ += ((wy[0] - wx0) * c.hy) * 0.5f;
+        syz = ((wy[2] - wz0) * c.hy) * 0.5f;
       }
       if (k + 1 < b.bz) {
-        szz = (wbz[s + sxy] - wz0) * c.hz;
-        sxz += ((wbx[s + sxy] - wx0) * c.hz) * 0.5f;
-        syz += ((wby[s + sxy] - wy0) * c.hz) * 0.5f;
+        szz = (wz[2] - wz0) * c.hz;
+        sxz += ((wz[0] - wx0) * c.hz) * 0.5f;
+        syz += ((wz[1] - wy0) * c.hz) * 0.5f;
       }
-      float qq[6] = {q0[s] + c.sstep * sxx, q1[s] + c.sstep * sxy_, q2[s] + c.sstep * sxz,
-                     q3[s] + c.sstep * syy, q4[s] + c.sstep * syz, q5[s] + c.sstep * szz};
+      float qq[6] = {qc[0] + c.sstep * sxx, qc[1] + c.sstep * sxy_, qc[2] + c.sstep * sxz,
+                     qc[3] + c.sstep * syy, qc[4] + c.sstep * syz, qc[5] + c.sstep * szz};
       const float fro = sqrtf(qq[0] * qq[0] + qq[3] * qq[3] + qq[5] * qq[5] +
                               2.0f * (qq[1] * qq[1] + qq[2] * qq[2] + qq[4] * qq[4]));
       if (fro > c.alpha0) {
