@@ -878,7 +878,8 @@ def main():
                 "roofline": roofline, "kernels": kernels,
                 "e2e": {"value": round(e2e_value, 4), "unit": UNIT, "h2d_bytes_per_step": int(N * 8 + N),
                         "d2h_bytes_per_step": int(N * 8)},
-                "gpu_launches": int(launches), "clocks": clocks.summary()}
+                "gpu_launches": int(launches), "clocks": clocks.summary(),
+                "autotune": {k: v["choice"] for k, v in ctx.autotune_entries().items()}}
         line.update(extra)
         if cpu is not None:
             line["cpu_baseline"] = cpu
