@@ -143,7 +143,7 @@ void nltv_impl(qsm_ctx* ctx, const GridDims& d, const double* f, const uint8_t* 
       tv_fft(ctx, v, 1);
       first = 2;
     }
-    tv_iterate(ctx, v, first, max_iter, watch, poll);
+    tv_iterate(ctx, v, first, max_iter, watch, poll, tv_poll_launches(progress));
     // the step after the last iteration tests x_max and, when that does not converge,
     // makes the reference's last z/u update (skipped on the device once done)
     tv_step_launch(ctx, v, (int)((max_iter + 1) % 2), 0);

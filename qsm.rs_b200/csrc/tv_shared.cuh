@@ -849,11 +849,14 @@ inline cudaGraphExec_t instantiate(qsm_ctx* ctx, cudaGraph_t graph) {
 
 // Enqueue iterations first..last (1-based, inclusive) of an initialised volume whose
 // TvState has k == first.  Pairs of iterations run as one CUDA graph; when `watch`,
-// poll() (which reads the device state and returns true once done) runs every 16
-// iterations, so that a converged solve stops launching.  Returns poll()'s last answer
+// poll() (which reads the device state and returns true once done) runs every
+// `poll_launches` graph launches (2 * poll_launches iterations), so that a converged
+// solve stops launching and progress reaches the caller.  Returns poll()'s last answer
 // (false when it never ran).
 template <typename T, class Poll>
-bool tv_iterate(qsm_ctx* ctx, const TvVol<T>& v, size_t first, size_t last, bool watch, const Poll& poll) {
+bool tv_iterate(qsm_ctx* ctx, const TvVol<T>& v, size_t first, size_t last, bool watch, const Poll& poll,
+                size_t poll_launches = 8) {
+  if (poll_launches < 1) poll_launches = 1;
   if (last < first) return false;
   const size_t count = last - first + 1;
   bool converged = false;
@@ -861,7 +864,7 @@ bool tv_iterate(qsm_ctx* ctx, const TvVol<T>& v, size_t first, size_t last, bool
     // eager launches (per-kernel timing, or too short to be worth a graph)
     for (size_t it = first; it <= last && !converged; ++it) {
       tv_iter(ctx, v, (int)(it % 2));
-      if (watch && ((it - first + 1) % 16 == 0)) converged = poll();
+      if (watch && ((it - first + 1) % (2 * poll_launches) == 0)) converged = poll();
     }
     return converged;
   }
@@ -882,7 +885,7 @@ bool tv_iterate(qsm_ctx* ctx, const TvVol<T>& v, size_t first, size_t last, bool
   ctx->launches = l0;
   cudaGraphExec_t exec = instantiate(ctx, graph);
   const size_t pairs = count / 2;
-  const size_t chunk = 8;  // graph launches (16 iterations) between host polls when watching
+  const size_t chunk = poll_launches;  // graph launches between host polls when watching
   try {
     size_t launched = 0;
     while (launched < pairs && !converged) {
@@ -903,6 +906,12 @@ bool tv_iterate(qsm_ctx* ctx, const TvVol<T>& v, size_t first, size_t last, bool
   return converged;
 }
 
+// Graph launches between host polls: with a progress callback after every launch (the
+// caller hears of each iteration at most two iterations late), otherwise every 8
+// launches (only the convergence flag is read; launches after convergence return at
+// once on the device).
+inline size_t tv_poll_launches(qsm_progress_fn progress) { return progress != nullptr ? 1 : 8; }
+
 // Iterate an initialised volume (tv_setup or an equivalent) until relative_change < tol
 // or max_iter iterations, write chi, and deliver progress as (iter, max_iter) per
 // iteration plus (iters, iters) on convergence (src/inversion/tv.rs:78-93).  Returns the
@@ -922,7 +931,7 @@ size_t tv_run(qsm_ctx* ctx, const TvVol<T>& v, size_t max_iter, double tol, qsm_
       for (; reported < completed; ++reported) progress(user, reported + 1, max_iter);
     return hs.done != 0;
   };
-  tv_iterate(ctx, v, 1, max_iter, watch, poll);
+  tv_iterate(ctx, v, 1, max_iter, watch, poll, tv_poll_launches(progress));
   bool converged = poll();
   size_t completed = converged ? (size_t)hs.conv_iter : max_iter;
   if (!converged && max_iter >= 1 && tol > 0.0) {

@@ -183,6 +183,29 @@ def test_lsqr_operator_mixed_compile_time_x(ctx32, nx):
     assert rel(got.view(np.float64), rt.view(np.float64)) < 1e-6
 
 
+# every base compile-time length in the X role, with compile-time lengths on y and z too
+XYZ64 = [(64, 96, 128), (96, 128, 160), (128, 160, 176), (160, 176, 192), (176, 192, 256), (192, 256, 64),
+         (256, 64, 96), (384, 96, 64)]
+
+
+@pytest.mark.parametrize("dims", XYZ64, ids=["x".join(map(str, d)) for d in XYZ64])
+def test_lsqr_operator_f64_compile_time_passes(ctx64, dims):
+    """In FP64 the operator's X pass over full rows and its Y and Z passes take the
+    compile-time kernels at the base lengths: against the oracle, and against the runtime
+    engine (same radices, so agreement to FP64 rounding)."""
+    grid = Grid.new(*dims, 1.0, 1.2, 0.9)
+    w, x = _operator_case(grid, sum(dims))
+    want = _oracle_lsqr_operator(grid, OBLIQUE, w, x).view(np.float64)
+    got = _lsqr_operator(ctx64, grid, OBLIQUE, w, x)
+    assert rel(got.view(np.float64), want) < 1e-12, rel(got.view(np.float64), want)
+    ctx64.plan_mode = "runtime"
+    try:
+        rt = _lsqr_operator(ctx64, grid, OBLIQUE, w, x)
+    finally:
+        ctx64.plan_mode = "compiled"
+    assert rel(got.view(np.float64), rt.view(np.float64)) < 1e-13
+
+
 def test_ilsqr_mixed_vs_f64_384x384x256(ctx32, ctx64):
     """Configuration 5's grid: the mixed context (float fastQSM step, FP64 Krylov steps)
     against the FP64 context."""
