@@ -269,6 +269,9 @@ template <typename T> struct OpScaleD {
   using C = cplx_t<T>;
   KSpace K;
   const double* s;
+  // the dipole evaluation runs over a staged tile (k_pass_yz_st_op): inside the first
+  // stage's direct loads it lengthened their latency chain (309 against 256 us in float)
+  static constexpr bool kStagedPre = true;
   __device__ __forceinline__ C pre(C v, int ix, int iy, int iz, long long) const {
     return cscale(cscale(v, (T)*s), (T)dip(K, ix, iy, iz));
   }
@@ -284,6 +287,11 @@ template <typename T> struct OpLsqrOut {
   const C* old;
   LsqrState* st;
   int mode;
+  // the compile-time pass stages `old` through shared memory (k_pass_yz_dx_old)
+  static constexpr bool kReadsOld = true;
+  struct Scalars {
+    double coef, sc;
+  };
   __device__ __forceinline__ C pre(C v, int, int, int, long long) const { return v; }
   __device__ __forceinline__ C post(C v, int ix, int iy, int iz, long long idx, double& acc) const {
     C r = cscale(v, (T)dip(K, ix, iy, iz));
@@ -292,6 +300,21 @@ template <typename T> struct OpLsqrOut {
       const double sc = mode == 0 ? st->su : st->sv;
       const C o = cscale(old[idx], (T)sc);
       r = cadd(r, cscale(o, (T)coef));
+    }
+    acc += (double)r.x * (double)r.x + (double)r.y * (double)r.y;
+    return r;
+  }
+  __device__ __forceinline__ const C* old_src() const { return mode <= 1 ? old : nullptr; }
+  __device__ __forceinline__ Scalars scalars() const {
+    if (mode > 1) return Scalars{0.0, 0.0};
+    return Scalars{mode == 0 ? -st->alpha : -st->beta, mode == 0 ? st->su : st->sv};
+  }
+  // post() with the old value and the scalars already in hand (same arithmetic)
+  __device__ __forceinline__ C post_old(C v, int ix, int iy, int iz, C oldv, const Scalars& s, double& acc) const {
+    C r = cscale(v, (T)dip(K, ix, iy, iz));
+    if (mode <= 1) {
+      const C o = cscale(oldv, (T)s.sc);
+      r = cadd(r, cscale(o, (T)s.coef));
     }
     acc += (double)r.x * (double)r.x + (double)r.y * (double)r.y;
     return r;
@@ -784,10 +807,9 @@ void ilsqr_impl(qsm_ctx* ctx, const GridDims& d, const double* f, const uint8_t*
   run_yz_acc<T, -1, 2, true>(ctx, ff, t, ub, OpLsqrOut<T>{K, nullptr, lst, 2}, partials, counter, nullptr, "fft_z_lsqr");
   // y = A(s*x) written to dst with the given epilogue mode
   auto apply_a = [&](const C* x, const double* s, C* dst, const C* old, int mode) {
-    // (the staged runtime pass: evaluating the dipole scale inside a direct-fetch first
-    // stage ran 309 us against 256 us at 384x384x256 in float, 619 against 450 us in
-    // double)
-    run_yz<T, +1, 2>(ctx, ff, x, t, OpScaleD<T>{K, s}, ldone);
+    // compile-time staged pass (a direct-fetch first stage with the dipole scale in its
+    // loads ran 309 against 256 us at 384x384x256 in float, 619 against 450 us in double)
+    run_yz<T, +1, 2, true>(ctx, ff, x, t, OpScaleD<T>{K, s}, ldone);
     run_yz<T, +1, 1>(ctx, ff, t, t, OpId<T>{}, ldone);
     run_x_full<T, +1, -1, true>(ctx, ff, LoadSpecRow<T>{t, ff.g.pitch}, MidWeightRe<T>{wl, d.nx, invn},
                           StoreSpecRow<T>{t, ff.g.pitch}, ldone, "fft_x_lsqr");

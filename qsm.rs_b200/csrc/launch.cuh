@@ -428,6 +428,42 @@ bool run_yz_fixed(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_t<T
 
 constexpr int kMaxPersistentBlocks = 4096;
 
+// One compile-time operator pass: k_pass_yz_dx_old when the op's epilogue reads a second
+// array (ACC only), k_pass_yz_st_op when its pre hook wants a staged tile, else
+// k_pass_yz_dx_op.  False when the block does not fit.
+template <typename T, int DIR, int AXIS, bool ACC, class FP, class Op>
+bool launch_yz_op_fx(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* tw, const cplx_t<T>* src, cplx_t<T>* dst,
+                     const Op& op, double* partials, unsigned* counter, const int* done, const char* name) {
+  constexpr int P = fx_cols<T>();
+  const TileWalk w = tile_walk(f, AXIS, P);
+  unsigned grid = 0;
+  if constexpr (ACC && ReadsOld<Op>::value) {
+    auto kern = k_pass_yz_dx_old<T, DIR, AXIS, FP, P, Op>;
+    const size_t smem = dx_smem<T>(FP::n, P) + (size_t)FP::n * P * sizeof(cplx_t<T>);
+    if (!fx_launch_ok(ctx, kern, P * FP::T, smem, &grid, w.ntiles)) return false;
+    if (grid > (unsigned)kMaxPersistentBlocks) return false;
+    LaunchScope ls(ctx, name);
+    kern<<<grid, dim3(P, FP::T), smem, ctx->stream>>>(f.g, w, tw, src, dst, op, partials, counter, done);
+    ls.done();
+  } else if constexpr (!ACC && StagedPre<Op>::value) {
+    auto kern = k_pass_yz_st_op<T, DIR, AXIS, FP, P, Op>;
+    const size_t smem = yz_smem<T>(FP::n, P);
+    if (!fx_launch_ok(ctx, kern, P * FP::T, smem, &grid, w.ntiles)) return false;
+    LaunchScope ls(ctx, name);
+    kern<<<grid, dim3(P, FP::T), smem, ctx->stream>>>(f.g, w, tw, src, dst, op, done);
+    ls.done();
+  } else {
+    auto kern = k_pass_yz_dx_op<T, DIR, AXIS, FP, P, Op, ACC>;
+    const size_t smem = dx_smem<T>(FP::n, P);
+    if (!fx_launch_ok(ctx, kern, P * FP::T, smem, &grid, w.ntiles)) return false;
+    if (ACC && grid > (unsigned)kMaxPersistentBlocks) return false;
+    LaunchScope ls(ctx, name);
+    kern<<<grid, dim3(P, FP::T), smem, ctx->stream>>>(f.g, w, tw, src, dst, op, partials, counter, done);
+    ls.done();
+  }
+  return true;
+}
+
 // Compile-time Y/Z pass that carries an operator (k_pass_yz_dx_op), lengths of
 // QSM_FIXED_PLANS; ACC as in run_yz_acc.  Returns false when the plan is not one of them.
 template <typename T, int DIR, int AXIS, bool ACC, class Op>
@@ -438,19 +474,9 @@ bool run_yz_op_fixed(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* src, cplx_
     const FftPlan1D& pl = (AXIS == 1) ? f.py : f.pz;
     const cplx_t<T>* tw = (AXIS == 1) ? f.twy : f.twz;
 #define QSM_TRY_YZO(N_, T_, R0_, R1_, R2_)                                                         \
-    if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(pl) && fx_cols<T>() * T_ <= 1024) {                   \
-      using FP = FixedPlan<N_, T_, R0_, R1_, R2_>;                                                \
-      auto kern = k_pass_yz_dx_op<T, DIR, AXIS, FP, fx_cols<T>(), Op, ACC>;                            \
-      const size_t smem = dx_smem<T>(N_, fx_cols<T>());                                                \
-      const TileWalk w = tile_walk(f, AXIS, fx_cols<T>());                                             \
-      unsigned grid = 0;                                                                          \
-      if (!fx_launch_ok(ctx, kern, fx_cols<T>() * T_, smem, &grid, w.ntiles)) return false;            \
-      if (ACC && grid > (unsigned)kMaxPersistentBlocks) return false;                             \
-      LaunchScope ls(ctx, name);                                                                  \
-      kern<<<grid, dim3(fx_cols<T>(), T_), smem, ctx->stream>>>(f.g, w, tw, src, dst, op, partials, counter, done); \
-      ls.done();                                                                                  \
-      return true;                                                                                \
-    }
+    if (FixedPlan<N_, T_, R0_, R1_, R2_>::matches(pl) && fx_cols<T>() * T_ <= 1024)                \
+      return launch_yz_op_fx<T, DIR, AXIS, ACC, FixedPlan<N_, T_, R0_, R1_, R2_>>(ctx, f, tw, src, dst, op, partials, \
+                                                                                counter, done, name);
     QSM_FIXED_PLANS(QSM_TRY_YZO)
 #undef QSM_TRY_YZO
     return false;

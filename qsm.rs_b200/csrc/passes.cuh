@@ -858,6 +858,129 @@ __global__ void __launch_bounds__(P* FP::T, yz_dx_min_blocks<T, P * FP::T>())
   }
 }
 
+// Ops whose pre hook is costly enough (a k-space evaluation per element) that it should
+// run on a staged tile rather than inside the first stage's loads (kStagedPre).
+template <class Op, class = void> struct StagedPre : std::false_type {};
+template <class Op> struct StagedPre<Op, std::void_t<decltype(Op::kStagedPre)>> : std::bool_constant<Op::kStagedPre> {};
+
+// Compile-time Y/Z operator pass in staged form: the tile is copied into shared memory
+// with cp.async, double-buffered so the next tile's copy overlaps this tile's work, the
+// pre hook runs over the staged tile, and the transform (FP) reads its first stage from
+// shared memory and hands each output to the post hook on its way to global memory.
+template <typename T, int DIR, int AXIS, class FP, int P, class Op>
+__global__ void __launch_bounds__(P* FP::T, yz_dx_min_blocks<T, P * FP::T>())
+    k_pass_yz_st_op(Geom g, TileWalk w, const cplx_t<T>* __restrict__ twg, const cplx_t<T>* src, cplx_t<T>* dst,
+                    Op op, const int* __restrict__ done) {
+  using C = cplx_t<T>;
+  constexpr int n = FP::n;
+  if (done != nullptr && *done) return;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* tw = reinterpret_cast<C*>(smraw);
+  C* buf0 = tw + ((n + 7) & ~7);
+  C* buf1 = buf0 + n * P;
+  const int tid = threadIdx.x + threadIdx.y * P;
+  for (int i = tid; i < n; i += P * FP::T) tw[i] = twg[i];
+  const int px = threadIdx.x;
+  const int t = threadIdx.y;
+  SAStridedC<P> sa;
+  int tile = blockIdx.x;
+  if (tile < w.ntiles) issue_tile(src, buf0, g, w, tile, n, P);
+  cp_async_commit();
+  for (int it = 0; tile < w.ntiles; tile += gridDim.x, ++it) {
+    C* cur = (it & 1) ? buf1 : buf0;
+    C* nxt = (it & 1) ? buf0 : buf1;
+    const int next = tile + gridDim.x;
+    if (next < w.ntiles) issue_tile(src, nxt, g, w, next, n, P);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    const int tx = tile % w.ntx, outer = tile / w.ntx;
+    const int col = tx * P + px;
+    const bool active = col < g.nxh;
+    const long long base = col + (long long)outer * w.ostride;
+    C* sp = cur + px;
+    if (active) {
+      for (int e = t; e < n; e += FP::T) {
+        const long long idx = base + e * w.estride;
+        sp[sa(e)] = (AXIS == 1) ? op.pre(sp[sa(e)], col, e, outer, idx) : op.pre(sp[sa(e)], col, outer, e, idx);
+      }
+    }
+    __syncthreads();
+    auto fetch = [&](int e) -> C { return sp[sa(e)]; };
+    auto emit = [&](int e, C v) {
+      const long long idx = base + e * w.estride;
+      dst[idx] = (AXIS == 1) ? op.post(v, col, e, outer, idx) : op.post(v, col, outer, e, idx);
+    };
+    // the transform ends with a block barrier, so the buffer may be refilled next
+    FP::template run<DIR>(t, active, sp, sa, tw, fetch, emit);
+  }
+  cp_async_wait<0>();
+}
+
+// Ops whose store epilogue reads a second array at the stored element (kReadsOld): the
+// LSQR update u' = A v - alpha u reads u where it writes u' (the two may be the same
+// buffer).  Inside the transform's last stage such a read sits between two stores that
+// may alias it, so each of a thread's elements waited for its own load in turn.
+template <class Op, class = void> struct ReadsOld : std::false_type {};
+template <class Op> struct ReadsOld<Op, std::void_t<decltype(Op::kReadsOld)>> : std::bool_constant<Op::kReadsOld> {};
+
+// k_pass_yz_dx_op (ACC) for ops that read a second array in the epilogue.  The tile of
+// that array (op.old_src(), or none) is staged into shared memory with cp.async when the
+// tile starts, so it arrives while the transform runs; the transform's last stage writes
+// its values back into the tile buffer, and a coalesced epilogue then applies
+// op.post_old(v, .., old, scalars, acc) and stores.  op.scalars() (read once per block)
+// holds the op's scalars, which no block changes before the last one finishes.  The FP64
+// sum runs in the epilogue's element order, fixed for a given launch shape.
+template <typename T, int DIR, int AXIS, class FP, int P, class Op>
+__global__ void __launch_bounds__(P* FP::T, yz_dx_min_blocks<T, P * FP::T>())
+    k_pass_yz_dx_old(Geom g, TileWalk w, const cplx_t<T>* __restrict__ twg, const cplx_t<T>* src, cplx_t<T>* dst,
+                     Op op, double* __restrict__ partials, unsigned* counter, const int* __restrict__ done) {
+  using C = cplx_t<T>;
+  constexpr int n = FP::n;
+  if (done != nullptr && *done) return;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* tw = reinterpret_cast<C*>(smraw);
+  C* buf = tw + ((n + 7) & ~7);
+  C* obuf = buf + n * P;
+  const int tid = threadIdx.x + threadIdx.y * P;
+  for (int i = tid; i < n; i += P * FP::T) tw[i] = twg[i];
+  const int px = threadIdx.x;
+  const int t = threadIdx.y;
+  SAStridedC<P> sa;
+  C* sp = buf + px;
+  const C* osrc = op.old_src();
+  const auto sc = op.scalars();
+  double acc[1] = {0.0};
+  for (int tile = blockIdx.x; tile < w.ntiles; tile += gridDim.x) {
+    const int tx = tile % w.ntx, outer = tile / w.ntx;
+    const int col = tx * P + px;
+    const bool active = col < g.nxh;
+    const long long base = col + (long long)outer * w.ostride;
+    if (osrc != nullptr) issue_tile(osrc, obuf, g, w, tile, n, P);
+    cp_async_commit();
+    auto fetch = [&](int e) -> C {
+      const long long idx = base + e * w.estride;
+      const C v = src[idx];
+      return (AXIS == 1) ? op.pre(v, col, e, outer, idx) : op.pre(v, col, outer, e, idx);
+    };
+    auto emit = [&](int e, C v) { sp[sa(e)] = v; };
+    // the transform ends with a block barrier: the tile buffer holds its results
+    FP::template run<DIR>(t, active, sp, sa, tw, fetch, emit);
+    cp_async_wait<0>();
+    __syncthreads();
+    if (active) {
+      for (int e = t; e < n; e += FP::T) {
+        const long long idx = base + e * w.estride;
+        const C o = osrc != nullptr ? obuf[e * P + px] : mk<C>(T(0), T(0));
+        dst[idx] = (AXIS == 1) ? op.post_old(sp[sa(e)], col, e, outer, o, sc, acc[0])
+                               : op.post_old(sp[sa(e)], col, outer, e, o, sc, acc[0]);
+      }
+    }
+    __syncthreads();  // the next tile's copies and transform overwrite both buffers
+  }
+  if (grid_sum_last<1>(acc, partials, counter) && tid == 0) op.last(acc[0]);
+}
+
 // Compile-time form of k_z_fused_m (FP a FixedPlan, P columns per tile).  Both transforms are inlined,
 // so it is compiled for 512 threads per SM (128 registers): the 768-thread cap spills.  A
 // block whose size is not a multiple of 32 still occupies whole warps, so the block

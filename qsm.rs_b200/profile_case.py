@@ -3,14 +3,17 @@
 
     python qsm.rs_b200/profile_case.py tv --iters 4 [--precision mixed|f64] [--dims NX NY NZ]
     python qsm.rs_b200/profile_case.py tgv --dims 256 256 192 --iters 4
+    python qsm.rs_b200/profile_case.py ilsqr [--precision f64] [--dims NX NY NZ]
 
 tv : TV-ADMM (src/inversion/tv.rs:63-97) on the 256x256x176 ellipsoid brain phantom, or,
      with --dims, on a seeded N(0, 0.01) field with a full mask; a 2-iteration solve
      first tunes the launch shapes, and only the measured solve runs between
      cudaProfilerStart and cudaProfilerStop (ncu --profile-from-start off);
 tgv: TGV (src/inversion/tgv.rs:1045-1299) on an ellipsoid mask (semi-axes 0.42/0.45/0.40
-     of the grid) with uniform wrapped phase in [-3, 3] rad, 0.6 mm voxels, tol 0.
-Both run on cuda:0 and exit; nothing is timed.
+     of the grid) with uniform wrapped phase in [-3, 3] rad, 0.6 mm voxels, tol 0;
+ilsqr: iLSQR (src/inversion/ilsqr.rs:1307-1351) on 384x384x256 (or --dims) at 0.6 mm, the
+     field of 20 seeded ellipsoids inside an ellipsoid mask, default IlsqrParams.
+Each runs on cuda:0 and exits; nothing is timed.
 """
 import argparse
 import os
@@ -77,14 +80,38 @@ def run_tgv(a):
     print(f"tgv ok: {(nx, ny, nz)} x{a.iters}, |chi|max={float(out.abs().max()):.4g}")
 
 
+def run_ilsqr(a):
+    import torch
+    import qsmgpu
+    from qsmgpu import Grid, inversion, phantom
+    nx, ny, nz = a.dims or (384, 384, 256)
+    dev = torch.device("cuda", 0)
+    mask = phantom.ellipsoid_mask((nz, ny, nx), (0.42 * nx, 0.45 * ny, 0.40 * nz))
+    rng = np.random.default_rng(2)
+    chi = np.zeros((nz, ny, nx))
+    phantom.add_ellipsoids(chi, rng, 20, [(0.3 * n, 0.7 * n) for n in (nx, ny, nz)], semi=(3.0, 12.0))
+    chi *= mask
+    grid = Grid.new(nx, ny, nz, 0.6, 0.6, 0.6)
+    m8 = torch.from_numpy(mask.astype(np.uint8).ravel()).to(dev)
+    dchi = torch.from_numpy(chi.ravel()).to(dev)
+    with qsmgpu.Context(0, a.precision) as ctx:
+        f = torch.empty_like(dchi)
+        inversion.dipole_forward_device(ctx, dchi.data_ptr(), grid, (0.0, 0.0, 1.0), f.data_ptr())
+        o = [torch.empty_like(f) for _ in range(4)]
+        inversion.ilsqr_device(ctx, f.data_ptr(), m8.data_ptr(), grid, (0.0, 0.0, 1.0), inversion.IlsqrParams(),
+                               *[t.data_ptr() for t in o])
+    torch.cuda.synchronize()
+    print(f"ilsqr ok: {(nx, ny, nz)}, |chi|max={float(o[0].abs().max()):.4g}")
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["tv", "tgv"])
+    ap.add_argument("case", choices=["tv", "tgv", "ilsqr"])
     ap.add_argument("--iters", type=int, default=4)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "f64"])
     ap.add_argument("--dims", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"))
     a = ap.parse_args()
-    run_tv(a) if a.case == "tv" else run_tgv(a)
+    {"tv": run_tv, "tgv": run_tgv, "ilsqr": run_ilsqr}[a.case](a)
 
 
 if __name__ == "__main__":
