@@ -409,7 +409,7 @@ __device__ __forceinline__ bool interior(int i, int j, int k, const Box& b) {
 // voxel are the tile's own recent loads (L1) rather than another block's (L2).
 constexpr int kTgvBX = 32, kTgvBY = 8;
 // Resident blocks per SM the primal kernel is compiled for (its register budget).
-constexpr int kTgvPrimalBlocks = 6;
+constexpr int kTgvPrimalBlocks = 2;
 
 // Dual update (tgv.rs:1157-1213).  q selects the buffers holding phi_, chi_, w_.
 // Every array is accessed through a restrict-qualified pointer (no two alias, and no
@@ -588,8 +588,9 @@ __global__ void __launch_bounds__(kTgvBX* kTgvBY) k_tgv_dual(Box b, TgvArrays A,
 
 // Primal update and extrapolation (tgv.rs:1215-1271).  Buffers [1-q] hold the current
 // iterate x (read), [q] the extrapolation consumed by the dual step (overwritten with
-// x_new); [1-q] then receives 2 x_new - x.  Restrict-qualified pointers and the next
-// plane's masks fetched ahead, as in k_tgv_dual.
+// x_new); [1-q] then receives 2 x_new - x.  Restrict-qualified pointers, the next
+// plane's masks fetched ahead and the plane's values loaded before the update, as in
+// k_tgv_dual.
 __global__ void __launch_bounds__(kTgvBX* kTgvBY, kTgvPrimalBlocks) k_tgv_primal(Box b, TgvArrays A, TgvScalars c,
                                                                               TgvConst K, int q, int zchunk,
                                                                               const TgvFlag* flag) {
@@ -610,7 +611,6 @@ __global__ void __launch_bounds__(kTgvBX* kTgvBY, kTgvPrimalBlocks) k_tgv_primal
   float* __restrict__ chx = A.chi[1 - q];
   // eta and q are only ever updated inside mask0 (k_tgv_dual) and start at zero, so
   // m0*eta = eta and m0*q = q
-  auto eta_m = [&](long long t) { return etab[t]; };
   auto mq = [&](int comp, long long t) { return qb[comp][t]; };
   const int i = blockIdx.x * kTgvBX + threadIdx.x, j = blockIdx.y * kTgvBY + threadIdx.y;
   if (i >= b.bx || j >= b.by) return;
@@ -625,38 +625,94 @@ __global__ void __launch_bounds__(kTgvBX* kTgvBY, kTgvPrimalBlocks) k_tgv_primal
       nm0 = m0[s + sxy];
       nme = me[s + sxy];
     }
-    // phi
-    const float lap = in0 ? lap_neumann(eta_m, s, i, j, k, b, sxy, c) : 0.0f;
+    // every load of the plane first (clamped neighbour offsets give the values the
+    // Neumann faces substitute), then the update in the reference's order
+    const long long dxm = i > 0 ? -1 : 0, dxp = i + 1 < b.bx ? 1 : 0;
+    const long long dym = j > 0 ? -(long long)b.bx : 0, dyp = j + 1 < b.by ? (long long)b.bx : 0;
+    const long long dzm = k > 0 ? -sxy : 0, dzp = k + 1 < b.bz ? sxy : 0;
+    const long long ox[3] = {dxm, 0, dxp}, oy[3] = {dym, 0, dyp}, oz[3] = {dzm, 0, dzp};
+    float e27[27];  // eta at (i + di - 1, j + dj - 1, k + dk - 1): e27[(dk * 3 + dj) * 3 + di]
+    float pc[3] = {0.0f, 0.0f, 0.0f}, pm[3] = {0.0f, 0.0f, 0.0f};  // p at the voxel; p_a at the voxel - e_a
+    float mm[3] = {0.0f, 0.0f, 0.0f};  // mask0 at the voxel - e_a (1 or 0)
+    float qc[6], qx[3], qy[3], qz[3];  // q at the voxel; (q0,q1,q2)(x-1), (q1,q3,q4)(y-1), (q2,q4,q5)(z-1)
+#pragma unroll
+    for (int t = 0; t < 27; ++t) e27[t] = 0.0f;
+    if (in0) {
+#pragma unroll
+      for (int dk = 0; dk < 3; ++dk)
+#pragma unroll
+        for (int dj = 0; dj < 3; ++dj)
+#pragma unroll
+          for (int di = 0; di < 3; ++di) e27[(dk * 3 + dj) * 3 + di] = etab[s + ox[di] + oy[dj] + oz[dk]];
+      pm[0] = p0[s + dxm];
+      pm[1] = p1[s + dym];
+      pm[2] = p2[s + dzm];
+      mm[0] = m0[s + dxm] ? 1.0f : 0.0f;
+      mm[1] = m0[s + dym] ? 1.0f : 0.0f;
+      mm[2] = m0[s + dzm] ? 1.0f : 0.0f;
+    }
+    if (in0 || inm) {
+      pc[0] = p0[s];
+      pc[1] = p1[s];
+      pc[2] = p2[s];
+    }
+    if (inm) {
+#pragma unroll
+      for (int t = 0; t < 6; ++t) qc[t] = mq(t, s);
+      qx[0] = mq(0, s + dxm);
+      qx[1] = mq(1, s + dxm);
+      qx[2] = mq(2, s + dxm);
+      qy[0] = mq(1, s + dym);
+      qy[1] = mq(3, s + dym);
+      qy[2] = mq(4, s + dym);
+      qz[0] = mq(2, s + dzm);
+      qz[1] = mq(4, s + dzm);
+      qz[2] = mq(5, s + dzm);
+    }
     const float phi_old = phr[s];
+    const float chi_old = chr[s];
+    float wn[3], wo[3];
+#pragma unroll
+    for (int comp = 0; comp < 3; ++comp) wo[comp] = wn[comp] = A.w[1 - q][comp][s];
+    // phi
+    float lap = 0.0f;
+    if (in0) {
+      const float a0 = e27[13];
+      lap = c.hx2 * (e27[12] - 2.0f * a0 + e27[14]) + c.hy2 * (e27[10] - 2.0f * a0 + e27[16]) +
+            c.hz2 * (e27[4] - 2.0f * a0 + e27[22]);
+    }
     const float phi_new = (phi_old + c.tau * lap) / (1.0f + (inm ? c.tau : 0.0f));
     // chi: bdiv_masked (src/utils/gradient.rs:497-565) minus the stencil of m0*eta
     float t1 = 0.0f;
     if (in0) {
-      const float gxt = 1.0f * p0[s] * c.hx - (i > 0 ? (m0[s - 1] ? 1.0f : 0.0f) * p0[s - 1] * c.hx : 0.0f);
-      const float gyt = 1.0f * p1[s] * c.hy - (j > 0 ? (m0[s - b.bx] ? 1.0f : 0.0f) * p1[s - b.bx] * c.hy : 0.0f);
-      const float gzt = 1.0f * p2[s] * c.hz - (k > 0 ? (m0[s - sxy] ? 1.0f : 0.0f) * p2[s - sxy] * c.hz : 0.0f);
+      const float gxt = 1.0f * pc[0] * c.hx - (i > 0 ? mm[0] * pm[0] * c.hx : 0.0f);
+      const float gyt = 1.0f * pc[1] * c.hy - (j > 0 ? mm[1] * pm[1] * c.hy : 0.0f);
+      const float gzt = 1.0f * pc[2] * c.hz - (k > 0 ? mm[2] * pm[2] * c.hz : 0.0f);
       t1 = gxt + gyt + gzt;
     }
-    const float t2 = (in0 && interior(i, j, k, b)) ? stencil27(eta_m, s, b.bx, sxy, K) : 0.0f;
-    const float chi_old = chr[s];
+    float t2 = 0.0f;
+    if (in0 && interior(i, j, k, b)) {
+      float sum = 0.0f;
+#pragma unroll
+      for (int dk = 0; dk < 3; ++dk)
+#pragma unroll
+        for (int dj = 0; dj < 3; ++dj)
+#pragma unroll
+          for (int di = 0; di < 3; ++di) sum += K.st[(di * 3 + dj) * 3 + dk] * e27[(dk * 3 + dj) * 3 + di];
+      t2 = sum;
+    }
     const float chi_new = chi_old + c.tstep * (t1 - t2);
     // w: symdiv of m0*q (src/utils/gradient.rs:380-432), zero on the near faces
-    float wn[3], wo[3];
-#pragma unroll
-    for (int comp = 0; comp < 3; ++comp) wo[comp] = wn[comp] = A.w[1 - q][comp][s];
     if (inm) {
-      auto bw = [&](int cq, int axis) {
-        if (axis == 0) return i > 0 ? mq(cq, s - 1) : 0.0f;
-        if (axis == 1) return j > 0 ? mq(cq, s - b.bx) : 0.0f;
-        return k > 0 ? mq(cq, s - sxy) : 0.0f;
-      };
-      const float qa = mq(0, s), qb1 = mq(1, s), qc = mq(2, s), qd = mq(3, s), qe = mq(4, s), qf = mq(5, s);
-      const float dqx = (qa - bw(0, 0)) * c.hx + (qb1 - bw(1, 1)) * c.hy + (qc - bw(2, 2)) * c.hz;
-      const float dqy = (qb1 - bw(1, 0)) * c.hx + (qd - bw(3, 1)) * c.hy + (qe - bw(4, 2)) * c.hz;
-      const float dqz = (qc - bw(2, 0)) * c.hx + (qe - bw(4, 1)) * c.hy + (qf - bw(5, 2)) * c.hz;
-      wn[0] += c.tstep * (p0[s] + dqx);
-      wn[1] += c.tstep * (p1[s] + dqy);
-      wn[2] += c.tstep * (p2[s] + dqz);
+      const float bx0 = i > 0 ? qx[0] : 0.0f, bx1 = i > 0 ? qx[1] : 0.0f, bx2 = i > 0 ? qx[2] : 0.0f;
+      const float by1 = j > 0 ? qy[0] : 0.0f, by3 = j > 0 ? qy[1] : 0.0f, by4 = j > 0 ? qy[2] : 0.0f;
+      const float bz2 = k > 0 ? qz[0] : 0.0f, bz4 = k > 0 ? qz[1] : 0.0f, bz5 = k > 0 ? qz[2] : 0.0f;
+      const float dqx = (qc[0] - bx0) * c.hx + (qc[1] - by1) * c.hy + (qc[2] - bz2) * c.hz;
+      const float dqy = (qc[1] - bx1) * c.hx + (qc[3] - by3) * c.hy + (qc[4] - bz4) * c.hz;
+      const float dqz = (qc[2] - bx2) * c.hx + (qc[4] - by4) * c.hy + (qc[5] - bz5) * c.hz;
+      wn[0] += c.tstep * (pc[0] + dqx);
+      wn[1] += c.tstep * (pc[1] + dqy);
+      wn[2] += c.tstep * (pc[2] + dqz);
     }
     phw[s] = phi_new;
     phx[s] = 2.0f * phi_new - phi_old;
