@@ -79,7 +79,7 @@ bool stream_capturing(qsm_ctx* ctx) {
 }
 
 void autotune_pick(qsm_ctx* ctx, const std::string& key, const std::vector<int>& cands,
-                   const std::function<void(int)>& launch) {
+                   const std::function<void(int)>& launch, int rounds, int reps) {
   if (cands.empty()) return;
   TuneRec rec;
   if (cands.size() == 1) {
@@ -97,16 +97,15 @@ void autotune_pick(qsm_ctx* ctx, const std::string& key, const std::vector<int>&
   try {
     for (int c : cands) launch(c);  // warm-up (raises shared-memory limits, loads the code)
     QSM_CUDA(cudaGetLastError());
-    constexpr int kRounds = 3, kReps = 5;
-    for (int r = 0; r < kRounds; ++r) {
+    for (int r = 0; r < rounds; ++r) {
       for (size_t i = 0; i < cands.size(); ++i) {
         QSM_CUDA(cudaEventRecord(e0, ctx->stream));
-        for (int k = 0; k < kReps; ++k) launch(cands[i]);
+        for (int k = 0; k < reps; ++k) launch(cands[i]);
         QSM_CUDA(cudaEventRecord(e1, ctx->stream));
         QSM_CUDA(cudaEventSynchronize(e1));
         float ms = 0.f;
         QSM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        best[i] = std::min(best[i], 1000.f * ms / kReps);
+        best[i] = std::min(best[i], 1000.f * ms / reps);
       }
     }
   } catch (...) {

@@ -328,9 +328,9 @@ constexpr int kTuneEdge = 1, kTuneBlockPerTile = 2, kTuneBpsmShift = 2;  // kTun
 inline int tune_bpsm(int shape) { return (shape >> kTuneBpsmShift) & 15; }
 bool stream_capturing(qsm_ctx* ctx);
 // Time launch(c) for every candidate c on ctx->stream (after one warm-up launch each,
-// three rounds of five launches; the best round counts) and cache the fastest under key.
+// `rounds` rounds of `reps` launches; the best round counts) and cache the fastest under key.
 void autotune_pick(qsm_ctx* ctx, const std::string& key, const std::vector<int>& cands,
-                   const std::function<void(int)>& launch);
+                   const std::function<void(int)>& launch, int rounds = 3, int reps = 5);
 inline int tuned_shape(const qsm_ctx* ctx, const std::string& key) {
   if (ctx->forced_shape >= 0) return ctx->forced_shape;
   if (!ctx->autotune) return 0;
@@ -573,11 +573,14 @@ bool launch_zm_fx(qsm_ctx* ctx, const Fft3<T>& f, int shape, const cplx_t<T>* sr
 
 // Tune the launch shape of the compile-time Y/Z pass (DIR, AXIS) and of the multiplier
 // Z pass for grid f, running the candidates in place on `scratch` (a half spectrum of f
-// whose contents may be overwritten) and `mscratch` (a real half-spectrum array).  No-op
-// when the lengths have no compile-time pass, the shapes are cached, the autotuner is
-// off or the stream is capturing.
+// whose contents may be overwritten) and `mscratch` (a real half-spectrum array).  With
+// `chain`, each candidate is timed inside that sequence of launches instead (the solver's
+// own chain of passes, which looks the shape up under the same key), so that it is judged
+// where it runs: after the pass that fills the L2-resident spectrum, not back to back
+// with itself.  No-op when the lengths have no compile-time pass, the shapes are cached,
+// the autotuner is off or the stream is capturing.
 template <typename T, int DIR, int AXIS, bool W>
-void tune_yz_fixed(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* scratch) {
+void tune_yz_fixed(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* scratch, const std::function<void()>* chain = nullptr) {
   {
     if (!compiled_plans(ctx)) return;
     const std::string key = yz_tune_key<T>("yz_fx", f, AXIS, DIR);
@@ -590,9 +593,12 @@ void tune_yz_fixed(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* scratch) {
       const size_t smem = dx_smem<T>(FP::n, fx_cols<T>());                                             \
       ensure_smem(kern, smem);                                                                    \
       const auto cands = yz_candidates(f, fx_cols<T>(), kern, fx_cols<T>() * FP::T, smem);                  \
-      autotune_pick(ctx, key, cands, [&](int c) {                                                 \
-        launch_yz_fx<T, DIR, AXIS, FP>(ctx, f, c, scratch, scratch, nullptr, false);               \
-      });                                                                                         \
+      if (chain != nullptr)                                                                       \
+        autotune_pick(ctx, key, cands, [&](int c) { ctx->tuned[key] = TuneRec{c, {}}; (*chain)(); }, 2, 3); \
+      else                                                                                        \
+        autotune_pick(ctx, key, cands, [&](int c) {                                               \
+          launch_yz_fx<T, DIR, AXIS, FP>(ctx, f, c, scratch, scratch, nullptr, false);             \
+        });                                                                                       \
       return;                                                                                     \
     }
     QSM_FIXED_PLANS(QSM_TUNE_YZ)
@@ -604,7 +610,8 @@ void tune_yz_fixed(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* scratch) {
 }
 
 template <typename T, bool W>
-void tune_z_fused_m(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* scratch, T* mscratch) {
+void tune_z_fused_m(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* scratch, T* mscratch,
+                    const std::function<void()>* chain = nullptr) {
   if constexpr (std::is_same<T, float>::value) {
     if (!compiled_plans(ctx)) return;
     const std::string key = yz_tune_key<T>("zm_fx", f, 2, -1);
@@ -617,9 +624,12 @@ void tune_z_fused_m(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* scratch, T* mscra
       const size_t smem = zm_smem<T>(FP::n, FP::n, kZmCols);                                      \
       ensure_smem(kfx, smem);                                                                     \
       const auto cands = yz_candidates(f, kZmCols, kfx, kZmCols * FP::T, smem);                   \
-      autotune_pick(ctx, key, cands, [&](int c) {                                                 \
-        launch_zm_fx<T, FP>(ctx, f, c, scratch, scratch, mscratch, nullptr, false);                \
-      });                                                                                         \
+      if (chain != nullptr)                                                                       \
+        autotune_pick(ctx, key, cands, [&](int c) { ctx->tuned[key] = TuneRec{c, {}}; (*chain)(); }, 2, 3); \
+      else                                                                                        \
+        autotune_pick(ctx, key, cands, [&](int c) {                                               \
+          launch_zm_fx<T, FP>(ctx, f, c, scratch, scratch, mscratch, nullptr, false);              \
+        });                                                                                       \
       return;                                                                                     \
     }
     QSM_FIXED_PLANS(QSM_TUNE_ZM)

@@ -6,8 +6,8 @@
 
 namespace qsm {
 
-template void tv_fft<float>(qsm_ctx*, const TvVol<float>&, int);
-template void tv_fft<double>(qsm_ctx*, const TvVol<double>&, int);
+template void tv_fft<float>(qsm_ctx*, const TvVol<float>&, int, const int*);
+template void tv_fft<double>(qsm_ctx*, const TvVol<double>&, int, const int*);
 template void tv_tune<float>(qsm_ctx*, const TvVol<float>&);
 template void tv_tune<double>(qsm_ctx*, const TvVol<double>&);
 

@@ -808,8 +808,7 @@ template <typename T> void tv_step_launch(qsm_ctx* ctx, const TvVol<T>& v, int q
 
 // y_i = Re IFFT(rho * sym(inv_a) * F(div)) into yb[q], skipped once the state is done
 // (compile-time passes for the wide length list; instantiated once, in tv_fft.cu)
-template <typename T> void tv_fft(qsm_ctx* ctx, const TvVol<T>& v, int q) {
-  const int* done = &v.st->done;
+template <typename T> void tv_fft(qsm_ctx* ctx, const TvVol<T>& v, int q, const int* done) {
   run_x_r2c<T, true>(ctx, v.f, v.spec, LoadCast<T, T>{v.div, v.d.nx}, done);
   run_yz<T, -1, 1, true>(ctx, v.f, v.spec, v.spec, OpId<T>{}, done);
   if (v.use_mult) run_z_fused_m<T, true>(ctx, v.f, v.spec, v.spec, v.mult, done);
@@ -817,13 +816,20 @@ template <typename T> void tv_fft(qsm_ctx* ctx, const TvVol<T>& v, int q) {
   run_yz<T, +1, 1, true>(ctx, v.f, v.spec, v.spec, OpId<T>{}, done);
   run_x_c2r<T, true>(ctx, v.f, v.spec, StoreReal<T>{v.yb[q], v.d.nx, v.scale}, done);
 }
-extern template void tv_fft<float>(qsm_ctx*, const TvVol<float>&, int);
-extern template void tv_fft<double>(qsm_ctx*, const TvVol<double>&, int);
+extern template void tv_fft<float>(qsm_ctx*, const TvVol<float>&, int, const int*);
+extern template void tv_fft<double>(qsm_ctx*, const TvVol<double>&, int, const int*);
+template <typename T> void tv_fft(qsm_ctx* ctx, const TvVol<T>& v, int q) { tv_fft(ctx, v, q, &v.st->done); }
 
+// Each pass's candidates are timed inside the iteration's own chain of FFT passes (X r2c,
+// Y, Z, Y, X c2r on the volume's buffers, which hold no data yet), one pass after the other
+// with the passes already tuned at their choice: timed alone, back to back with itself,
+// a pass favoured shapes that were slower in the chain (one block per tile: 17.0 against
+// 18.6 us alone, 201.4 against 196.4 us per TV-ADMM iteration at 256x256x176).
 template <typename T> void tv_tune(qsm_ctx* ctx, const TvVol<T>& v) {
-  tune_yz_fixed<T, -1, 1, true>(ctx, v.f, v.spec);
-  tune_yz_fixed<T, +1, 1, true>(ctx, v.f, v.spec);
-  if (v.use_mult) tune_z_fused_m<T, true>(ctx, v.f, v.spec, v.mult);
+  const std::function<void()> chain = [&] { tv_fft(ctx, v, 0, nullptr); };
+  tune_yz_fixed<T, -1, 1, true>(ctx, v.f, v.spec, &chain);
+  tune_yz_fixed<T, +1, 1, true>(ctx, v.f, v.spec, &chain);
+  if (v.use_mult) tune_z_fused_m<T, true>(ctx, v.f, v.spec, v.mult, &chain);
 }
 
 template <typename T> void tv_iter(qsm_ctx* ctx, const TvVol<T>& v, int q) {
