@@ -408,8 +408,10 @@ __device__ __forceinline__ bool interior(int i, int j, int k, const Box& b) {
 // `zchunk` planes of one (i, j) column: no index division, and the y/z neighbours of a
 // voxel are the tile's own recent loads (L1) rather than another block's (L2).
 constexpr int kTgvBX = 32, kTgvBY = 8;
-// Resident blocks per SM the primal kernel is compiled for (its register budget).
-constexpr int kTgvPrimalBlocks = 2;
+// Resident blocks per SM the primal and dual kernels are compiled for (their register
+// budgets: 85 registers a thread, no spills; the plane's values are held in registers).
+constexpr int kTgvPrimalBlocks = 3;
+constexpr int kTgvDualBlocks = 3;
 
 // Dual update (tgv.rs:1157-1213).  q selects the buffers holding phi_, chi_, w_.
 // Every array is accessed through a restrict-qualified pointer (no two alias, and no
@@ -417,7 +419,7 @@ constexpr int kTgvPrimalBlocks = 2;
 // plane are fetched while the current plane computes, and every value a plane needs is
 // loaded into registers before its update, so a plane waits on one round of loads.  The
 // arithmetic is that of the reference, in its order.
-__global__ void __launch_bounds__(kTgvBX* kTgvBY) k_tgv_dual(Box b, TgvArrays A, TgvScalars c, TgvConst K, int q,
+__global__ void __launch_bounds__(kTgvBX* kTgvBY, kTgvDualBlocks) k_tgv_dual(Box b, TgvArrays A, TgvScalars c, TgvConst K, int q,
                                                              int zchunk, const TgvFlag* flag) {
   if (flag->done) return;
   const long long sxy = (long long)b.bx * b.by;
