@@ -677,12 +677,14 @@ __global__ void __maxnreg__(YzRegCap<T>::value)
 // bounds, j mod Ns, twiddle strides and shared-memory addressing fold into constants.
 // Plain copies (k_pass_yz_dx) and the multiplier Z pass (k_z_fused_m_fx).
 // ------------------------------------------------------------------------------
-// Resident blocks per SM the compile-time Y/Z passes are compiled for: three blocks of
-// up to 256 threads in float; in double (twice the registers per value) three blocks of
-// up to 128 threads and two of up to 256, so the long plans (384: 208 threads) do not
-// spill.
+// Resident blocks per SM the compile-time Y/Z passes are compiled for: four blocks of
+// up to 256 threads in float (64 registers; no plan of the two lists spills more than 4
+// bytes, and with the five-block multiplier Z pass the TV-ADMM iteration at 256x256x176
+// went from 0.1956 to 0.1941 ms); in double (twice the registers
+// per value) three blocks of up to 128 threads and two of up to 256, so the long plans
+// (384: 208 threads) do not spill.
 template <typename T, int THREADS> constexpr int yz_dx_min_blocks() {
-  if constexpr (sizeof(T) == 4) return THREADS <= 256 ? 3 : 1;
+  if constexpr (sizeof(T) == 4) return THREADS <= 256 ? 4 : 1;
   else return THREADS <= 128 ? 3 : (THREADS <= 256 ? 2 : 1);
 }
 
@@ -982,15 +984,25 @@ __global__ void __launch_bounds__(P* FP::T, yz_dx_min_blocks<T, P * FP::T>())
 }
 
 // Compile-time form of k_z_fused_m (FP a FixedPlan, P columns per tile).  Both transforms are inlined,
-// so it is compiled for 512 threads per SM (128 registers): the 768-thread cap spills.  A
+// so it is compiled for 512 or 640 threads per SM (zm_budget): the 768-thread cap spills.  A
 // block whose size is not a multiple of 32 still occupies whole warps, so the block
 // count per SM is taken on the warp-rounded size.
-template <int THREADS> constexpr int zm_min_blocks() {
+template <int THREADS, int BUDGET = 512> constexpr int zm_min_blocks() {
   constexpr int rounded = (THREADS + 31) / 32 * 32;
-  return rounded <= 512 ? 512 / rounded : 1;
+  return rounded <= BUDGET ? BUDGET / rounded : 1;
+}
+// Threads per SM the multiplier Z pass of length N is compiled for: 640 (five 128-thread
+// blocks, at most 102 registers) where that compiles without spills, as for the 176-point
+// benchmark axis (TV-ADMM 256x256x176: 2 us per iteration less); 512 for the lengths whose
+// plan spilled at 640 (ptxas: 4-92 bytes per thread).
+template <int N> constexpr int zm_budget() {
+  return (N == 75 || N == 125 || N == 128 || N == 135 || N == 150 || N == 180 || N == 216 || N == 224 ||
+          N == 225 || N == 240 || N == 256)
+             ? 512
+             : 640;
 }
 template <typename T, class FP, int P>
-__global__ void __launch_bounds__(P* FP::T, zm_min_blocks<P * FP::T>())
+__global__ void __launch_bounds__(P* FP::T, zm_min_blocks<P * FP::T, zm_budget<FP::n>()>())
     k_z_fused_m_fx(Geom g, TileWalk w, const cplx_t<T>* __restrict__ twg, const cplx_t<T>* src, cplx_t<T>* dst,
                    const T* __restrict__ mult, const int* __restrict__ done) {
   using C = cplx_t<T>;
