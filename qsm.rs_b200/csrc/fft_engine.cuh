@@ -224,6 +224,18 @@ __device__ __forceinline__ void fft_stage(C (&v)[EMAX], const FftPlan1D& pl, int
 // The same Stockham stage with every size known at compile time (radix R, span NS,
 // length N, threads per pencil TT): loop bounds, guards, j mod NS and the twiddle
 // strides fold into constants.  Used for the axis lengths of the benchmark volumes.
+// Fetch tag for a first stage whose inputs are already in the thread's registers, and
+// emit tag for a last stage that leaves its outputs there after applying a hook
+// (hook(e, value) -> value): a plan's last stage leaves thread j holding elements
+// j + r * (N / R_last) in v[c * R + r], the layout the first stage of the plan with the
+// reversed radices reads, so two transforms in a row can pass their values in registers.
+struct FetchInRegs {};
+template <class Hook> struct EmitInRegs {
+  Hook& hook;
+};
+template <class E> struct IsEmitInRegs : std::false_type {};
+template <class H> struct IsEmitInRegs<EmitInRegs<H>> : std::true_type {};
+
 template <int R, int NS, int N, int TT, int DIR, bool FIRST, bool LAST, typename C, class SA, class Fetch,
           class Emit>
 __device__ __forceinline__ void fft_stage_fixed(C (&v)[kFftEmax], int t, bool active, C* sp, const SA& sa,
@@ -231,21 +243,27 @@ __device__ __forceinline__ void fft_stage_fixed(C (&v)[kFftEmax], int t, bool ac
   constexpr int NB = N / R;
   constexpr int CM = (NB + TT - 1) / TT;
   constexpr int TWS = N / (NS * R);
+  constexpr bool kRegsIn = FIRST && std::is_same<Fetch, FetchInRegs>::value;
+  constexpr bool kRegsOut = LAST && IsEmitInRegs<Emit>::value;
   static_assert(CM * R <= kFftEmax, "stage does not fit the register budget");
-  if (active) {
+  if constexpr (!kRegsIn) {
+    if (active) {
 #pragma unroll
-    for (int c = 0; c < CM; ++c) {
-      const int j = t + c * TT;
-      if ((NB % TT == 0) || j < NB) {
+      for (int c = 0; c < CM; ++c) {
+        const int j = t + c * TT;
+        if ((NB % TT == 0) || j < NB) {
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-          if constexpr (FIRST) v[c * R + r] = fetch(j + r * NB);
-          else v[c * R + r] = sp[sa(j + r * NB)];
+          for (int r = 0; r < R; ++r) {
+            if constexpr (FIRST) v[c * R + r] = fetch(j + r * NB);
+            else v[c * R + r] = sp[sa(j + r * NB)];
+          }
         }
       }
     }
+    // With the inputs in registers there is nothing to order here: the stage before
+    // (the other transform's last) read shared memory only ahead of its own barrier.
+    __syncthreads();
   }
-  __syncthreads();
   if (active) {
 #pragma unroll
     for (int c = 0; c < CM; ++c) {
@@ -264,17 +282,29 @@ __device__ __forceinline__ void fft_stage_fixed(C (&v)[kFftEmax], int t, bool ac
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           const int e = base + r * NS;
-          if constexpr (LAST) emit(e, v[c * R + r]);
+          if constexpr (kRegsOut) v[c * R + r] = emit.hook(e, v[c * R + r]);
+          else if constexpr (LAST) emit(e, v[c * R + r]);
           else sp[sa(e)] = v[c * R + r];
         }
       }
     }
   }
-  __syncthreads();
+  // A last stage that keeps its outputs in registers wrote no shared memory.
+  if constexpr (!kRegsOut) __syncthreads();
 }
 
 // A compile-time plan: length N, TT threads per pencil, radices R0, R1[, R2].
-template <int N, int TT, int R0, int R1, int R2 = 1> struct FixedPlan {
+template <int N, int TT, int R0, int R1, int R2 = 1> struct FixedPlan;
+// The plan with its radices in reverse order (see FetchInRegs).
+template <class FP> struct ReversePlan;
+template <int N, int TT, int R0, int R1> struct ReversePlan<FixedPlan<N, TT, R0, R1, 1>> {
+  using type = FixedPlan<N, TT, R1, R0, 1>;
+};
+template <int N, int TT, int R0, int R1, int R2> struct ReversePlan<FixedPlan<N, TT, R0, R1, R2>> {
+  using type = FixedPlan<N, TT, R2, R1, R0>;
+};
+
+template <int N, int TT, int R0, int R1, int R2> struct FixedPlan {
   static constexpr int n = N, T = TT;
   static __host__ __device__ constexpr bool matches(const FftPlan1D& pl) {
     return pl.n == N && pl.m == N && pl.T == TT && pl.radix[0] == R0 && pl.radix[1] == R1 &&
@@ -284,6 +314,12 @@ template <int N, int TT, int R0, int R1, int R2 = 1> struct FixedPlan {
   static __device__ __forceinline__ void run(int t, bool active, C* sp, const SA& sa, const C* tw, Fetch& fetch,
                                              Emit& emit) {
     C v[kFftEmax];
+    run_v<DIR>(v, t, active, sp, sa, tw, fetch, emit);
+  }
+  // The stages over a caller-held register array (FetchInRegs / EmitInRegs).
+  template <int DIR, typename C, class SA, class Fetch, class Emit>
+  static __device__ __forceinline__ void run_v(C (&v)[kFftEmax], int t, bool active, C* sp, const SA& sa,
+                                               const C* tw, Fetch& fetch, Emit& emit) {
     if constexpr (R2 == 1) {
       fft_stage_fixed<R0, 1, N, TT, DIR, true, false>(v, t, active, sp, sa, tw, fetch, emit);
       fft_stage_fixed<R1, R0, N, TT, DIR, false, true>(v, t, active, sp, sa, tw, fetch, emit);

@@ -187,10 +187,11 @@ __global__ void k_x_full(Geom g, const __grid_constant__ FftPlan1D pl, const cpl
 
 // Compile-time form of k_x_full with both transforms (FP a FixedPlan): the first
 // transform's first stage fetches through the loader, its last stage applies the mid
-// hook on the way into shared memory, and the second transform's last stage hands its
-// values straight to the store functor, so a row makes two shared-memory round trips
-// fewer than in k_x_full.  Every element of a row is fetched in the first stage, before
-// any store of that row, so the loader and the store may address the same rows.
+// hook and passes the values in registers to the second transform (the reversed plan),
+// whose last stage hands its values straight to the store functor, so a row makes three
+// shared-memory round trips fewer than in k_x_full.  Every element of a row is fetched
+// in the first stage, before any store of that row, so the loader and the store may
+// address the same rows.
 template <typename T, class FP, int D1, int D2, class Load, class Mid, class Store>
 __global__ void k_x_full_fx(Geom g, const cplx_t<T>* __restrict__ twg, Load ld, Mid mid, Store st0,
                             const int* __restrict__ done) {
@@ -210,13 +211,16 @@ __global__ void k_x_full_fx(Geom g, const cplx_t<T>* __restrict__ twg, Load ld, 
   SAPadded<PadG<T>::G> sa;
   Store st = st0;
   auto fetch_g = [&](int e) -> C { return ld(row, e); };
-  auto emit_mid = [&](int e, C v) { sp[sa(e)] = mid(v, row, e); };
-  auto fetch_s = [&](int e) -> C { return sp[sa(e)]; };
   auto emit_g = [&](int e, C v) { st(row, e, v); };
-  // the first transform's last stage ends with a block barrier, so the second one's
-  // first stage sees every mid-weighted element
-  FP::template run<D1>(t, active, sp, sa, tw, fetch_g, emit_mid);
-  FP::template run<D2>(t, active, sp, sa, tw, fetch_s, emit_g);
+  // The first transform's last stage applies the mid hook in registers and the second
+  // transform, the reversed plan, starts from them (FetchInRegs): no shared-memory round
+  // trip and no barrier between the two.
+  C v[kFftEmax];
+  auto hook = [&](int e, C x) -> C { return mid(x, row, e); };
+  EmitInRegs<decltype(hook)> keep{hook};
+  FetchInRegs in_regs;
+  FP::template run_v<D1>(v, t, active, sp, sa, tw, fetch_g, keep);
+  ReversePlan<FP>::type::template run_v<D2>(v, t, active, sp, sa, tw, in_regs, emit_g);
   st.finish();
 }
 
