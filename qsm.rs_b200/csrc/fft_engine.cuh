@@ -320,11 +320,19 @@ template <int N, int TT, int R0, int R1, int R2> struct FixedPlan {
   template <int DIR, typename C, class SA, class Fetch, class Emit>
   static __device__ __forceinline__ void run_v(C (&v)[kFftEmax], int t, bool active, C* sp, const SA& sa,
                                                const C* tw, Fetch& fetch, Emit& emit) {
+    auto none = [] {};
+    run_v<DIR>(v, t, active, sp, sa, tw, fetch, emit, none);
+  }
+  // ... calling after_first() once the first stage has fetched every input and passed its
+  // barrier, so a pass can release its input while the later stages run.
+  template <int DIR, typename C, class SA, class Fetch, class Emit, class Hook>
+  static __device__ __forceinline__ void run_v(C (&v)[kFftEmax], int t, bool active, C* sp, const SA& sa,
+                                               const C* tw, Fetch& fetch, Emit& emit, Hook& after_first) {
+    fft_stage_fixed<R0, 1, N, TT, DIR, true, false>(v, t, active, sp, sa, tw, fetch, emit);
+    after_first();
     if constexpr (R2 == 1) {
-      fft_stage_fixed<R0, 1, N, TT, DIR, true, false>(v, t, active, sp, sa, tw, fetch, emit);
       fft_stage_fixed<R1, R0, N, TT, DIR, false, true>(v, t, active, sp, sa, tw, fetch, emit);
     } else {
-      fft_stage_fixed<R0, 1, N, TT, DIR, true, false>(v, t, active, sp, sa, tw, fetch, emit);
       fft_stage_fixed<R1, R0, N, TT, DIR, false, false>(v, t, active, sp, sa, tw, fetch, emit);
       fft_stage_fixed<R2, R0 * R1, N, TT, DIR, false, true>(v, t, active, sp, sa, tw, fetch, emit);
     }

@@ -11,6 +11,7 @@ template <typename Tin, typename T> struct LoadCast {
   const Tin* p;
   int nx;
   __device__ __forceinline__ T operator()(int row, int e) const { return (T)p[(long long)row * nx + e]; }
+  __device__ __forceinline__ const Tin* row_begin(int row) const { return p + (long long)row * nx; }
 };
 
 // value where mask != 0, else 0

@@ -91,7 +91,7 @@ template <typename T> inline long long x_blocks(const Fft3<T>& f) {
 
 // Compile-time X kernels (float) for the lengths of QSM_FIXED_PLANS (and of
 // QSM_FIXED_PLANS_WIDE when W); false when the plan is not one of them.
-template <typename T, bool W, class Load>
+template <typename T, bool W, bool DEAD, class Load>
 bool run_x_r2c_fixed(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* spec, const Load& ld, const int* done) {
   if (!compiled_plans(ctx)) return false;
   if constexpr (!std::is_same<T, float>::value && !W) {
@@ -104,7 +104,7 @@ bool run_x_r2c_fixed(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* spec, const Load
       const int Tt = x_block_t(T_);                                                                \
       const int P = x_pencils_per_block<T>(T_);                                                    \
       const size_t smem = (size_t)(N_ + P * x_rowlen<T>(N_)) * sizeof(C);                          \
-      auto kern = k_x_r2c_fx<T, FP, Load>;                                                         \
+      auto kern = k_x_r2c_fx<T, FP, Load, DEAD>;                                                       \
       ensure_smem(kern, smem);                                                                     \
       LaunchScope ls(ctx, "fft_x_r2c");                                                            \
       kern<<<(unsigned)x_blocks(f), dim3(Tt, P), smem, ctx->stream>>>(f.g, f.twx, spec, ld, done); \
@@ -120,7 +120,7 @@ bool run_x_r2c_fixed(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* spec, const Load
   }
 }
 
-template <typename T, bool W, class Store>
+template <typename T, bool W, bool DEAD, class Store>
 bool run_x_c2r_fixed(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* spec, const Store& st, const int* done) {
   if (!compiled_plans(ctx)) return false;
   if constexpr (!std::is_same<T, float>::value && !W) {
@@ -133,7 +133,7 @@ bool run_x_c2r_fixed(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* spec, cons
       const int Tt = x_block_t(T_);                                                                \
       const int P = x_pencils_per_block<T>(T_);                                                    \
       const size_t smem = (size_t)(N_ + P * x_rowlen<T>(N_)) * sizeof(C);                          \
-      auto kern = k_x_c2r_fx<T, FP, Store>;                                                        \
+      auto kern = k_x_c2r_fx<T, FP, Store, DEAD>;                                                      \
       ensure_smem(kern, smem);                                                                     \
       LaunchScope ls(ctx, "fft_x_c2r");                                                            \
       kern<<<(unsigned)x_blocks(f), dim3(Tt, P), smem, ctx->stream>>>(f.g, f.twx, spec, st, done); \
@@ -149,9 +149,11 @@ bool run_x_c2r_fixed(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* spec, cons
   }
 }
 
-template <typename T, bool W = false, class Load>
+// DEAD (compile-time kernels only): the pass reads ld's rows for the last time and drops
+// their L2 lines (k_x_r2c_fx); ld then provides row_begin.
+template <typename T, bool W = false, bool DEAD = false, class Load>
 void run_x_r2c(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* spec, const Load& ld, const int* done) {
-  if (run_x_r2c_fixed<T, W>(ctx, f, spec, ld, done)) return;
+  if (run_x_r2c_fixed<T, W, DEAD>(ctx, f, spec, ld, done)) return;
   using C = cplx_t<T>;
   const int Tt = x_block_t(f.px.T);
   const int P = x_pencils_per_block<T>(f.px.T);
@@ -163,9 +165,11 @@ void run_x_r2c(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* spec, const Load& ld, 
   ls.done();
 }
 
-template <typename T, bool W = false, class Store>
+// DEAD (compile-time kernels only): the pass reads the half spectrum for the last time and
+// drops its L2 lines (k_x_c2r_fx).
+template <typename T, bool W = false, bool DEAD = false, class Store>
 void run_x_c2r(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* spec, const Store& st, const int* done) {
-  if (run_x_c2r_fixed<T, W>(ctx, f, spec, st, done)) return;
+  if (run_x_c2r_fixed<T, W, DEAD>(ctx, f, spec, st, done)) return;
   using C = cplx_t<T>;
   const int Tt = x_block_t(f.px.T);
   const int P = x_pencils_per_block<T>(f.px.T);

@@ -807,14 +807,18 @@ template <typename T> void tv_step_launch(qsm_ctx* ctx, const TvVol<T>& v, int q
 }
 
 // y_i = Re IFFT(rho * sym(inv_a) * F(div)) into yb[q], skipped once the state is done
-// (compile-time passes for the wide length list; instantiated once, in tv_fft.cu)
+// (compile-time passes for the wide length list; instantiated once, in tv_fft.cu).
+// div and the half spectrum are dead once the X passes have read them (the next step
+// writes div and the next X r2c writes the spectrum before either is read again), so
+// those passes drop their L2 lines rather than leave them to be written back to HBM
+// while the stencil streams.
 template <typename T> void tv_fft(qsm_ctx* ctx, const TvVol<T>& v, int q, const int* done) {
-  run_x_r2c<T, true>(ctx, v.f, v.spec, LoadCast<T, T>{v.div, v.d.nx}, done);
+  run_x_r2c<T, true, true>(ctx, v.f, v.spec, LoadCast<T, T>{v.div, v.d.nx}, done);
   run_yz<T, -1, 1, true>(ctx, v.f, v.spec, v.spec, OpId<T>{}, done);
   if (v.use_mult) run_z_fused_m<T, true>(ctx, v.f, v.spec, v.spec, v.mult, done);
   else run_z_fused<T>(ctx, v.f, v.spec, v.spec, v.mul, done);
   run_yz<T, +1, 1, true>(ctx, v.f, v.spec, v.spec, OpId<T>{}, done);
-  run_x_c2r<T, true>(ctx, v.f, v.spec, StoreReal<T>{v.yb[q], v.d.nx, v.scale}, done);
+  run_x_c2r<T, true, true>(ctx, v.f, v.spec, StoreReal<T>{v.yb[q], v.d.nx, v.scale}, done);
 }
 extern template void tv_fft<float>(qsm_ctx*, const TvVol<float>&, int, const int*);
 extern template void tv_fft<double>(qsm_ctx*, const TvVol<double>&, int, const int*);
