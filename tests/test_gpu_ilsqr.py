@@ -192,7 +192,8 @@ XYZ64 = [(64, 96, 128), (96, 128, 160), (128, 160, 176), (160, 176, 192), (176, 
 def test_lsqr_operator_f64_compile_time_passes(ctx64, dims):
     """In FP64 the operator's X pass over full rows and its Y and Z passes take the
     compile-time kernels at the base lengths: against the oracle, and against the runtime
-    engine (same radices, so agreement to FP64 rounding)."""
+    engine (same factorisation; the X kernel's second transform runs the radices in
+    reverse order, so the two agree to FP64 rounding, not bit for bit)."""
     grid = Grid.new(*dims, 1.0, 1.2, 0.9)
     w, x = _operator_case(grid, sum(dims))
     want = _oracle_lsqr_operator(grid, OBLIQUE, w, x).view(np.float64)
