@@ -1078,11 +1078,15 @@ __global__ void __launch_bounds__(P* FP::T, zm_min_blocks<P * FP::T, zm_budget<F
     const long long base = col + (long long)iy * w.ostride;
     C* sp = cur + px;
     auto fetch = [&](int e) -> C { return sp[sa(e)]; };
-    // forward transform back into the tile, scaled by the multiplier on the way out
-    auto emit_m = [&](int e, C v) { sp[sa(e)] = cscale(v, mcur[e * P + px]); };
-    FP::template run<-1>(t, active, sp, sa, tw, fetch, emit_m);
+    // forward transform scaled by the multiplier in registers, handed to the inverse
+    // transform (the reversed plan) without a shared-memory round trip (FetchInRegs)
+    auto scale = [&](int e, C v) -> C { return cscale(v, mcur[e * P + px]); };
+    EmitInRegs<decltype(scale)> keep{scale};
+    FetchInRegs in_regs;
     auto emit = [&](int e, C v) { dst[base + e * w.estride] = v; };
-    FP::template run<+1>(t, active, sp, sa, tw, fetch, emit);
+    C v[kFftEmax];
+    FP::template run_v<-1>(v, t, active, sp, sa, tw, fetch, keep);
+    ReversePlan<FP>::type::template run_v<+1>(v, t, active, sp, sa, tw, in_regs, emit);
   }
   cp_async_wait<0>();
 }
