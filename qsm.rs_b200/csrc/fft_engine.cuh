@@ -236,8 +236,17 @@ template <class Hook> struct EmitInRegs {
 template <class E> struct IsEmitInRegs : std::false_type {};
 template <class H> struct IsEmitInRegs<EmitInRegs<H>> : std::true_type {};
 
-template <int R, int NS, int N, int TT, int DIR, bool FIRST, bool LAST, typename C, class SA, class Fetch,
-          class Emit>
+// Twiddle tables with one gap entry after every 16 (TWP in the compile-time stages).  In
+// the X passes the 16 threads of a row read W^(j*r*s) for 16 consecutive j, a stride that
+// puts power-of-two r on a few shared-memory banks in the dense table (r = 8 at length
+// 256: eight-way conflicts) and on distinct banks in the padded one.
+__host__ __device__ constexpr int tw_pad(int i) { return i + (i >> 4); }
+// Complex entries a padded table of n twiddles occupies (even, so what follows it stays
+// 16-byte aligned).
+__host__ __device__ constexpr int tw_table_len(int n) { return (tw_pad(n - 1) + 2) & ~1; }
+
+template <int R, int NS, int N, int TT, int DIR, bool FIRST, bool LAST, bool TWP, typename C, class SA,
+          class Fetch, class Emit>
 __device__ __forceinline__ void fft_stage_fixed(C (&v)[kFftEmax], int t, bool active, C* sp, const SA& sa,
                                                 const C* tw, Fetch& fetch, Emit& emit) {
   constexpr int NB = N / R;
@@ -273,7 +282,7 @@ __device__ __forceinline__ void fft_stage_fixed(C (&v)[kFftEmax], int t, bool ac
         if constexpr (NS > 1) {
 #pragma unroll
           for (int r = 1; r < R; ++r) {
-            const C w = tw[k * r * TWS];
+            const C w = tw[TWP ? tw_pad(k * r * TWS) : k * r * TWS];
             v[c * R + r] = (DIR < 0) ? cmul(v[c * R + r], w) : cmulc(v[c * R + r], w);
           }
         }
@@ -310,31 +319,32 @@ template <int N, int TT, int R0, int R1, int R2> struct FixedPlan {
     return pl.n == N && pl.m == N && pl.T == TT && pl.radix[0] == R0 && pl.radix[1] == R1 &&
            (R2 == 1 ? pl.nstages == 2 : (pl.nstages == 3 && pl.radix[2] == R2));
   }
-  template <int DIR, typename C, class SA, class Fetch, class Emit>
+  // TWP: tw is a padded table (tw_pad).
+  template <int DIR, bool TWP = false, typename C, class SA, class Fetch, class Emit>
   static __device__ __forceinline__ void run(int t, bool active, C* sp, const SA& sa, const C* tw, Fetch& fetch,
                                              Emit& emit) {
     C v[kFftEmax];
-    run_v<DIR>(v, t, active, sp, sa, tw, fetch, emit);
+    run_v<DIR, TWP>(v, t, active, sp, sa, tw, fetch, emit);
   }
   // The stages over a caller-held register array (FetchInRegs / EmitInRegs).
-  template <int DIR, typename C, class SA, class Fetch, class Emit>
+  template <int DIR, bool TWP = false, typename C, class SA, class Fetch, class Emit>
   static __device__ __forceinline__ void run_v(C (&v)[kFftEmax], int t, bool active, C* sp, const SA& sa,
                                                const C* tw, Fetch& fetch, Emit& emit) {
     auto none = [] {};
-    run_v<DIR>(v, t, active, sp, sa, tw, fetch, emit, none);
+    run_v<DIR, TWP>(v, t, active, sp, sa, tw, fetch, emit, none);
   }
   // ... calling after_first() once the first stage has fetched every input and passed its
   // barrier, so a pass can release its input while the later stages run.
-  template <int DIR, typename C, class SA, class Fetch, class Emit, class Hook>
+  template <int DIR, bool TWP = false, typename C, class SA, class Fetch, class Emit, class Hook>
   static __device__ __forceinline__ void run_v(C (&v)[kFftEmax], int t, bool active, C* sp, const SA& sa,
                                                const C* tw, Fetch& fetch, Emit& emit, Hook& after_first) {
-    fft_stage_fixed<R0, 1, N, TT, DIR, true, false>(v, t, active, sp, sa, tw, fetch, emit);
+    fft_stage_fixed<R0, 1, N, TT, DIR, true, false, TWP>(v, t, active, sp, sa, tw, fetch, emit);
     after_first();
     if constexpr (R2 == 1) {
-      fft_stage_fixed<R1, R0, N, TT, DIR, false, true>(v, t, active, sp, sa, tw, fetch, emit);
+      fft_stage_fixed<R1, R0, N, TT, DIR, false, true, TWP>(v, t, active, sp, sa, tw, fetch, emit);
     } else {
-      fft_stage_fixed<R1, R0, N, TT, DIR, false, false>(v, t, active, sp, sa, tw, fetch, emit);
-      fft_stage_fixed<R2, R0 * R1, N, TT, DIR, false, true>(v, t, active, sp, sa, tw, fetch, emit);
+      fft_stage_fixed<R1, R0, N, TT, DIR, false, false, TWP>(v, t, active, sp, sa, tw, fetch, emit);
+      fft_stage_fixed<R2, R0 * R1, N, TT, DIR, false, true, TWP>(v, t, active, sp, sa, tw, fetch, emit);
     }
   }
 };

@@ -103,8 +103,8 @@ bool run_x_r2c_fixed(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* spec, const Load
       using FP = FixedPlan<N_, T_, R0_, R1_, R2_>;                                                 \
       const int Tt = x_block_t(T_);                                                                \
       const int P = x_pencils_per_block<T>(T_);                                                    \
-      const size_t smem = (size_t)(N_ + P * x_rowlen<T>(N_)) * sizeof(C);                          \
-      auto kern = k_x_r2c_fx<T, FP, Load, DEAD>;                                                       \
+      const size_t smem = (size_t)(x_tw_len<T>(N_) + P * x_rowlen<T>(N_)) * sizeof(C);            \
+      auto kern = k_x_r2c_fx<T, FP, Load, DEAD>;                                                   \
       ensure_smem(kern, smem);                                                                     \
       LaunchScope ls(ctx, "fft_x_r2c");                                                            \
       kern<<<(unsigned)x_blocks(f), dim3(Tt, P), smem, ctx->stream>>>(f.g, f.twx, spec, ld, done); \
@@ -132,8 +132,8 @@ bool run_x_c2r_fixed(qsm_ctx* ctx, const Fft3<T>& f, const cplx_t<T>* spec, cons
       using FP = FixedPlan<N_, T_, R0_, R1_, R2_>;                                                 \
       const int Tt = x_block_t(T_);                                                                \
       const int P = x_pencils_per_block<T>(T_);                                                    \
-      const size_t smem = (size_t)(N_ + P * x_rowlen<T>(N_)) * sizeof(C);                          \
-      auto kern = k_x_c2r_fx<T, FP, Store, DEAD>;                                                      \
+      const size_t smem = (size_t)(x_tw_len<T>(N_) + P * x_rowlen<T>(N_)) * sizeof(C);            \
+      auto kern = k_x_c2r_fx<T, FP, Store, DEAD>;                                                  \
       ensure_smem(kern, smem);                                                                     \
       LaunchScope ls(ctx, "fft_x_c2r");                                                            \
       kern<<<(unsigned)x_blocks(f), dim3(Tt, P), smem, ctx->stream>>>(f.g, f.twx, spec, st, done); \
@@ -210,7 +210,7 @@ void run_x_full(qsm_ctx* ctx, const Fft3<T>& f, const Load& ld, const Mid& mid, 
       using FP = FixedPlan<N_, T_, R0_, R1_, R2_>;                                                 \
       const int Tt = x_block_t(T_);                                                                \
       const int P = x_pencils_per_block<T>(T_);                                                    \
-      const size_t smem = (size_t)(N_ + P * x_rowlen<T>(N_)) * sizeof(C);                          \
+      const size_t smem = (size_t)(x_tw_len<T>(N_) + P * x_rowlen<T>(N_)) * sizeof(C);            \
       auto kern = k_x_full_fx<T, FP, D1, D2, Load, Mid, Store>;                                    \
       ensure_smem(kern, smem);                                                                     \
       const long long blocks = ((long long)f.g.nrows() + P - 1) / P;                              \

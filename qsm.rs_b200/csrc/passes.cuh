@@ -37,6 +37,13 @@ template <> struct PadG<float> { static constexpr int G = 16; };
 template <> struct PadG<double> { static constexpr int G = 8; };
 
 template <typename T> __host__ __device__ inline int x_rowlen(int n) { return n + n / PadG<T>::G + 1; }
+// Twiddle table of the compile-time X passes: padded (tw_pad) in double, where it took
+// iLSQR's FP64 X pass at length 384 from 523 to 504 us; dense in float, where the extra
+// index arithmetic made the length-256 passes slower (r2c 25.5 -> 27.2 us).
+template <typename T> constexpr bool x_tw_padded() { return sizeof(T) == 8; }
+template <typename T> __host__ __device__ constexpr int x_tw_len(int n) {
+  return x_tw_padded<T>() ? tw_table_len(n) : n;
+}
 
 // Identity pointwise op: Y/Z passes with it go smem -> registers -> global.
 template <typename T> struct OpId {
@@ -212,10 +219,11 @@ __global__ void k_x_full_fx(Geom g, const cplx_t<T>* __restrict__ twg, Load ld, 
   static_assert(D1 != 0 && D2 != 0, "both transforms");
   if (done != nullptr && *done) return;
   extern __shared__ __align__(16) unsigned char smraw[];
+  constexpr bool TWP = x_tw_padded<T>();
   C* tw = reinterpret_cast<C*>(smraw);
-  C* sm = tw + N;
+  C* sm = tw + x_tw_len<T>(N);
   const int tid = threadIdx.x + threadIdx.y * blockDim.x;
-  for (int i = tid; i < N; i += blockDim.x * blockDim.y) tw[i] = twg[i];
+  for (int i = tid; i < N; i += blockDim.x * blockDim.y) tw[TWP ? tw_pad(i) : i] = twg[i];
   const int t = threadIdx.x;
   const int row = blockIdx.x * blockDim.y + threadIdx.y;
   const bool active = row < g.nrows() && t < TT;
@@ -231,8 +239,8 @@ __global__ void k_x_full_fx(Geom g, const cplx_t<T>* __restrict__ twg, Load ld, 
   auto hook = [&](int e, C x) -> C { return mid(x, row, e); };
   EmitInRegs<decltype(hook)> keep{hook};
   FetchInRegs in_regs;
-  FP::template run_v<D1>(v, t, active, sp, sa, tw, fetch_g, keep);
-  ReversePlan<FP>::type::template run_v<D2>(v, t, active, sp, sa, tw, in_regs, emit_g);
+  FP::template run_v<D1, TWP>(v, t, active, sp, sa, tw, fetch_g, keep);
+  ReversePlan<FP>::type::template run_v<D2, TWP>(v, t, active, sp, sa, tw, in_regs, emit_g);
   st.finish();
 }
 
@@ -331,10 +339,11 @@ __global__ void k_x_r2c_fx(Geom g, const cplx_t<T>* __restrict__ twg, cplx_t<T>*
   using C = cplx_t<T>;
   constexpr int N = FP::n, TT = FP::T, NXH = N / 2 + 1;
   extern __shared__ __align__(16) unsigned char smraw[];
+  constexpr bool TWP = x_tw_padded<T>();
   C* tw = reinterpret_cast<C*>(smraw);
-  C* sm = tw + N;
+  C* sm = tw + x_tw_len<T>(N);
   const int tid = threadIdx.x + threadIdx.y * blockDim.x;
-  for (int i = tid; i < N; i += blockDim.x * blockDim.y) tw[i] = twg[i];
+  for (int i = tid; i < N; i += blockDim.x * blockDim.y) tw[TWP ? tw_pad(i) : i] = twg[i];
   if (done != nullptr && *done) return;
   const int t = threadIdx.x;
   const int p = threadIdx.y;
@@ -346,7 +355,7 @@ __global__ void k_x_r2c_fx(Geom g, const cplx_t<T>* __restrict__ twg, cplx_t<T>*
   SAPadded<PadG<T>::G> sa;
   auto fetch = [&](int e) -> C { return mk<C>(ld(a, e), hasb ? ld(b, e) : T(0)); };
   auto emit = [&](int e, C v) { sp[sa(e)] = v; };
-  FP::template run<-1>(t, active, sp, sa, tw, fetch, emit);
+  FP::template run<-1, TWP>(t, active, sp, sa, tw, fetch, emit);
   // Here rather than between the stages, where the discards slowed the pass (27.0
   // against 25.3 us at 256x256x176); the c2r pass gains from the earlier point.
   if constexpr (DEAD) {
@@ -376,10 +385,11 @@ __global__ void k_x_c2r_fx(Geom g, const cplx_t<T>* __restrict__ twg, const cplx
   using C = cplx_t<T>;
   constexpr int N = FP::n, TT = FP::T;
   extern __shared__ __align__(16) unsigned char smraw[];
+  constexpr bool TWP = x_tw_padded<T>();
   C* tw = reinterpret_cast<C*>(smraw);
-  C* sm = tw + N;
+  C* sm = tw + x_tw_len<T>(N);
   const int tid = threadIdx.x + threadIdx.y * blockDim.x;
-  for (int i = tid; i < N; i += blockDim.x * blockDim.y) tw[i] = twg[i];
+  for (int i = tid; i < N; i += blockDim.x * blockDim.y) tw[TWP ? tw_pad(i) : i] = twg[i];
   if (done != nullptr && *done) return;
   const int t = threadIdx.x;
   const int p = threadIdx.y;
@@ -415,7 +425,7 @@ __global__ void k_x_c2r_fx(Geom g, const cplx_t<T>* __restrict__ twg, const cplx
     }
   };
   C v[kFftEmax];
-  FP::template run_v<+1>(v, t, active, sp, sa, tw, fetch, emit, release);
+  FP::template run_v<+1, TWP>(v, t, active, sp, sa, tw, fetch, emit, release);
   st.finish();
 }
 
