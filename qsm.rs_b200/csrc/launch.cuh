@@ -598,7 +598,7 @@ void tune_yz_fixed(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* scratch, const std
       ensure_smem(kern, smem);                                                                    \
       const auto cands = yz_candidates(f, fx_cols<T>(), kern, fx_cols<T>() * FP::T, smem);                  \
       if (chain != nullptr)                                                                       \
-        autotune_pick(ctx, key, cands, [&](int c) { ctx->tuned[key] = TuneRec{c, {}}; (*chain)(); }, 2, 3); \
+        autotune_pick(ctx, key, cands, [&](int c) { ctx->tuned[key] = TuneRec{c, {}}; (*chain)(); }, 3, 4); \
       else                                                                                        \
         autotune_pick(ctx, key, cands, [&](int c) {                                               \
           launch_yz_fx<T, DIR, AXIS, FP>(ctx, f, c, scratch, scratch, nullptr, false);             \
@@ -629,7 +629,7 @@ void tune_z_fused_m(qsm_ctx* ctx, const Fft3<T>& f, cplx_t<T>* scratch, T* mscra
       ensure_smem(kfx, smem);                                                                     \
       const auto cands = yz_candidates(f, kZmCols, kfx, kZmCols * FP::T, smem);                   \
       if (chain != nullptr)                                                                       \
-        autotune_pick(ctx, key, cands, [&](int c) { ctx->tuned[key] = TuneRec{c, {}}; (*chain)(); }, 2, 3); \
+        autotune_pick(ctx, key, cands, [&](int c) { ctx->tuned[key] = TuneRec{c, {}}; (*chain)(); }, 3, 4); \
       else                                                                                        \
         autotune_pick(ctx, key, cands, [&](int c) {                                               \
           launch_zm_fx<T, FP>(ctx, f, c, scratch, scratch, mscratch, nullptr, false);              \

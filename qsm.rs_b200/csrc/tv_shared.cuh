@@ -824,13 +824,24 @@ extern template void tv_fft<float>(qsm_ctx*, const TvVol<float>&, int, const int
 extern template void tv_fft<double>(qsm_ctx*, const TvVol<double>&, int, const int*);
 template <typename T> void tv_fft(qsm_ctx* ctx, const TvVol<T>& v, int q) { tv_fft(ctx, v, q, &v.st->done); }
 
-// Each pass's candidates are timed inside the iteration's own chain of FFT passes (X r2c,
-// Y, Z, Y, X c2r on the volume's buffers, which hold no data yet), one pass after the other
-// with the passes already tuned at their choice: timed alone, back to back with itself,
-// a pass favoured shapes that were slower in the chain (one block per tile: 17.0 against
-// 18.6 us alone, 201.4 against 196.4 us per TV-ADMM iteration at 256x256x176).
+// Each pass's candidates are timed inside a whole iteration (the stencil, then X r2c, Y,
+// Z, Y, X c2r on the volume's buffers, which hold no data yet), one pass after the other
+// with the passes already tuned at their choice.  Timed alone, back to back with itself,
+// a pass favoured shapes that were slower in the iteration (one block per tile: 17.0
+// against 18.6 us alone, 201.4 against 196.4 us per TV-ADMM iteration at 256x256x176);
+// timed in the FFT passes without the stencil, with L2 holding the spectrum rather than
+// the stencil's streams, the fused Z pass's pick changed from box to box (35.5 against
+// 37.2 us in the iteration).  The stencil runs on a state made for the tuning (iteration
+// 2, tol 0, so it never stops early); every caller initialises the state afterwards.
 template <typename T> void tv_tune(qsm_ctx* ctx, const TvVol<T>& v) {
-  const std::function<void()> chain = [&] { tv_fft(ctx, v, 0, nullptr); };
+  TvState tune_state{};
+  tune_state.k = 2;
+  tune_state.tol = 0.0;
+  QSM_CUDA(cudaMemcpyAsync(v.st, &tune_state, sizeof(TvState), cudaMemcpyHostToDevice, ctx->stream));
+  const std::function<void()> chain = [&] {
+    tv_step_launch(ctx, v, 0, 0);
+    tv_fft(ctx, v, 0, nullptr);
+  };
   tune_yz_fixed<T, -1, 1, true>(ctx, v.f, v.spec, &chain);
   tune_yz_fixed<T, +1, 1, true>(ctx, v.f, v.spec, &chain);
   if (v.use_mult) tune_z_fused_m<T, true>(ctx, v.f, v.spec, v.mult, &chain);
